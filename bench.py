@@ -1,0 +1,366 @@
+"""Benchmark of the XaNSoNS histogram hot path on B200.
+
+Workload (one "step"): the DebyePDF scenario of calcPDFandDebye on a seeded synthetic rock-salt
+nanocube -- 30^3 unit cells, a = 5.64 A, 10 % vacancies, Gaussian displacement 0.07 A (~1.94e5 atoms,
+two species with neutron lengths 3.63 / 9.58 fm): the per-element-pair u64 pair-distance histogram at
+0.001 A bins (bit-identical to the reference), the rPDF on those bins, and I(q) on 4096 q points in
+[0.1, 25) A^-1.  Metric: atom pairs per second (N(N-1)/2 pairs per step).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Ours: `value` times the device-resident path (xns_pdf_and_debye_device: coordinates already in HBM),
+`e2e` the host-buffer C-ABI call (xns_calc_pdf_and_debye) from pinned host memory, H2D and D2H inside
+the timed region.  L2 (126 MB) is flushed by writing a 512 MB buffer before every timed step (the
+inputs, 4.7 MB, would otherwise stay L2-resident).  With N ranks each rank computes its own structure
+(seed = rank): weak scaling, no collective on the data path; the time is the max over ranks.
+
+Reference: the reference's own CPU calc functions (CalcFunctions.cpp compiled from its sources into
+oracle/_ref/libxnsref.so; the FP64 oracle port if that build is absent) on all host cores, on a bounded
+sample of the same workload (a smaller cube of the same lattice), rank 0 only.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "softx-d-16-00083_b200"))
+
+METRIC = "atom-pairs/s"
+CELLS, A, VAC, SIGMA = 30, 5.64, 0.1, 0.07
+BIN, NQ, QMIN, QMAX = 0.001, 4096, 0.1, 25.0
+SL = [3.63, 9.58]
+HIST_FLOPS_PER_PAIR = 10  # the reference's per-pair FP64 arithmetic: 3 sub, 3 mul, 2 add, sqrt, divide
+
+
+def workload(seed, cells=CELLS):
+    from xns_b200 import synth
+    els = synth.rocksalt_cube(cells=cells, a=A, vacancy=VAC, sigma=SIGMA, seed=seed)
+    nh = synth.hist_size(els, BIN)
+    q = synth.q_mesh(QMIN, QMAX, NQ)
+    p0 = atomic_density(els)
+    return els, nh, q, p0
+
+
+def atomic_density(els):
+    """GetAtomicDensity (CalcFunctions.cpp:204-223) restated in numpy: atoms within a third of the
+    ensemble size of the centre, divided by that sphere's volume."""
+    xyz = np.concatenate(els)
+    c = xyz.mean(axis=0)
+    d2 = ((xyz - c) ** 2).sum(axis=1)
+    r2 = (0.33333 * 2 * np.sqrt(d2.max())) ** 2
+    return float((d2 < r2).sum() / (4 / 3 * np.pi * np.sqrt(r2) ** 3))
+
+
+def npairs(els):
+    n = sum(len(e) for e in els)
+    return n * (n - 1) // 2
+
+
+def config_block(els, nh, extra=None):
+    c = {"workload": "DebyePDF rock-salt nanocube %d^3 cells a=%.2f A, %d atoms, hist bin %.3f A (%d bins x 3 pairs), "
+                     "rPDF, I(q) %d q in [%.1f,%.1f)" % (CELLS, A, sum(len(e) for e in els), BIN, nh, NQ, QMIN, QMAX),
+         "atoms": int(sum(len(e) for e in els)), "pairs_per_step": int(npairs(els)), "nhist": int(nh), "nq": NQ,
+         "l2": "flushed (512 MB write) before every timed step"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ---- clocks -----------------------------------------------------------------------------------------
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---- CPU baseline ---------------------------------------------------------------------------------
+def cpu_reference_sample(target_s=12.0):
+    """Times the reference's calcPDFandDebye (DebyePDF, rPDF, the same bin and q mesh) on a cube of the
+    same lattice, grown until one pass takes about target_s.  Returns (pairs/s, kind, cores, sample)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    cores = os.cpu_count() or 1
+    try:
+        R = orc.Reference(threads=cores)
+        kind = "reference"
+    except FileNotFoundError:
+        R = None
+        kind = "port"
+    O = orc.Oracle()
+
+    def run(cells):
+        els, nh, q, p0 = workload(1000, cells)
+        t = time.perf_counter()
+        if R is not None:
+            R.pdf_and_debye(els, nh, BIN, 4, 2, p0, q, 0, sl=SL)
+        else:
+            h = O.hist(els, nh, BIN)
+            O.pdf(h, [len(e) for e in els], nh, BIN, 2, p0, SL)
+            O.int_1d_hist(h, [len(e) for e in els], nh, BIN, q, 0, sl=SL)
+        return time.perf_counter() - t, els
+
+    cells = 6
+    dt, els = run(cells)
+    while dt < target_s / 4 and cells < CELLS:
+        # pairs grow as cells^6, the transform as cells: step the size by the measured time
+        grow = min(max((target_s / max(dt, 1e-3)) ** (1 / 6), 1.15), 1.8)
+        cells = min(CELLS, max(cells + 1, int(cells * grow)))
+        dt, els = run(cells)
+    pairs = npairs(els)
+    sample = ("one calcPDFandDebye pass (histogram + rPDF + I(q), %d q) on a %d^3-cell cube of the same lattice, %d atoms, "
+              "%.3g pairs, %.2f s" % (NQ, cells, sum(len(e) for e in els), pairs, dt))
+    return pairs / dt, kind, cores, sample, (cells, dt)
+
+
+# ---- reference arm --------------------------------------------------------------------------------
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    v, kind, cores, sample, (cells, dt0) = cpu_reference_sample()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    els, nh, q, p0 = workload(1000, cells)
+    if kind == "reference":
+        R = orc.Reference(threads=cores)
+        step = lambda: R.pdf_and_debye(els, nh, BIN, 4, 2, p0, q, 0, sl=SL)  # noqa: E731
+    else:
+        O = orc.Oracle()
+
+        def step():
+            h = O.hist(els, nh, BIN)
+            O.pdf(h, [len(e) for e in els], nh, BIN, 2, p0, SL)
+            O.int_1d_hist(h, [len(e) for e in els], nh, BIN, q, 0, sl=SL)
+    for _ in range(args.warmup):
+        step()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = (time.perf_counter() - t) / args.steps
+    value = npairs(els) / dt
+    line = {"metric": METRIC, "value": value, "unit": "pairs/s", "impl": "reference", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": config_block(*workload(0)[:2], extra={"sample": sample, "reference_cells": cells}),
+            "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---- our arm --------------------------------------------------------------------------------------
+def ours(args, rank, world, local_rank):
+    import ctypes as C
+
+    import torch
+    import xns_b200
+    from xns_b200 import lib
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    ctx = xns_b200.Context(local_rank)
+    stream = torch.cuda.current_stream(dev)
+    ctx.set_stream(stream.cuda_stream)
+
+    els, nh, q, p0 = workload(rank)
+    n_el = np.array([len(e) for e in els], dtype=np.uint32)
+    P = 3
+    pairs = npairs(els)
+    sl = np.array(SL)
+    xyz = np.ascontiguousarray(np.concatenate(els))
+    d_xyz = torch.from_numpy(xyz).to(dev)
+    d_hist = torch.zeros(P * nh, dtype=torch.int64, device=dev)
+    d_I = torch.zeros(NQ, dtype=torch.float64, device=dev)
+    d_pdf = torch.zeros((1 + P) * nh, dtype=torch.float64, device=dev)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    p = C.c_void_p
+
+    def step_device():
+        st = lib.xns_pdf_and_debye_device(ctx.handle, p(d_xyz.data_ptr()), n_el.ctypes.data_as(p), len(n_el), nh, BIN, 4, 2,
+                                          p0, q.ctypes.data_as(p), NQ, 0, None, sl.ctypes.data_as(p), 0, 0.0,
+                                          p(d_I.data_ptr()), p(d_pdf.data_ptr()), p(d_hist.data_ptr()))
+        if st:
+            raise xns_b200.XnsError(st, lib.xns_last_error(ctx.handle).decode())
+
+    lib.xns_pdf_and_debye_device.argtypes = [p, p, p, C.c_uint32, C.c_uint32, C.c_double, C.c_int, C.c_int, C.c_double, p,
+                                             C.c_uint32, C.c_int, p, p, C.c_int, C.c_double, p, p, p]
+    lib.xns_last_stage_ms.argtypes = [p, C.c_int]
+    lib.xns_last_stage_ms.restype = C.c_double
+    lib.xns_measure_fma_peak.argtypes = [p, C.c_int, C.POINTER(C.c_double)]
+
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+
+    def barrier():
+        if dist:
+            tdist.barrier()
+
+    # warm-up
+    for _ in range(args.warmup):
+        step_device()
+    torch.cuda.synchronize()
+
+    clocks = Clocks(local_rank)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    launches0 = ctx.kernel_launches
+    total_ms, hist_ms, iq_ms, pdf_ms = 0.0, 0.0, 0.0, 0.0
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        ev0.record(stream)
+        step_device()
+        ev1.record(stream)
+        ev1.synchronize()
+        total_ms += ev0.elapsed_time(ev1)
+        hist_ms += lib.xns_last_stage_ms(ctx.handle, 0)
+        pdf_ms += lib.xns_last_stage_ms(ctx.handle, 1)
+        iq_ms += lib.xns_last_stage_ms(ctx.handle, 2)
+    torch.cuda.synchronize()
+    barrier()
+    launches = ctx.kernel_launches - launches0
+    clk = clocks.stop()
+    ms_step = total_ms / args.steps
+    if dist:
+        t = torch.tensor([ms_step], device=dev)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        ms_step = float(t.item())
+
+    # end-to-end through the host-buffer C ABI from pinned host memory
+    pin_xyz = [torch.from_numpy(np.ascontiguousarray(e)).pin_memory() for e in els]
+    table = (C.c_void_p * len(els))(*[t.data_ptr() for t in pin_xyz])
+    pin_I = torch.zeros(NQ, dtype=torch.float64).pin_memory()
+    pin_pdf = torch.zeros((1 + P) * nh, dtype=torch.float64).pin_memory()
+    lib.xns_calc_pdf_and_debye.argtypes = [p, p, p, C.c_uint32, C.c_uint32, C.c_double, C.c_int, C.c_int, C.c_double, p,
+                                           C.c_uint32, C.c_int, p, p, C.c_int, C.c_double, p, p, p]
+
+    def step_e2e():
+        st = lib.xns_calc_pdf_and_debye(ctx.handle, table, n_el.ctypes.data_as(p), len(n_el), nh, BIN, 4, 2, p0,
+                                        q.ctypes.data_as(p), NQ, 0, None, sl.ctypes.data_as(p), 0, 0.0,
+                                        p(pin_I.data_ptr()), p(pin_pdf.data_ptr()), None)
+        if st:
+            raise xns_b200.XnsError(st, lib.xns_last_error(ctx.handle).decode())
+
+    for _ in range(max(1, args.warmup // 2)):
+        step_e2e()
+    e2e_ms = 0.0
+    barrier()
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        ev0.record(stream)
+        step_e2e()
+        ev1.record(stream)
+        ev1.synchronize()
+        e2e_ms += ev0.elapsed_time(ev1)
+    e2e_ms /= args.steps
+    if dist:
+        t = torch.tensor([e2e_ms], device=dev)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    h2d = int(xyz.nbytes + q.nbytes + sl.nbytes)
+    d2h = int(NQ * 8 + (1 + P) * nh * 8)
+
+    if rank != 0:
+        return 0
+    # roofline of the dominant kernel: the histogram, FP64-pipe bound
+    peak = C.c_double(0)
+    lib.xns_measure_fma_peak(ctx.handle, 1, C.byref(peak))
+    peak32 = C.c_double(0)
+    lib.xns_measure_fma_peak(ctx.handle, 0, C.byref(peak32))
+    hist_avg = hist_ms / args.steps
+    achieved = HIST_FLOPS_PER_PAIR * pairs / (hist_avg * 1e-3) / 1e12
+    line = {"metric": METRIC, "value": world * pairs / (ms_step * 1e-3), "unit": "pairs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 distances + u64 counts (histogram), f32 sums with f64 "
+                                                                "reductions (I(q))",
+            "data": "synthetic (seeded)",
+            "patterns_per_s": world / (ms_step * 1e-3),
+            "config": config_block(els, nh, {"parallelism": "replicas x%d (one structure per rank)" % world}),
+            "stages_ms": {"histogram": hist_avg, "pdf": pdf_ms / args.steps, "iq": iq_ms / args.steps},
+            "roofline": {"kernel": "hist_tiles_kernel", "bound": "fp64", "achieved": achieved, "peak": peak.value,
+                         "unit": "TFLOP/s", "frac": achieved / peak.value if peak.value else None, "traffic": None,
+                         "peak_source": "measured in-process (DFMA loop, xns_measure_fma_peak)",
+                         "flops_per_pair": HIST_FLOPS_PER_PAIR, "fp32_peak_tflops": peak32.value},
+            "e2e": {"value": world * pairs / (e2e_ms * 1e-3), "unit": "pairs/s", "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(launches), "clocks": clk}
+    if world == 1 and not args.no_cpu_baseline:
+        v, kind, cores, sample, _ = cpu_reference_sample()
+        line["cpu_baseline"] = {"value": v, "unit": "pairs/s", "cores": cores, "kind": kind, "sample": sample}
+    print(json.dumps(line))
+    ctx.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local_rank))
+    try:
+        return ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as tdist
+            tdist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

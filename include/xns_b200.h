@@ -1,0 +1,137 @@
+/* xns_b200 -- B200 (sm_100a) implementation of the XaNSoNS scattering calc functions.
+ *
+ * C ABI: plain pointers and sizes, int status, caller-owned outputs.  The library owns its device
+ * memory and its CUDA stream; every call is synchronous with respect to the host buffers it is given.
+ *
+ * Conventions shared by all entry points
+ *   - Coordinates are passed per element, exactly as the reference's vector<vect3d<double>> ra[Nel]
+ *     holds them: xyz_el[e] points at n_el[e] packed x y z double triples (vect3d<double> is three
+ *     doubles, typedefs.h:83-142, so &ra[e][0].x can be passed directly).
+ *   - Element pairs (a <= b) are numbered in the reference's loop order (a outer, b inner);
+ *     P = nel(nel+1)/2.  Histograms are element-pair major: hist[t*nhist + k].
+ *   - source: XNS_NEUTRON uses sl[e] (scattering lengths); XNS_XRAY uses ff[e][iq] (form factor on the
+ *     q mesh), as the reference's SL / FF vectors (ReadXML.cpp:329-331).
+ *   - The q mesh is the array the reference builds, q[i] = qmin + i*(qmax-qmin)/N (ReadXML.cpp:220-222);
+ *     uniform meshes take the fast path, any other mesh a per-term kernel.
+ *   - Errors: a non-zero status; xns_last_error() gives a one-line description.  On error the
+ *     outputs are unspecified.  No entry point falls back to CPU computation.
+ */
+#ifndef XNS_B200_H
+#define XNS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define XNS_OK 0
+#define XNS_ERR_ARG 1      /* invalid argument */
+#define XNS_ERR_CUDA 2     /* CUDA runtime error (message in xns_last_error) */
+#define XNS_ERR_NODEV 3    /* no sm_100 device / library not built for it */
+#define XNS_ERR_RANGE 4    /* a pair distance fell beyond the histogram (reference: out-of-bounds write) */
+#define XNS_ERR_NOMEM 5    /* device allocation failed */
+
+/* typedefs.h:50-56 */
+#define XNS_NEUTRON 0
+#define XNS_XRAY 1
+#define XNS_RDF 0
+#define XNS_PDF 1
+#define XNS_RPDF 2
+/* scenarios, typedefs.h:43-47 */
+#define XNS_DEBYE_HIST 2
+#define XNS_PDF_ONLY 3
+#define XNS_DEBYE_PDF 4
+
+typedef struct xns_ctx xns_ctx;
+
+/* Context on one CUDA device (device = -1 picks the current one).  Replaces the reference's
+ * SetDeviceCuda (CalcFunctionsCUDA.cu:1485-1519): it requires compute capability 10.x. */
+int xns_create(int device, xns_ctx **out);
+void xns_destroy(xns_ctx *ctx);
+const char *xns_last_error(const xns_ctx *ctx);
+const char *xns_status_string(int status);
+/* Run on the caller's stream (a cudaStream_t) instead of the library's own; NULL restores it. */
+int xns_set_stream(xns_ctx *ctx, void *stream);
+/* Device time of the most recent call's kernels, in milliseconds (CUDA events). */
+double xns_last_kernel_ms(const xns_ctx *ctx);
+/* Number of kernels the library launched since the context was created. */
+uint64_t xns_kernel_launches(const xns_ctx *ctx);
+/* Kernel-only device time (CUDA events on the library's stream) of one stage of the most recent call:
+ * 0 histogram, 1 PDF, 2 histogram -> I(q), 3 Debye double sum, 4 2D amplitude; -1 if it did not run. */
+double xns_last_stage_ms(const xns_ctx *ctx, int stage);
+
+/* ---- host-buffer entry points (what the reference's calc functions become) ---------------------- */
+
+/* Pair-distance histogram.  Replaces calcHist (CalcFunctions.cpp:757-809) and calcHistCuda
+ * (CalcFunctionsCUDA.cu:855-920).  hist: P*nhist counts, bit-identical to the reference's FP64
+ * (unsigned int)(|ri-rj|/bin).  XNS_ERR_RANGE if some distance maps to a bin >= nhist. */
+int xns_calc_hist(xns_ctx *ctx, const double *const *xyz_el, const uint32_t *n_el, uint32_t nel, uint32_t nhist, double bin,
+                  uint64_t *hist);
+
+/* Histogram -> I(q).  Replaces calcInt1DHist (CalcFunctions.cpp:810-911) and calcInt1DHistCuda
+ * (CalcFunctionsCUDA.cu:988-1045).  ff: nel pointers to nq doubles (X-ray) or NULL; sl: nel doubles
+ * (neutron) or NULL.  I: nq doubles, already divided by ntot and polarisation-corrected if polar. */
+int xns_calc_int_1d_hist(xns_ctx *ctx, const uint64_t *hist, const uint32_t *n_el, uint32_t nel, uint32_t nhist, double bin,
+                         const double *q, uint32_t nq, int source, const double *const *ff, const double *sl, int polar,
+                         double lambda, double *I);
+
+/* PDF / RDF / rPDF from a histogram.  Replaces the PDF branch of calcPDFandDebye
+ * (CalcFunctions.cpp:919-960) and calcPDFCuda (CalcFunctionsCUDA.cu:1048-1160).  sl: the per-element
+ * weights the reference uses there.  pdf: (1+P)*nhist doubles, total first. */
+int xns_calc_pdf(xns_ctx *ctx, const uint64_t *hist, const uint32_t *n_el, uint32_t nel, uint32_t nhist, double bin,
+                 int pdftype, double p0, const double *sl, double *pdf);
+
+/* Histogram + PDF + I(q) in one device pass.  Replaces calcPDFandDebye (CalcFunctions.cpp:912-968) and
+ * calcPDFandDebyeCuda (CalcFunctionsCUDA.cu:1078-1160).  scenario: XNS_DEBYE_HIST, XNS_PDF_ONLY or
+ * XNS_DEBYE_PDF; I (nq) is written for DEBYE_HIST / DEBYE_PDF, pdf ((1+P)*nhist) for PDF_ONLY / DEBYE_PDF.
+ * hist_out, when non-NULL, receives the P*nhist counts as well. */
+int xns_calc_pdf_and_debye(xns_ctx *ctx, const double *const *xyz_el, const uint32_t *n_el, uint32_t nel, uint32_t nhist,
+                           double bin, int scenario, int pdftype, double p0, const double *q, uint32_t nq, int source,
+                           const double *const *ff, const double *sl, int polar, double lambda, double *I, double *pdf,
+                           uint64_t *hist_out);
+
+/* Exact Debye double sum.  Replaces calcIntDebye (CalcFunctions.cpp:547-633) and calcIntDebyeCuda
+ * (CalcFunctionsCUDA.cu:1276-1355).  I: nq doubles. */
+int xns_calc_int_debye(xns_ctx *ctx, const double *const *xyz_el, const uint32_t *n_el, uint32_t nel, const double *q,
+                       uint32_t nq, int source, const double *const *ff, const double *sl, int polar, double lambda, double *I);
+
+/* Debye double sum split into block-pair parts.  Replaces calcIntPartialDebye (CalcFunctions.cpp:634-756)
+ * and calcIntPartialDebyeCuda (CalcFunctionsCUDA.cu:1377-1481).  n_el_block[e*nblocks+b] = atoms of
+ * element e in block b (ra[e] holds block 0's atoms first).  I: (1 + nblocks(nblocks+1)/2)*nq, total first. */
+int xns_calc_int_partial_debye(xns_ctx *ctx, const double *const *xyz_el, const uint32_t *n_el, uint32_t nel,
+                               uint32_t nblocks, const uint32_t *n_el_block, const double *q, uint32_t nq, int source,
+                               const double *const *ff, const double *sl, int polar, double lambda, double *I);
+
+/* 2D pattern on the reference's polar (q, phi) mesh, averaged over the Euler-angle mesh.  Replaces
+ * calcInt2D (CalcFunctions.cpp:969-1091) and calcInt2DCuda (CalcFunctionsCUDA.cu:653-776).  Euler angles
+ * in radians; convention as typedefs.h:59-70.  I2D: nq x nfi row-major; I: nq (phi average). */
+int xns_calc_int_2d(xns_ctx *ctx, const double *const *xyz_el, const uint32_t *n_el, uint32_t nel, const double *q,
+                    uint32_t nq, uint32_t nfi, const double *euler_min, const double *euler_max, const uint32_t *euler_n,
+                    uint32_t convention, double lambda, int source, const double *const *ff, const double *sl, int polar,
+                    double *I2D, double *I);
+
+/* ---- device-buffer entry points ----------------------------------------------------------------- */
+
+/* calcPDFandDebye (CalcFunctions.cpp:912-968) on device-resident data: xyz_dev is a device array of
+ * sum(n_el) x y z double triples, element-major (the reference's dataCopyCUDA staging,
+ * CalcFunctionsCUDA.cu:1522-1555, kept in FP64); hist_dev (P*nhist), I_dev (nq) and pdf_dev
+ * ((1+P)*nhist) are device arrays.  q, ff, sl stay host arrays.  Synchronous: returns after the
+ * kernels finished; xns_last_kernel_ms() gives their device time. */
+int xns_pdf_and_debye_device(xns_ctx *ctx, const double *xyz_dev, const uint32_t *n_el, uint32_t nel, uint32_t nhist,
+                             double bin, int scenario, int pdftype, double p0, const double *q, uint32_t nq, int source,
+                             const double *const *ff, const double *sl, int polar, double lambda, double *I_dev,
+                             double *pdf_dev, uint64_t *hist_dev);
+
+/* ---- utilities (no reference counterpart) -------------------------------------------------------- */
+
+/* Measured FMA-pipe throughput of this device in TFLOP/s (an FMA counts 2 flops): FP64 when fp64 != 0,
+ * FP32 otherwise.  The roofline denominator for the FP64 distance and FP32 sinc kernels. */
+int xns_measure_fma_peak(xns_ctx *ctx, int fp64, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* XNS_B200_H */

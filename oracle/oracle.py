@@ -1,0 +1,230 @@
+"""Test infrastructure only: ctypes access to the checkers.
+
+    Oracle()      the FP64 C restatement (oracle/liboracle.so, built from xns_oracle.c)
+    Reference()   the reference's own CPU calc functions compiled from its sources
+                  (oracle/_ref/libxnsref.so, built by oracle/Makefile where the sources exist)
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU legs use this module, as the checker or the
+timed CPU baseline; the product never does.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libxnsref.so")
+
+_p = C.c_void_p
+_u32 = C.c_uint32
+_dbl = C.c_double
+_int = C.c_int
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_p)
+
+
+def _flat(elements):
+    arrs = [np.ascontiguousarray(e, dtype=np.float64).reshape(-1, 3) for e in elements]
+    n_el = np.array([len(a) for a in arrs], dtype=np.uint32)
+    xyz = np.ascontiguousarray(np.concatenate(arrs) if len(arrs) else np.zeros((0, 3)))
+    return xyz, n_el
+
+
+def _ff(ff, nq):
+    return None if ff is None else np.ascontiguousarray(np.asarray(ff, dtype=np.float64).reshape(-1, nq))
+
+
+def _f64(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Oracle:
+    def __init__(self, path=ORACLE_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError("%s is not built (make -C oracle)" % path)
+        L = self.lib = C.CDLL(path)
+        L.xo_rot_matrix.argtypes = [_p, _u32, _p]
+        L.xo_hist_size.argtypes = [_p, _p, _u32, _dbl]
+        L.xo_hist_size.restype = _u32
+        L.xo_atomic_density.argtypes = [_p, _p, _u32]
+        L.xo_atomic_density.restype = _dbl
+        L.xo_hist.argtypes = [_p, _p, _u32, _u32, _dbl, _p]
+        L.xo_int_debye.argtypes = [_p, _p, _u32, _p, _u32, _int, _p, _p, _int, _dbl, _p]
+        L.xo_int_partial_debye.argtypes = [_p, _p, _u32, _u32, _p, _p, _u32, _int, _p, _p, _int, _dbl, _p]
+        L.xo_int_1d_hist.argtypes = [_p, _p, _u32, _u32, _dbl, _p, _u32, _int, _p, _p, _int, _dbl, _p]
+        L.xo_pdf.argtypes = [_p, _p, _u32, _u32, _dbl, _int, _dbl, _p, _p]
+        L.xo_int_2d.argtypes = [_p, _p, _u32, _p, _u32, _u32, _p, _p, _p, _u32, _dbl, _int, _p, _p, _int, _p, _p]
+        L.xo_amp_plane.argtypes = [_p, _p, _u32, _dbl, _dbl, _u32, _dbl, _dbl, _u32, _int, _p, _p, _p]
+
+    def rot_matrix(self, euler, convention):
+        e = _f64(euler)
+        m = np.zeros(9)
+        self.lib.xo_rot_matrix(_ptr(e), convention, _ptr(m))
+        return m.reshape(3, 3)
+
+    def hist_size(self, elements, bin):
+        xyz, n = _flat(elements)
+        return self.lib.xo_hist_size(_ptr(xyz), _ptr(n), len(n), bin)
+
+    def atomic_density(self, elements):
+        xyz, n = _flat(elements)
+        return self.lib.xo_atomic_density(_ptr(xyz), _ptr(n), len(n))
+
+    def hist(self, elements, nhist, bin):
+        xyz, n = _flat(elements)
+        out = np.zeros(len(n) * (len(n) + 1) // 2 * nhist, dtype=np.uint64)
+        if self.lib.xo_hist(_ptr(xyz), _ptr(n), len(n), nhist, bin, _ptr(out)):
+            raise ValueError("pair distance beyond nhist")
+        return out
+
+    def int_debye(self, elements, q, source, ff=None, sl=None, polar=False, lam=0.0):
+        xyz, n = _flat(elements)
+        q = _f64(q)
+        out = np.zeros(len(q))
+        self.lib.xo_int_debye(_ptr(xyz), _ptr(n), len(n), _ptr(q), len(q), source, _ptr(_ff(ff, len(q))), _ptr(_f64(sl)),
+                              int(polar), lam, _ptr(out))
+        return out
+
+    def int_partial_debye(self, elements, n_el_block, q, source, ff=None, sl=None, polar=False, lam=0.0):
+        xyz, n = _flat(elements)
+        neb = np.ascontiguousarray(n_el_block, dtype=np.uint32)
+        nb = neb.shape[1]
+        q = _f64(q)
+        out = np.zeros((1 + nb * (nb + 1) // 2) * len(q))
+        self.lib.xo_int_partial_debye(_ptr(xyz), _ptr(n), len(n), nb, _ptr(neb), _ptr(q), len(q), source,
+                                      _ptr(_ff(ff, len(q))), _ptr(_f64(sl)), int(polar), lam, _ptr(out))
+        return out
+
+    def int_1d_hist(self, hist, n_el, nhist, bin, q, source, ff=None, sl=None, polar=False, lam=0.0):
+        h = np.ascontiguousarray(hist, dtype=np.uint64)
+        n = np.ascontiguousarray(n_el, dtype=np.uint32)
+        q = _f64(q)
+        out = np.zeros(len(q))
+        self.lib.xo_int_1d_hist(_ptr(h), _ptr(n), len(n), nhist, bin, _ptr(q), len(q), source, _ptr(_ff(ff, len(q))),
+                                _ptr(_f64(sl)), int(polar), lam, _ptr(out))
+        return out
+
+    def pdf(self, hist, n_el, nhist, bin, pdftype, p0, sl):
+        h = np.ascontiguousarray(hist, dtype=np.uint64)
+        n = np.ascontiguousarray(n_el, dtype=np.uint32)
+        P = len(n) * (len(n) + 1) // 2
+        out = np.zeros((1 + P) * nhist)
+        self.lib.xo_pdf(_ptr(h), _ptr(n), len(n), nhist, bin, pdftype, p0, _ptr(_f64(sl)), _ptr(out))
+        return out
+
+    def int_2d(self, elements, q, nfi, euler_min, euler_max, euler_n, convention, lam, source, ff=None, sl=None,
+               polar=False):
+        xyz, n = _flat(elements)
+        q = _f64(q)
+        I2D = np.zeros((len(q), nfi))
+        I = np.zeros(len(q))
+        en = np.ascontiguousarray(euler_n, dtype=np.uint32)
+        self.lib.xo_int_2d(_ptr(xyz), _ptr(n), len(n), _ptr(q), len(q), nfi, _ptr(_f64(euler_min)), _ptr(_f64(euler_max)),
+                           _ptr(en), convention, lam, source, _ptr(_ff(ff, len(q))), _ptr(_f64(sl)), int(polar), _ptr(I2D),
+                           _ptr(I))
+        return I2D, I
+
+    def amp_plane(self, elements, qx0, dqx, nqx, qy0, dqy, nqy, source, coef=None, sl=None):
+        xyz, n = _flat(elements)
+        out = np.zeros((nqy, nqx))
+        self.lib.xo_amp_plane(_ptr(xyz), _ptr(n), len(n), qx0, dqx, nqx, qy0, dqy, nqy, source,
+                              _ptr(_f64(coef)), _ptr(_f64(sl)), _ptr(out))
+        return out
+
+
+class Reference:
+    """The reference's own calc functions (CalcFunctions.cpp) behind oracle/ref_harness.cpp."""
+
+    def __init__(self, path=REF_SO, threads=None):
+        if not os.path.exists(path):
+            raise FileNotFoundError("%s is not built (make -C oracle ref, needs the reference sources)" % path)
+        self.threads = threads or os.cpu_count() or 1
+        L = self.lib = C.CDLL(path)
+        L.xnsref_rot_matrix.argtypes = [_p, _u32, _p]
+        L.xnsref_hist_size.argtypes = [_p, _p, _u32, _dbl]
+        L.xnsref_hist_size.restype = _u32
+        L.xnsref_atomic_density.argtypes = [_p, _p, _u32]
+        L.xnsref_atomic_density.restype = _dbl
+        L.xnsref_calc_hist.argtypes = [_p, _p, _u32, _u32, _dbl, _int, _p]
+        L.xnsref_calc_int_debye.argtypes = [_p, _p, _u32, _p, _u32, _int, _p, _p, _int, _dbl, _int, _p]
+        L.xnsref_calc_int_partial_debye.argtypes = [_p, _p, _u32, _u32, _p, _p, _u32, _int, _p, _p, _int, _dbl, _int, _p]
+        L.xnsref_calc_int_1d_hist.argtypes = [_p, _p, _u32, _u32, _dbl, _p, _u32, _int, _p, _p, _int, _dbl, _int, _p]
+        L.xnsref_calc_pdf_and_debye.argtypes = [_p, _p, _u32, _u32, _dbl, _int, _int, _dbl, _p, _u32, _int, _p, _p, _int,
+                                                _dbl, _int, _p, _p]
+        L.xnsref_calc_int_2d.argtypes = [_p, _p, _u32, _p, _u32, _u32, _p, _p, _p, _u32, _dbl, _int, _p, _p, _int, _int,
+                                         _p, _p]
+
+    def rot_matrix(self, euler, convention):
+        e = _f64(euler)
+        m = np.zeros(9)
+        self.lib.xnsref_rot_matrix(_ptr(e), convention, _ptr(m))
+        return m.reshape(3, 3)
+
+    def hist_size(self, elements, bin):
+        xyz, n = _flat(elements)
+        return self.lib.xnsref_hist_size(_ptr(xyz), _ptr(n), len(n), bin)
+
+    def atomic_density(self, elements):
+        xyz, n = _flat(elements)
+        return self.lib.xnsref_atomic_density(_ptr(xyz), _ptr(n), len(n))
+
+    def hist(self, elements, nhist, bin):
+        xyz, n = _flat(elements)
+        out = np.zeros(len(n) * (len(n) + 1) // 2 * nhist, dtype=np.uint64)
+        self.lib.xnsref_calc_hist(_ptr(xyz), _ptr(n), len(n), nhist, bin, self.threads, _ptr(out))
+        return out
+
+    def int_debye(self, elements, q, source, ff=None, sl=None, polar=False, lam=0.0):
+        xyz, n = _flat(elements)
+        q = _f64(q)
+        out = np.zeros(len(q))
+        self.lib.xnsref_calc_int_debye(_ptr(xyz), _ptr(n), len(n), _ptr(q), len(q), source, _ptr(_ff(ff, len(q))),
+                                       _ptr(_f64(sl)), int(polar), lam, self.threads, _ptr(out))
+        return out
+
+    def int_partial_debye(self, elements, n_el_block, q, source, ff=None, sl=None, polar=False, lam=0.0):
+        xyz, n = _flat(elements)
+        neb = np.ascontiguousarray(n_el_block, dtype=np.uint32)
+        nb = neb.shape[1]
+        q = _f64(q)
+        out = np.zeros((1 + nb * (nb + 1) // 2) * len(q))
+        self.lib.xnsref_calc_int_partial_debye(_ptr(xyz), _ptr(n), len(n), nb, _ptr(neb), _ptr(q), len(q), source,
+                                               _ptr(_ff(ff, len(q))), _ptr(_f64(sl)), int(polar), lam, self.threads,
+                                               _ptr(out))
+        return out
+
+    def int_1d_hist(self, hist, n_el, nhist, bin, q, source, ff=None, sl=None, polar=False, lam=0.0):
+        h = np.ascontiguousarray(hist, dtype=np.uint64)
+        n = np.ascontiguousarray(n_el, dtype=np.uint32)
+        q = _f64(q)
+        out = np.zeros(len(q))
+        self.lib.xnsref_calc_int_1d_hist(_ptr(h), _ptr(n), len(n), nhist, bin, _ptr(q), len(q), source,
+                                         _ptr(_ff(ff, len(q))), _ptr(_f64(sl)), int(polar), lam, self.threads, _ptr(out))
+        return out
+
+    def pdf_and_debye(self, elements, nhist, bin, scenario, pdftype, p0, q, source, ff=None, sl=None, polar=False,
+                      lam=0.0):
+        xyz, n = _flat(elements)
+        P = len(n) * (len(n) + 1) // 2
+        q = _f64(q) if q is not None else np.zeros(1)
+        I = np.zeros(len(q))
+        pdf = np.zeros((1 + P) * nhist)
+        self.lib.xnsref_calc_pdf_and_debye(_ptr(xyz), _ptr(n), len(n), nhist, bin, scenario, pdftype, p0, _ptr(q), len(q),
+                                           source, _ptr(_ff(ff, len(q))), _ptr(_f64(sl)), int(polar), lam, self.threads,
+                                           _ptr(I), _ptr(pdf))
+        return I, pdf
+
+    def int_2d(self, elements, q, nfi, euler_min, euler_max, euler_n, convention, lam, source, ff=None, sl=None,
+               polar=False):
+        xyz, n = _flat(elements)
+        q = _f64(q)
+        I2D = np.zeros((len(q), nfi))
+        I = np.zeros(len(q))
+        en = np.ascontiguousarray(euler_n, dtype=np.uint32)
+        self.lib.xnsref_calc_int_2d(_ptr(xyz), _ptr(n), len(n), _ptr(q), len(q), nfi, _ptr(_f64(euler_min)),
+                                    _ptr(_f64(euler_max)), _ptr(en), convention, lam, source, _ptr(_ff(ff, len(q))),
+                                    _ptr(_f64(sl)), int(polar), self.threads, _ptr(I2D), _ptr(I))
+        return I2D, I

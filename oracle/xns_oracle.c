@@ -1,0 +1,429 @@
+/* Test infrastructure only -- the ORACLE, not the product.  See xns_oracle.h.
+ *
+ * FP64 restatement of the reference CPU calc functions.  The arithmetic of every quantity that the
+ * reference turns into an integer (the histogram bin index) is written operation by operation in the
+ * reference's order and compiled without FMA contraction, so histograms are bit-identical to the
+ * reference's.  Floating-point sums are accumulated in a different order than the reference's
+ * OpenMP zig-zag schedule, so intensities agree to FP64 rounding (~1e-13 relative), not bit for bit.
+ */
+#include "xns_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define XO_PI 3.1415926535897932384626433832795028841971693993 /* typedefs.h:73 */
+
+static uint32_t total_atoms(const uint32_t *n_el, uint32_t nel) {
+  uint32_t n = 0;
+  for (uint32_t e = 0; e < nel; e++) n += n_el[e];
+  return n;
+}
+
+static size_t el_offset(const uint32_t *n_el, uint32_t e) {
+  size_t off = 0;
+  for (uint32_t i = 0; i < e; i++) off += n_el[i];
+  return off;
+}
+
+/* vect3d::mag() of (ri - rj): sqrt(SQR(x) + SQR(y) + SQR(z)), typedefs.h:130 */
+static double pair_dist(const double *ri, const double *rj) {
+  double dx = ri[0] - rj[0], dy = ri[1] - rj[1], dz = ri[2] - rj[2];
+  return sqrt(dx * dx + dy * dy + dz * dz);
+}
+
+/* ---- rotation ------------------------------------------------------------------------------- */
+
+static void rot_axis(int axis, double a, double m[9]) {
+  double c = cos(a), s = sin(a);
+  memset(m, 0, 9 * sizeof(double));
+  if (axis == 0) { m[0] = 1; m[4] = c; m[5] = -s; m[7] = s; m[8] = c; }
+  if (axis == 1) { m[4] = 1; m[0] = c; m[2] = s; m[6] = -s; m[8] = c; }
+  if (axis == 2) { m[8] = 1; m[0] = c; m[1] = -s; m[3] = s; m[4] = c; }
+}
+
+static void mat_mul(const double a[9], const double b[9], double out[9]) {
+  double t[9];
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++) t[3 * r + c] = a[3 * r] * b[c] + a[3 * r + 1] * b[3 + c] + a[3 * r + 2] * b[6 + c];
+  memcpy(out, t, sizeof(t));
+}
+
+/* calcRotMatrix, CalcFunctions.cpp:46-115: for convention "UVW" (typedefs.h:59-70) the matrix is the
+ * intrinsic product R_U(alpha) R_V(beta) R_W(gamma). */
+void xo_rot_matrix(const double euler[3], uint32_t convention, double m[9]) {
+  static const int axes[12][3] = {{0, 2, 0}, {0, 1, 0}, {1, 0, 1}, {1, 2, 1}, {2, 1, 2}, {2, 0, 2},
+                                  {0, 2, 1}, {0, 1, 2}, {1, 0, 2}, {1, 2, 0}, {2, 1, 0}, {2, 0, 1}};
+  double r0[9], r1[9], r2[9];
+  const int *ax = axes[convention % 12];
+  rot_axis(ax[0], euler[0], r0);
+  rot_axis(ax[1], euler[1], r1);
+  rot_axis(ax[2], euler[2], r2);
+  mat_mul(r0, r1, m);
+  mat_mul(m, r2, m);
+}
+
+/* ---- structure metadata --------------------------------------------------------------------- */
+
+/* GetHistSize, CalcFunctions.cpp:224-243 */
+uint32_t xo_hist_size(const double *xyz, const uint32_t *n_el, uint32_t nel, double bin) {
+  uint32_t n = total_atoms(n_el, nel);
+  if (!n) return 1;
+  double mx[3], mn[3];
+  for (int k = 0; k < 3; k++) mx[k] = mn[k] = xyz[k];
+  for (uint32_t i = 0; i < n; i++)
+    for (int k = 0; k < 3; k++) {
+      double v = xyz[3 * (size_t)i + k];
+      if (mx[k] < v) mx[k] = v;
+      if (mn[k] > v) mn[k] = v;
+    }
+  double d[3] = {mx[0] - mn[0], mx[1] - mn[1], mx[2] - mn[2]};
+  return (uint32_t)(sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) / bin) + 1;
+}
+
+/* GetCenter / GetEnsembleSize / GetAtomicDensity, CalcFunctions.cpp:197-223 */
+double xo_atomic_density(const double *xyz, const uint32_t *n_el, uint32_t nel) {
+  uint32_t n = total_atoms(n_el, nel);
+  double c[3] = {0, 0, 0};
+  for (uint32_t i = 0; i < n; i++)
+    for (int k = 0; k < 3; k++) c[k] += xyz[3 * (size_t)i + k];
+  for (int k = 0; k < 3; k++) c[k] /= n;
+  double rmax = 0;
+  for (uint32_t i = 0; i < n; i++) {
+    double dx = c[0] - xyz[3 * (size_t)i], dy = c[1] - xyz[3 * (size_t)i + 1], dz = c[2] - xyz[3 * (size_t)i + 2];
+    double s = dx * dx + dy * dy + dz * dz;
+    if (s > rmax) rmax = s;
+  }
+  double size = 2. * sqrt(rmax);
+  double r2 = (0.33333 * size) * (0.33333 * size);
+  uint32_t count = 0;
+  for (uint32_t i = 0; i < n; i++) {
+    double dx = c[0] - xyz[3 * (size_t)i], dy = c[1] - xyz[3 * (size_t)i + 1], dz = c[2] - xyz[3 * (size_t)i + 2];
+    if (dx * dx + dy * dy + dz * dz < r2) count++;
+  }
+  double r = sqrt(r2);
+  return count / (4. / 3. * XO_PI * r * r * r);
+}
+
+/* ---- histogram ------------------------------------------------------------------------------ */
+
+/* calcHist, CalcFunctions.cpp:757-809: for a <= b, pairs i<j (a == b) or all (i, j), bin
+ * (unsigned int)(rij / bin) with rij from vect3d::mag() in FP64. */
+int xo_hist(const double *xyz, const uint32_t *n_el, uint32_t nel, uint32_t nhist, double bin, uint64_t *hist) {
+  uint32_t P = nel * (nel + 1) / 2;
+  memset(hist, 0, sizeof(uint64_t) * (size_t)P * nhist);
+  int bad = 0;
+  uint32_t t = 0;
+  for (uint32_t a = 0; a < nel; a++) {
+    for (uint32_t b = a; b < nel; b++, t++) {
+      const double *ra = xyz + 3 * el_offset(n_el, a), *rb = xyz + 3 * el_offset(n_el, b);
+      uint64_t *h = hist + (size_t)t * nhist;
+      int na = (int)n_el[a];
+#pragma omp parallel reduction(| : bad)
+      {
+        uint64_t *loc = (uint64_t *)calloc(nhist, sizeof(uint64_t));
+#pragma omp for schedule(dynamic, 16)
+        for (int i = 0; i < na; i++) {
+          uint32_t j0 = (a == b) ? (uint32_t)i + 1 : 0;
+          for (uint32_t j = j0; j < n_el[b]; j++) {
+            double r = pair_dist(ra + 3 * (size_t)i, rb + 3 * (size_t)j);
+            double k = r / bin;
+            if (!(k < (double)nhist)) { bad = 1; continue; }
+            loc[(uint32_t)k] += 1;
+          }
+        }
+#pragma omp critical
+        for (uint32_t k = 0; k < nhist; k++) h[k] += loc[k];
+        free(loc);
+      }
+    }
+  }
+  return bad ? -1 : 0;
+}
+
+/* ---- Debye sums ----------------------------------------------------------------------------- */
+
+/* PolarFactor1D, CalcFunctions.cpp:460-468 */
+static void polar_1d(double *I, const double *q, double lambda, uint32_t nq) {
+  for (uint32_t iq = 0; iq < nq; iq++) {
+    double s = q[iq] * (lambda * 0.25 / XO_PI);
+    double c2 = 1. - 2. * s * s;
+    I[iq] *= 0.5 * (1. + c2 * c2);
+  }
+}
+
+static double weight(int source, const double *ff, const double *sl, uint32_t nq, uint32_t e, uint32_t iq) {
+  return source == XO_XRAY ? ff[(size_t)e * nq + iq] : sl[e];
+}
+
+/* Sum over the pairs (i in [i0,i1) of element a, j in element b, j > i when same element) of
+ * sin(q r)/(q r + 1e-8), CalcFunctions.cpp:574-583; acc[nq] += result.  jlo/jhi restrict j. */
+static void debye_pairs(const double *ra, const double *rb, uint32_t i0, uint32_t i1, uint32_t jlo, uint32_t jhi, int same,
+                        const double *q, uint32_t nq, double *acc) {
+#pragma omp parallel
+  {
+    double *loc = (double *)calloc(nq, sizeof(double));
+#pragma omp for schedule(dynamic, 4)
+    for (int i = (int)i0; i < (int)i1; i++) {
+      uint32_t js = jlo;
+      if (same && (uint32_t)i + 1 > js) js = (uint32_t)i + 1;
+      for (uint32_t j = js; j < jhi; j++) {
+        double r = pair_dist(ra + 3 * (size_t)i, rb + 3 * (size_t)j);
+        for (uint32_t iq = 0; iq < nq; iq++) {
+          double x = r * q[iq];
+          loc[iq] += sin(x) / (x + 0.00000001);
+        }
+      }
+    }
+#pragma omp critical
+    for (uint32_t iq = 0; iq < nq; iq++) acc[iq] += loc[iq];
+    free(loc);
+  }
+}
+
+/* calcIntDebye, CalcFunctions.cpp:547-633 */
+void xo_int_debye(const double *xyz, const uint32_t *n_el, uint32_t nel, const double *q, uint32_t nq, int source,
+                  const double *ff, const double *sl, int polar, double lambda, double *I) {
+  uint32_t ntot = total_atoms(n_el, nel);
+  double *s = (double *)malloc(sizeof(double) * nq);
+  memset(I, 0, sizeof(double) * nq);
+  for (uint32_t a = 0; a < nel; a++)
+    for (uint32_t b = a; b < nel; b++) {
+      memset(s, 0, sizeof(double) * nq);
+      debye_pairs(xyz + 3 * el_offset(n_el, a), xyz + 3 * el_offset(n_el, b), 0, n_el[a], 0, n_el[b], a == b, q, nq, s);
+      for (uint32_t iq = 0; iq < nq; iq++)
+        I[iq] += s[iq] * weight(source, ff, sl, nq, a, iq) * weight(source, ff, sl, nq, b, iq) * 2.;
+    }
+  for (uint32_t e = 0; e < nel; e++)
+    for (uint32_t iq = 0; iq < nq; iq++) {
+      double w = weight(source, ff, sl, nq, e, iq);
+      I[iq] += n_el[e] * (w * w);
+    }
+  for (uint32_t iq = 0; iq < nq; iq++) I[iq] /= ntot;
+  if (polar) polar_1d(I, q, lambda, nq);
+  free(s);
+}
+
+/* calcIntPartialDebye, CalcFunctions.cpp:634-756.  Part index of blocks (u <= v):
+ * nblocks*u - u(u+1)/2 + v (:686). */
+void xo_int_partial_debye(const double *xyz, const uint32_t *n_el, uint32_t nel, uint32_t nblocks, const uint32_t *n_el_block,
+                          const double *q, uint32_t nq, int source, const double *ff, const double *sl, int polar,
+                          double lambda, double *I) {
+  uint32_t ntot = total_atoms(n_el, nel);
+  uint32_t nparts = nblocks * (nblocks + 1) / 2;
+  double *s = (double *)malloc(sizeof(double) * nq);
+  memset(I, 0, sizeof(double) * (size_t)(nparts + 1) * nq);
+  for (uint32_t a = 0; a < nel; a++)
+    for (uint32_t b = a; b < nel; b++) {
+      const double *ra = xyz + 3 * el_offset(n_el, a), *rb = xyz + 3 * el_offset(n_el, b);
+      uint32_t ia = 0;
+      for (uint32_t u = 0; u < nblocks; u++) {
+        uint32_t na = n_el_block[a * nblocks + u];
+        uint32_t jb = 0;
+        for (uint32_t v = 0; v < nblocks; v++) {
+          uint32_t nb = n_el_block[b * nblocks + v];
+          if (a != b || v >= u) {
+            uint32_t lo = u < v ? u : v, hi = u < v ? v : u;
+            uint32_t part = nblocks * lo - lo * (lo + 1) / 2 + hi;
+            memset(s, 0, sizeof(double) * nq);
+            debye_pairs(ra, rb, ia, ia + na, jb, jb + nb, a == b, q, nq, s);
+            for (uint32_t iq = 0; iq < nq; iq++)
+              I[(size_t)(part + 1) * nq + iq] +=
+                  s[iq] * weight(source, ff, sl, nq, a, iq) * weight(source, ff, sl, nq, b, iq) * 2.;
+          }
+          jb += nb;
+        }
+        ia += na;
+      }
+    }
+  for (uint32_t e = 0; e < nel; e++)
+    for (uint32_t u = 0; u < nblocks; u++) {
+      uint32_t part = nblocks * u - u * (u + 1) / 2 + u;
+      for (uint32_t iq = 0; iq < nq; iq++) {
+        double w = weight(source, ff, sl, nq, e, iq);
+        I[(size_t)(part + 1) * nq + iq] += n_el_block[e * nblocks + u] * (w * w);
+      }
+    }
+  for (size_t k = nq; k < (size_t)(nparts + 1) * nq; k++) I[k] /= ntot;
+  if (polar)
+    for (uint32_t p = 1; p <= nparts; p++) polar_1d(I + (size_t)p * nq, q, lambda, nq);
+  for (uint32_t p = 1; p <= nparts; p++)
+    for (uint32_t iq = 0; iq < nq; iq++) I[iq] += I[(size_t)p * nq + iq];
+  free(s);
+}
+
+/* calcInt1DHist, CalcFunctions.cpp:810-911: r_k = (k + 0.5) bin, empty bins skipped (:857). */
+void xo_int_1d_hist(const uint64_t *hist, const uint32_t *n_el, uint32_t nel, uint32_t nhist, double bin, const double *q,
+                    uint32_t nq, int source, const double *ff, const double *sl, int polar, double lambda, double *I) {
+  uint32_t ntot = total_atoms(n_el, nel);
+  double *s = (double *)malloc(sizeof(double) * nq);
+  memset(I, 0, sizeof(double) * nq);
+  uint32_t t = 0;
+  for (uint32_t a = 0; a < nel; a++)
+    for (uint32_t b = a; b < nel; b++, t++) {
+      const uint64_t *h = hist + (size_t)t * nhist;
+      memset(s, 0, sizeof(double) * nq);
+#pragma omp parallel
+      {
+        double *loc = (double *)calloc(nq, sizeof(double));
+#pragma omp for schedule(static)
+        for (int k = 0; k < (int)nhist; k++) {
+          if (!h[k]) continue;
+          double r = ((double)k + 0.5) * bin;
+          for (uint32_t iq = 0; iq < nq; iq++) {
+            double x = r * q[iq];
+            loc[iq] += h[k] * sin(x) / (x + 0.00000001);
+          }
+        }
+#pragma omp critical
+        for (uint32_t iq = 0; iq < nq; iq++) s[iq] += loc[iq];
+        free(loc);
+      }
+      for (uint32_t iq = 0; iq < nq; iq++)
+        I[iq] += 2. * s[iq] * weight(source, ff, sl, nq, a, iq) * weight(source, ff, sl, nq, b, iq);
+    }
+  for (uint32_t e = 0; e < nel; e++)
+    for (uint32_t iq = 0; iq < nq; iq++) {
+      double w = weight(source, ff, sl, nq, e, iq);
+      I[iq] += n_el[e] * (w * w);
+    }
+  for (uint32_t iq = 0; iq < nq; iq++) I[iq] /= ntot;
+  if (polar) polar_1d(I, q, lambda, nq);
+  free(s);
+}
+
+/* PDF branch of calcPDFandDebye, CalcFunctions.cpp:919-960.  As in the reference, the radius of
+ * element pair t's bin k is evaluated as (t*nhist + k + 0.5)*bin (the loop variable runs over the
+ * concatenated histogram, :939-951); for t = 0 that is the bin centre. */
+void xo_pdf(const uint64_t *hist, const uint32_t *n_el, uint32_t nel, uint32_t nhist, double bin, int pdftype, double p0,
+            const double *sl, double *pdf) {
+  uint32_t ntot = total_atoms(n_el, nel);
+  uint32_t P = nel * (nel + 1) / 2;
+  memset(pdf, 0, sizeof(double) * (size_t)(1 + P) * nhist);
+  double fav2 = 0;
+  for (uint32_t e = 0; e < nel; e++) fav2 += sl[e] * n_el[e];
+  fav2 /= ntot;
+  fav2 *= fav2;
+  size_t nstart = 0;
+  for (uint32_t a = 0; a < nel; a++)
+    for (uint32_t b = a; b < nel; b++, nstart += nhist) {
+      double mult, sub, r, mij = sl[a] * sl[b] / fav2;
+      for (size_t i = nstart; i < nstart + nhist; i++) {
+        switch (pdftype) {
+          case XO_RDF:
+            mult = 2. / (bin * ntot);
+            pdf[nhist + i] = hist[i] * mult;
+            break;
+          case XO_PDF:
+            mult = 0.5 / (XO_PI * bin * p0 * ntot);
+            r = (i + 0.5) * bin;
+            pdf[nhist + i] = hist[i] * mult / (r * r);
+            break;
+          default:
+            mult = 2. / (bin * ntot);
+            sub = (b > a) ? 8. * XO_PI * p0 * (double)n_el[a] * (double)n_el[b] / ((double)ntot * (double)ntot)
+                          : 4. * XO_PI * p0 * ((double)n_el[a] * (double)n_el[a]) / ((double)ntot * (double)ntot);
+            r = (i + 0.5) * bin;
+            pdf[nhist + i] = hist[i] * mult / r - sub * r;
+            break;
+        }
+      }
+      for (uint32_t i = 0; i < nhist; i++) pdf[i] += pdf[nhist + nstart + i] * mij;
+    }
+}
+
+/* ---- 2D ------------------------------------------------------------------------------------- */
+
+/* calcInt2D, CalcFunctions.cpp:969-1091 (including sin(theta) = q lambda/4pi, "costheta" = 1 - sin^2,
+ * :999-1002; Euler mesh mid-points, :1007-1018; normalisation, polarisation and phi average, :1066-1076) */
+void xo_int_2d(const double *xyz, const uint32_t *n_el, uint32_t nel, const double *q, uint32_t nq, uint32_t nfi,
+               const double euler_min[3], const double euler_max[3], const uint32_t euler_n[3], uint32_t convention,
+               double lambda, int source, const double *ff, const double *sl, int polar, double *I2D, double *I) {
+  uint32_t ntot = total_atoms(n_el, nel);
+  double dfi = 2. * XO_PI / nfi;
+  double d[3];
+  for (int k = 0; k < 3; k++) d[k] = euler_n[k] < 2 ? 0 : (euler_max[k] - euler_min[k]) / euler_n[k];
+  memset(I2D, 0, sizeof(double) * (size_t)nq * nfi);
+  for (uint32_t ia = 0; ia < euler_n[0]; ia++)
+    for (uint32_t ib = 0; ib < euler_n[1]; ib++)
+      for (uint32_t ig = 0; ig < euler_n[2]; ig++) {
+        double eul[3] = {euler_min[0] + (ia + 0.5) * d[0], euler_min[1] + (ib + 0.5) * d[1], euler_min[2] + (ig + 0.5) * d[2]};
+        double m[9];
+        xo_rot_matrix(eul, convention, m);
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int iq = 0; iq < (int)nq; iq++) {
+          double st = q[iq] * (lambda * 0.25 / XO_PI), ct = 1. - st * st;
+          for (uint32_t ifi = 0; ifi < nfi; ifi++) {
+            double v[3] = {ct * cos(ifi * dfi) * q[iq], ct * sin(ifi * dfi) * q[iq], -st * q[iq]};
+            /* qv' = R^T qv (CS rows are the columns of R, :1020-1022) */
+            double w[3];
+            for (int c = 0; c < 3; c++) w[c] = v[0] * m[c] + v[1] * m[3 + c] + v[2] * m[6 + c];
+            double Ar = 0, Ai = 0;
+            size_t off = 0;
+            for (uint32_t e = 0; e < nel; e++) {
+              double ar = 0, ai = 0;
+              for (uint32_t j = 0; j < n_el[e]; j++, off++) {
+                const double *r = xyz + 3 * off;
+                double x = w[0] * r[0] + w[1] * r[1] + w[2] * r[2];
+                ar += cos(x);
+                ai += sin(x);
+              }
+              double f = weight(source, ff, sl, nq, e, (uint32_t)iq);
+              Ar += f * ar;
+              Ai += f * ai;
+            }
+            I2D[(size_t)iq * nfi + ifi] += Ar * Ar + Ai * Ai;
+          }
+        }
+      }
+  double norm = 1. / ((double)ntot * euler_n[0] * euler_n[1] * euler_n[2]);
+  for (uint32_t iq = 0; iq < nq; iq++) {
+    double fac = 1;
+    if (polar) {
+      double s = q[iq] * (lambda * 0.25 / XO_PI), c2 = 1. - 2. * s * s;
+      fac = 0.5 * (1. + c2 * c2);
+    }
+    double sum = 0;
+    for (uint32_t ifi = 0; ifi < nfi; ifi++) {
+      double *p = I2D + (size_t)iq * nfi + ifi;
+      *p *= norm;
+      *p *= fac;
+      sum += *p;
+    }
+    I[iq] = sum / nfi;
+  }
+}
+
+double xo_ff_gauss(const double *c, double q) {
+  double s2 = (q / (4. * XO_PI)) * (q / (4. * XO_PI));
+  return c[0] * exp(-c[4] * s2) + c[1] * exp(-c[5] * s2) + c[2] * exp(-c[6] * s2) + c[3] * exp(-c[7] * s2) + c[8];
+}
+
+void xo_amp_plane(const double *xyz, const uint32_t *n_el, uint32_t nel, double qx0, double dqx, uint32_t nqx, double qy0,
+                  double dqy, uint32_t nqy, int source, const double *coef, const double *sl, double *I) {
+  uint32_t ntot = total_atoms(n_el, nel);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int iy = 0; iy < (int)nqy; iy++) {
+    double qy = qy0 + iy * dqy;
+    for (uint32_t ix = 0; ix < nqx; ix++) {
+      double qx = qx0 + ix * dqx, qm = sqrt(qx * qx + qy * qy);
+      double Ar = 0, Ai = 0;
+      size_t off = 0;
+      for (uint32_t e = 0; e < nel; e++) {
+        double ar = 0, ai = 0;
+        for (uint32_t j = 0; j < n_el[e]; j++, off++) {
+          double x = qx * xyz[3 * off] + qy * xyz[3 * off + 1];
+          ar += cos(x);
+          ai += sin(x);
+        }
+        double f = source == XO_XRAY ? xo_ff_gauss(coef + 9 * e, qm) : sl[e];
+        Ar += f * ar;
+        Ai += f * ai;
+      }
+      I[(size_t)iy * nqx + ix] = (Ar * Ar + Ai * Ai) / ntot;
+    }
+  }
+}

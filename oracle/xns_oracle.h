@@ -1,0 +1,75 @@
+/* Test infrastructure only -- the ORACLE, not the product.
+ *
+ * An FP64 C restatement of the reference XaNSoNS CPU calc functions (CalcFunctions.cpp), used by
+ * tests/ and by bench.py's CPU-baseline leg to check the CUDA library.  Each function cites the
+ * reference lines it restates.  It is pinned against the reference's own code compiled from source
+ * (oracle/_ref/libxnsref.so, built by oracle/Makefile) and against the committed golden vectors in
+ * tests/golden/.  Nothing in the product links or calls this file.
+ *
+ * Coordinates are one flat array of x y z triples, element-major: element 0's n_el[0] atoms first,
+ * in the same order as the reference's ra[0], then element 1's, ...  Element pairs (a <= b) are
+ * numbered in the reference's loop order (a outer, b inner), P = nel(nel+1)/2.
+ */
+#ifndef XNS_ORACLE_H
+#define XNS_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define XO_NEUTRON 0
+#define XO_XRAY 1
+#define XO_RDF 0
+#define XO_PDF 1
+#define XO_RPDF 2
+
+/* calcRotMatrix (CalcFunctions.cpp:46-115): intrinsic rotation for the 12 Euler conventions
+ * (XZX=0 ... ZXY=11, typedefs.h:59-70); m is row-major 3x3. */
+void xo_rot_matrix(const double euler[3], uint32_t convention, double m[9]);
+
+/* GetHistSize (CalcFunctions.cpp:224-243) and GetAtomicDensity (:204-223). */
+uint32_t xo_hist_size(const double *xyz, const uint32_t *n_el, uint32_t nel, double bin);
+double xo_atomic_density(const double *xyz, const uint32_t *n_el, uint32_t nel);
+
+/* calcHist (CalcFunctions.cpp:757-809): u64 counts of (unsigned)(|ri - rj| / bin), element pair
+ * major.  Returns 0, or -1 when a distance falls beyond nhist (the reference writes out of bounds
+ * there; the restatement refuses). */
+int xo_hist(const double *xyz, const uint32_t *n_el, uint32_t nel, uint32_t nhist, double bin, uint64_t *hist);
+
+/* calcIntDebye (CalcFunctions.cpp:547-633).  ff: nel rows of nq (X-ray); sl: nel (neutron). */
+void xo_int_debye(const double *xyz, const uint32_t *n_el, uint32_t nel, const double *q, uint32_t nq, int source,
+                  const double *ff, const double *sl, int polar, double lambda, double *I);
+
+/* calcIntPartialDebye (CalcFunctions.cpp:634-756).  n_el_block[e*nblocks+b]; I: (1+Nparts)*nq, total first. */
+void xo_int_partial_debye(const double *xyz, const uint32_t *n_el, uint32_t nel, uint32_t nblocks, const uint32_t *n_el_block,
+                          const double *q, uint32_t nq, int source, const double *ff, const double *sl, int polar,
+                          double lambda, double *I);
+
+/* calcInt1DHist (CalcFunctions.cpp:810-911). */
+void xo_int_1d_hist(const uint64_t *hist, const uint32_t *n_el, uint32_t nel, uint32_t nhist, double bin, const double *q,
+                    uint32_t nq, int source, const double *ff, const double *sl, int polar, double lambda, double *I);
+
+/* PDF branch of calcPDFandDebye (CalcFunctions.cpp:919-960); pdf: (1+P)*nhist, total first. */
+void xo_pdf(const uint64_t *hist, const uint32_t *n_el, uint32_t nel, uint32_t nhist, double bin, int pdftype, double p0,
+            const double *sl, double *pdf);
+
+/* calcInt2D (CalcFunctions.cpp:969-1091).  Euler angles in radians.  I2D: nq x nfi row-major. */
+void xo_int_2d(const double *xyz, const uint32_t *n_el, uint32_t nel, const double *q, uint32_t nq, uint32_t nfi,
+               const double euler_min[3], const double euler_max[3], const uint32_t euler_n[3], uint32_t convention,
+               double lambda, int source, const double *ff, const double *sl, int polar, double *I2D, double *I);
+
+/* Cartesian q-plane (no reference counterpart; the reference's amplitude sum CalcFunctions.cpp:1026-1046
+ * evaluated at q = (qx0 + ix*dqx, qy0 + iy*dqy, 0)).  Form factor per element: X-ray
+ * f(q) = sum_k a_k exp(-b_k (q/4pi)^2) + c with coef[e*9 + 0..3] = a, [4..7] = b, [8] = c;
+ * neutron f = sl[e].  I: nqy rows of nqx, I[iy*nqx+ix] = |A|^2 / Ntot. */
+void xo_amp_plane(const double *xyz, const uint32_t *n_el, uint32_t nel, double qx0, double dqx, uint32_t nqx, double qy0,
+                  double dqy, uint32_t nqy, int source, const double *coef, const double *sl, double *I);
+
+/* Form factor model used by xo_amp_plane. */
+double xo_ff_gauss(const double *coef9, double q);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,161 @@
+// Histogram -> I(q) (replaces calcInt1DHist, CalcFunctions.cpp:810-911, and calcIntHistKernel*,
+// CalcFunctionsCUDA.cu:923-1045) and the fused histogram + PDF + I(q) entry point (calcPDFandDebye,
+// CalcFunctions.cpp:912-968).
+//
+//   I(q) = [ sum_e N_e w_e^2 + 2 sum_{a<=b} w_a w_b sum_k n_ab(k) sin(q r_k)/(q r_k + 1e-8) ] / N,
+//   r_k = (k + 0.5) * bin; empty bins contribute nothing (the reference skips them, :857).
+//
+// Each tile of SE_TILE bins of one element pair becomes a tile of sinc records (r_k, n_k) for the
+// shared sinc engine (sinc_engine.cuh).
+#include <string.h>
+
+#include "sinc_engine.cuh"
+
+using namespace xns_sinc;
+
+namespace {
+
+struct BinSrc {
+  const unsigned long long *hist;
+  uint32_t nhist;
+  uint32_t tiles_per_pair;
+  double bin;
+
+  __device__ uint32_t cls(unsigned long long w) const { return (uint32_t)(w / tiles_per_pair); }
+
+  __device__ int fill(unsigned long long w, PairRec *pr, void *, double dq) const {
+    const uint32_t t = (uint32_t)(w / tiles_per_pair);
+    const uint32_t b0 = (uint32_t)(w % tiles_per_pair) * SE_TILE;
+    const unsigned long long *h = hist + (size_t)t * nhist;
+    for (int e = threadIdx.x; e < SE_TILE; e += SE_THREADS) {
+      const uint32_t k = b0 + e;
+      PairRec rec = null_rec();
+      if (k < nhist) {
+        unsigned long long n = h[k];
+        if (n) rec = make_rec(((double)k + 0.5) * bin, (double)n, dq);
+      }
+      pr[e] = rec;
+    }
+    __syncthreads();
+    return SE_TILE;
+  }
+};
+
+}  // namespace
+
+int xns_hist_iq_device(xns_ctx *ctx, const unsigned long long *d_hist, const uint32_t *n_el, uint32_t nel, uint32_t nhist,
+                       double bin, const double *q, uint32_t nq, const double *d_w, int polar, double lambda, double *d_I) {
+  const uint32_t P = xns_npairs(nel);
+  uint32_t ntot = 0;
+  for (uint32_t e = 0; e < nel; e++) ntot += n_el[e];
+  if (ntot == 0) return xns_fail(ctx, XNS_ERR_ARG, "I(q): no atoms");
+  double q0 = 0, dq = 0;
+  const bool uniform = xns_uniform_mesh(q, nq, &q0, &dq);
+  SincParams p{};
+  p.q0 = q0;
+  p.dq = dq;
+  p.nq = nq;
+  p.ncls = P;
+  const uint32_t tpp = (nhist + SE_TILE - 1) / SE_TILE;
+  p.ntiles = (unsigned long long)tpp * P;
+  int st;
+  if (!uniform && (st = sinc_upload_q(ctx, q, nq, &p.q))) return st;
+  BinSrc src{d_hist, nhist, tpp, bin};
+  int grid = 0;
+  if ((st = xns_stage_begin(ctx, STAGE_IQ))) return st;
+  if ((st = run_sinc(ctx, p, src, 0, uniform, &grid))) return st;
+  if ((st = sinc_epilogue(ctx, grid, P, nel, 1, n_el, q, nq, uniform, q0, dq, d_w, ntot, polar, lambda, d_I))) return st;
+  return xns_stage_end(ctx, STAGE_IQ);
+}
+
+extern "C" int xns_calc_int_1d_hist(xns_ctx *ctx, const uint64_t *hist, const uint32_t *n_el, uint32_t nel, uint32_t nhist,
+                                    double bin, const double *q, uint32_t nq, int source, const double *const *ff,
+                                    const double *sl, int polar, double lambda, double *I) {
+  if (!ctx) return XNS_ERR_ARG;
+  if (!hist || !n_el || !q || !I || nel == 0 || nq == 0 || nhist == 0 || !(bin > 0))
+    return xns_fail(ctx, XNS_ERR_ARG, "I(q) from histogram: null pointer or zero size");
+  int st;
+  const size_t hbytes = sizeof(uint64_t) * (size_t)xns_npairs(nel) * nhist;
+  void *d_hist, *d_I;
+  if ((st = xns_scratch(ctx, SLOT_HIST, hbytes, &d_hist))) return st;
+  XNS_CUDA(ctx, cudaMemcpyAsync(d_hist, hist, hbytes, cudaMemcpyHostToDevice, ctx->stream));
+  double *d_w;
+  if ((st = xns_upload_weights(ctx, nel, nq, source, ff, sl, &d_w))) return st;
+  if ((st = xns_scratch(ctx, SLOT_OUT, sizeof(double) * nq, &d_I))) return st;
+  if ((st = xns_timer_start(ctx))) return st;
+  if ((st = xns_hist_iq_device(ctx, (const unsigned long long *)d_hist, n_el, nel, nhist, bin, q, nq, d_w, polar, lambda,
+                               (double *)d_I)))
+    return st;
+  if ((st = xns_timer_stop(ctx))) return st;
+  XNS_CUDA(ctx, cudaMemcpyAsync(I, d_I, sizeof(double) * nq, cudaMemcpyDeviceToHost, ctx->stream));
+  XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return XNS_OK;
+}
+
+extern "C" int xns_pdf_and_debye_device(xns_ctx *ctx, const double *xyz_dev, const uint32_t *n_el, uint32_t nel,
+                                        uint32_t nhist, double bin, int scenario, int pdftype, double p0, const double *q,
+                                        uint32_t nq, int source, const double *const *ff, const double *sl, int polar,
+                                        double lambda, double *I_dev, double *pdf_dev, uint64_t *hist_dev) {
+  if (!ctx) return XNS_ERR_ARG;
+  if (scenario != XNS_DEBYE_HIST && scenario != XNS_PDF_ONLY && scenario != XNS_DEBYE_PDF)
+    return xns_fail(ctx, XNS_ERR_ARG, "scenario must be Debye_hist (2), PDFonly (3) or DebyePDF (4)");
+  const bool want_iq = scenario != XNS_PDF_ONLY, want_pdf = scenario != XNS_DEBYE_HIST;
+  if (!hist_dev || (want_iq && (!I_dev || !q || nq == 0)) || (want_pdf && (!pdf_dev || !sl)))
+    return xns_fail(ctx, XNS_ERR_ARG, "pdf_and_debye_device: missing output or weights for the scenario");
+  int st;
+  DevCoords dc;
+  if ((st = xns_coords_from_device(ctx, xyz_dev, n_el, nel, &dc))) return st;
+  if (dc.ntot == 0) return xns_fail(ctx, XNS_ERR_ARG, "pdf_and_debye_device: no atoms");
+  double *d_w = nullptr;
+  if (want_iq && (st = xns_upload_weights(ctx, nel, nq, source, ff, sl, &d_w))) return st;
+  if ((st = xns_timer_start(ctx))) return st;
+  if ((st = xns_hist_device(ctx, dc, nhist, bin, (unsigned long long *)hist_dev))) return st;
+  if (want_pdf &&
+      (st = xns_pdf_device(ctx, (const unsigned long long *)hist_dev, n_el, nel, nhist, bin, pdftype, p0, sl, pdf_dev)))
+    return st;
+  if (want_iq && (st = xns_hist_iq_device(ctx, (const unsigned long long *)hist_dev, n_el, nel, nhist, bin, q, nq, d_w,
+                                          polar, lambda, I_dev)))
+    return st;
+  return xns_timer_stop(ctx);
+}
+
+extern "C" int xns_calc_pdf_and_debye(xns_ctx *ctx, const double *const *xyz_el, const uint32_t *n_el, uint32_t nel,
+                                      uint32_t nhist, double bin, int scenario, int pdftype, double p0, const double *q,
+                                      uint32_t nq, int source, const double *const *ff, const double *sl, int polar,
+                                      double lambda, double *I, double *pdf, uint64_t *hist_out) {
+  if (!ctx) return XNS_ERR_ARG;
+  if (scenario != XNS_DEBYE_HIST && scenario != XNS_PDF_ONLY && scenario != XNS_DEBYE_PDF)
+    return xns_fail(ctx, XNS_ERR_ARG, "scenario must be Debye_hist (2), PDFonly (3) or DebyePDF (4)");
+  const bool want_iq = scenario != XNS_PDF_ONLY, want_pdf = scenario != XNS_DEBYE_HIST;
+  if ((want_iq && (!I || !q || nq == 0)) || (want_pdf && (!pdf || !sl)))
+    return xns_fail(ctx, XNS_ERR_ARG, "calc_pdf_and_debye: missing output or weights for the scenario");
+  int st;
+  DevCoords dc;
+  if ((st = xns_upload_coords(ctx, xyz_el, n_el, nel, &dc))) return st;
+  if (dc.ntot == 0) return xns_fail(ctx, XNS_ERR_ARG, "calc_pdf_and_debye: no atoms");
+  const uint32_t P = xns_npairs(nel);
+  const size_t hbytes = sizeof(uint64_t) * (size_t)P * nhist;
+  void *d_hist, *d_I = nullptr, *d_pdf = nullptr;
+  double *d_w = nullptr;
+  if ((st = xns_scratch(ctx, SLOT_HIST, hbytes, &d_hist))) return st;
+  if (want_iq) {
+    if ((st = xns_upload_weights(ctx, nel, nq, source, ff, sl, &d_w))) return st;
+    if ((st = xns_scratch(ctx, SLOT_OUT, sizeof(double) * nq, &d_I))) return st;
+  }
+  if (want_pdf && (st = xns_scratch(ctx, SLOT_OUT2, sizeof(double) * (size_t)(1 + P) * nhist, &d_pdf))) return st;
+  if ((st = xns_timer_start(ctx))) return st;
+  if ((st = xns_hist_device(ctx, dc, nhist, bin, (unsigned long long *)d_hist))) return st;
+  if (want_pdf &&
+      (st = xns_pdf_device(ctx, (const unsigned long long *)d_hist, n_el, nel, nhist, bin, pdftype, p0, sl, (double *)d_pdf)))
+    return st;
+  if (want_iq && (st = xns_hist_iq_device(ctx, (const unsigned long long *)d_hist, n_el, nel, nhist, bin, q, nq, d_w, polar,
+                                          lambda, (double *)d_I)))
+    return st;
+  if ((st = xns_timer_stop(ctx))) return st;
+  if (want_iq) XNS_CUDA(ctx, cudaMemcpyAsync(I, d_I, sizeof(double) * nq, cudaMemcpyDeviceToHost, ctx->stream));
+  if (want_pdf)
+    XNS_CUDA(ctx, cudaMemcpyAsync(pdf, d_pdf, sizeof(double) * (size_t)(1 + P) * nhist, cudaMemcpyDeviceToHost, ctx->stream));
+  if (hist_out) XNS_CUDA(ctx, cudaMemcpyAsync(hist_out, d_hist, hbytes, cudaMemcpyDeviceToHost, ctx->stream));
+  XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return XNS_OK;
+}

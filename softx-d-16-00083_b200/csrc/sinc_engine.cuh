@@ -1,0 +1,204 @@
+// Sum of weighted sinc terms on a q mesh, shared by the exact Debye double sum (weights 1 per atom
+// pair) and the histogram transform (weight n_k per distance bin):
+//
+//   S_c(q_k) = sum_{records in class c} w * sin(q_k r) / (q_k r)
+//
+// Records (r, w) arrive in tiles of up to SE_TILE produced cooperatively by a Source in shared
+// memory.  A lane owns a chunk of M consecutive q values, a slot of lanes walks the tile's records.
+// On a uniform mesh q_k = q0 + k dq the lane seeds s_{-1} = sin(q_{k0-1} r) w/r and
+// s_0 = sin(q_{k0} r) w/r (phase reduced mod 2pi in FP64, MUFU sine of the float remainder) and runs
+// the Chebyshev recurrence s_{k+1} = 2cos(dq r) s_k - s_{k-1}: one FFMA per term for the sine and
+// one FADD for the sum, no transcendental.  2cos(dq r) = 2 - 4 sin^2(dq r / 2) keeps its rounding
+// relative to the small quantity 1 - cos for small dq r.  Sums run in FP32 over one tile
+// (<= SE_TILE/slots records per lane) and are added to per-thread FP64 totals in shared memory after
+// every tile (compensated block accumulation); CTAs then reduce in FP64 in the epilogue.  1/q_k is
+// applied in the epilogue.  A mesh that is not uniform uses a direct sine per term (DIRECT).
+#pragma once
+#include <math.h>
+
+#include <algorithm>
+
+#include "xns_internal.cuh"
+
+namespace xns_sinc {
+
+constexpr int SE_THREADS = 256;
+constexpr int SE_TILE = 2048;
+constexpr double TWO_PI = 6.283185307179586476925286766559;
+constexpr double INV_TWO_PI = 0.15915494309189533576888376337251;
+
+struct PairRec {
+  double r;      // distance (FP64)
+  float w_r;     // weight / r; 0 for a record that does not count
+  float c2;      // 2 cos(dq r)
+  float theta;   // dq r
+  float pad;
+};
+
+__device__ __forceinline__ PairRec make_rec(double r, double w, double dq) {
+  PairRec rec;
+  rec.r = r;
+  rec.w_r = (float)(w / r);
+  float th = (float)(dq * r);
+  float h = sinf(0.5f * th);
+  rec.c2 = 2.f - 4.f * h * h;
+  rec.theta = th;
+  rec.pad = 0.f;
+  return rec;
+}
+
+__device__ __forceinline__ PairRec null_rec() { return PairRec{1.0, 0.f, 2.f, 0.f, 0.f}; }
+
+__device__ __forceinline__ float sin_reduced(double x) {
+  double n = rint(x * INV_TWO_PI);
+  return __sinf((float)__fma_rn(-n, TWO_PI, x));
+}
+
+struct SincParams {
+  double q0, dq;      // uniform mesh
+  const double *q;    // the mesh itself (DIRECT)
+  uint32_t nq;
+  uint32_t ncls;
+  unsigned long long ntiles;
+  double *partial;    // [gridDim.x][ncls][nq] FP64, zeroed
+};
+
+// Shared memory: [M][SE_THREADS] FP64 totals (one column per thread), then SE_TILE records, then the
+// Source's own staging area.
+template <int M, bool DIRECT, class Src>
+__global__ void __launch_bounds__(SE_THREADS, 2) sinc_tiles_kernel(SincParams p, Src src, int lanes_per_slot) {
+  extern __shared__ double acc64[];
+  PairRec *pr = reinterpret_cast<PairRec *>(acc64 + M * SE_THREADS);
+  void *stage = reinterpret_cast<void *>(pr + SE_TILE);
+
+  const int tid = threadIdx.x;
+  const int nslots = SE_THREADS / lanes_per_slot;
+  const int slot = tid / lanes_per_slot;
+  const uint32_t k0 = (uint32_t)(tid % lanes_per_slot) * M;
+  const bool active = k0 < p.nq;
+  const double qk0 = p.q0 + (double)k0 * p.dq;
+#pragma unroll
+  for (int k = 0; k < M; k++) acc64[k * SE_THREADS + tid] = 0.0;
+  double qd[DIRECT ? M : 1];
+  if (DIRECT) {
+#pragma unroll
+    for (int k = 0; k < (DIRECT ? M : 1); k++) qd[k] = (k0 + k < p.nq) ? p.q[k0 + k] : 0.0;
+  }
+
+  int cur = -1;
+  for (unsigned long long w = blockIdx.x; w < p.ntiles; w += gridDim.x) {
+    const int c = (int)src.cls(w);
+    if (c != cur) {  // flush the previous class's FP64 totals to this CTA's slice
+      if (cur >= 0 && active) {
+        double *dst = p.partial + ((size_t)blockIdx.x * p.ncls + cur) * p.nq + k0;
+#pragma unroll
+        for (int k = 0; k < M; k++) {
+          if (k0 + k < p.nq) atomicAdd(dst + k, acc64[k * SE_THREADS + tid]);
+          acc64[k * SE_THREADS + tid] = 0.0;
+        }
+      }
+      cur = c;
+    }
+    const int n = src.fill(w, pr, stage, p.dq);  // ends with __syncthreads()
+    if (active) {
+      float blk[M];
+#pragma unroll
+      for (int k = 0; k < M; k++) blk[k] = 0.f;
+      for (int e = slot; e < n; e += 2 * nslots) {
+        const PairRec A = pr[e];
+        const int e2 = e + nslots;
+        const PairRec B = e2 < n ? pr[e2] : null_rec();
+        if (A.w_r == 0.f && B.w_r == 0.f) continue;
+        if (DIRECT) {
+#pragma unroll
+          for (int k = 0; k < M; k++) blk[k] += sin_reduced(qd[k] * A.r) * A.w_r + sin_reduced(qd[k] * B.r) * B.w_r;
+        } else {
+          double xa = qk0 * A.r, xb = qk0 * B.r;
+          double na = rint(xa * INV_TWO_PI), nb = rint(xb * INV_TWO_PI);
+          float ra = (float)__fma_rn(-na, TWO_PI, xa), rb = (float)__fma_rn(-nb, TWO_PI, xb);
+          float a0 = __sinf(ra) * A.w_r, am = __sinf(ra - A.theta) * A.w_r;
+          float b0 = __sinf(rb) * B.w_r, bm = __sinf(rb - B.theta) * B.w_r;
+          const float ca = A.c2, cb = B.c2;
+          blk[0] += a0 + b0;
+#pragma unroll
+          for (int k = 1; k < M; k++) {
+            float an = fmaf(ca, a0, -am);
+            float bn = fmaf(cb, b0, -bm);
+            blk[k] += an + bn;
+            am = a0;
+            a0 = an;
+            bm = b0;
+            b0 = bn;
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < M; k++) acc64[k * SE_THREADS + tid] += (double)blk[k];
+    }
+    __syncthreads();
+  }
+  if (cur >= 0 && active) {
+    double *dst = p.partial + ((size_t)blockIdx.x * p.ncls + cur) * p.nq + k0;
+#pragma unroll
+    for (int k = 0; k < M; k++)
+      if (k0 + k < p.nq) atomicAdd(dst + k, acc64[k * SE_THREADS + tid]);
+  }
+}
+
+// Reduction of the per-CTA FP64 partial sums plus the calc-function epilogue: 1/q, weights, self
+// term, 1/Ntot, polarisation factor and the sum over parts (CalcFunctions.cpp:592-625 and 733-755 for
+// the Debye sums, :872-906 for the histogram transform).  Classes are part * P + t.
+// out: [total | parts] when nparts > 1, else [total].
+__global__ void sinc_epilogue_kernel(const double *__restrict__ partial, int grid, uint32_t ncls, uint32_t nel,
+                                     uint32_t nparts, uint32_t nblocks, const uint32_t *__restrict__ pair_a,
+                                     const uint32_t *__restrict__ pair_b, const double *__restrict__ w,
+                                     const uint32_t *__restrict__ n_el_block, double q0, double dq,
+                                     const double *__restrict__ qmesh, uint32_t nq, uint32_t ntot, int polar, double lambda,
+                                     double *__restrict__ out);
+
+// Launches sinc_tiles_kernel with the persistent grid and zeroed partial sums; returns the status
+// and the grid size used.
+template <int M, bool DIRECT, class Src>
+int launch_sinc(xns_ctx *ctx, const SincParams &p, const Src &src, int lanes, size_t stage_bytes, int *grid_out) {
+  const size_t smem = sizeof(double) * M * SE_THREADS + sizeof(PairRec) * SE_TILE + stage_bytes;
+  auto kern = sinc_tiles_kernel<M, DIRECT, Src>;
+  XNS_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  XNS_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, SE_THREADS, smem));
+  unsigned long long grid = std::min<unsigned long long>(p.ntiles, (unsigned long long)ctx->num_sms * std::max(per_sm, 1));
+  if (grid == 0) grid = 1;
+  SincParams pp = p;
+  void *d;
+  int st;
+  size_t bytes = sizeof(double) * grid * p.ncls * p.nq;
+  if ((st = xns_scratch(ctx, SLOT_PARTIAL, bytes, &d))) return st;
+  XNS_CUDA(ctx, cudaMemsetAsync(d, 0, bytes, ctx->stream));
+  pp.partial = (double *)d;
+  if (p.ntiles) {
+    kern<<<(unsigned)grid, SE_THREADS, smem, ctx->stream>>>(pp, src, lanes);
+    XNS_LAUNCHED(ctx);
+  }
+  *grid_out = (int)grid;
+  return XNS_OK;
+}
+
+// Chooses M and the lanes per slot for nq and launches; DIRECT when the mesh is not uniform.
+template <class Src>
+int run_sinc(xns_ctx *ctx, SincParams p, const Src &src, size_t stage_bytes, bool uniform, int *grid_out) {
+  const int M = uniform ? 32 : 16;
+  const uint32_t chunks = (p.nq + M - 1) / M;
+  int lanes = 1;
+  while (lanes < (int)chunks) lanes <<= 1;
+  if (lanes > SE_THREADS) return xns_fail(ctx, XNS_ERR_ARG, "too many q points for one call");
+  if (uniform) return launch_sinc<32, false>(ctx, p, src, lanes, stage_bytes, grid_out);
+  return launch_sinc<16, true>(ctx, p, src, lanes, stage_bytes, grid_out);
+}
+
+// Uploads pair_a, pair_b, n_el_block and the q mesh for the epilogue and runs it.
+int sinc_epilogue(xns_ctx *ctx, int grid, uint32_t ncls, uint32_t nel, uint32_t nblocks, const uint32_t *n_el_block,
+                  const double *q, uint32_t nq, bool uniform, double q0, double dq, const double *d_w, uint32_t ntot,
+                  int polar, double lambda, double *d_out);
+// The q mesh as a device array (valid until the next call on the context).
+int sinc_upload_q(xns_ctx *ctx, const double *q, uint32_t nq, const double **d_q);
+
+}  // namespace xns_sinc

@@ -1,0 +1,145 @@
+// Drop-in replacement of the reference's four CPU calc functions (the signatures main.cpp:344-347
+// declares and CalcFunctions.cpp:547-1091 defines) on top of the xns_b200 CUDA library.
+//
+// Link the reference program with this file instead of its CPU calc functions: main.cpp, ReadXML.cpp,
+// IO.cpp and tinyxml2.cpp unchanged, CalcFunctions.cpp compiled with -D UseCUDA (which removes exactly
+// the four functions below, CalcFunctions.cpp:546-1092), plus this object and libxns_b200.so.  The
+// XML inputs, the stdout timing lines and the output files stay those of the reference.
+//
+// Contract kept from the reference: outputs are allocated here with new[] and freed by main
+// (main.cpp:518-524); inputs are borrowed; cfg->Nhist and cfg->p0 are set by the caller
+// (CalcFunctions.cpp:403-408); NumOMPthreads is ignored.  On a library error the function prints the
+// message and exits with -1 instead of returning a partial result.  The device is the one named by
+// the XNS_DEVICE environment variable (default 0).
+#include <chrono>
+#include <cstdlib>
+#include <cstring>
+
+#include "typedefs.h"
+#include "xns_b200.h"
+
+namespace {
+
+xns_ctx *context() {
+  static xns_ctx *ctx = nullptr;
+  if (!ctx) {
+    const char *dev = getenv("XNS_DEVICE");
+    int st = xns_create(dev ? atoi(dev) : 0, &ctx);
+    if (st) {
+      cout << "Error: " << xns_status_string(st) << ": " << xns_last_error(ctx) << endl;
+      exit(-1);
+    }
+  }
+  return ctx;
+}
+
+void check(int st) {
+  if (st) {
+    cout << "Error: " << xns_status_string(st) << ": " << xns_last_error(context()) << endl;
+    exit(-1);
+  }
+}
+
+// per-element coordinate pointers: vect3d<double> is three packed doubles
+vector<const double *> coords(const vector<vect3d<double> > *ra, unsigned int nel) {
+  static_assert(sizeof(vect3d<double>) == 3 * sizeof(double), "vect3d<double> must be three packed doubles");
+  vector<const double *> p(nel, nullptr);
+  for (unsigned int e = 0; e < nel; e++)
+    if (ra[e].size()) p[e] = &ra[e][0].x;
+  return p;
+}
+
+vector<const double *> ff_rows(const config *cfg, const vector<double *> &FF) {
+  vector<const double *> p;
+  if (cfg->source == xray)
+    for (unsigned int e = 0; e < FF.size(); e++) p.push_back(FF[e]);
+  return p;
+}
+
+float seconds_since(chrono::steady_clock::time_point t1) {
+  return chrono::duration_cast<chrono::duration<float> >(chrono::steady_clock::now() - t1).count();
+}
+
+}  // namespace
+
+// calcIntDebye, CalcFunctions.cpp:547
+void calcIntDebye(double **I, const config *cfg, const unsigned int *NatomEl, const vector<vect3d<double> > *ra,
+                  vector<double *> FF, vector<double> SL, const double *q, unsigned int Ntot, int NumOMPthreads) {
+  (void)Ntot;
+  (void)NumOMPthreads;
+  chrono::steady_clock::time_point t1 = chrono::steady_clock::now();
+  vector<const double *> xyz = coords(ra, cfg->Nel), ff = ff_rows(cfg, FF);
+  *I = new double[cfg->q.N];
+  check(xns_calc_int_debye(context(), xyz.data(), NatomEl, cfg->Nel, q, cfg->q.N, cfg->source, ff.empty() ? nullptr : ff.data(),
+                           SL.empty() ? nullptr : SL.data(), cfg->PolarFactor, cfg->lambda, *I));
+  cout << "1D pattern calculation time: " << seconds_since(t1) << " s" << endl;
+}
+
+// calcIntPartialDebye, CalcFunctions.cpp:634
+void calcIntPartialDebye(double **I, const config *cfg, const unsigned int *NatomEl, const vector<vect3d<double> > *ra,
+                         vector<double *> FF, vector<double> SL, const double *q, const block *Block, unsigned int Ntot,
+                         int NumOMPthreads) {
+  (void)Ntot;
+  (void)NumOMPthreads;
+  chrono::steady_clock::time_point t1 = chrono::steady_clock::now();
+  vector<const double *> xyz = coords(ra, cfg->Nel), ff = ff_rows(cfg, FF);
+  // atoms of element e in block b, as CalcFunctions.cpp:648-659 derives them
+  vector<uint32_t> neb((size_t)cfg->Nel * cfg->Nblocks, 0);
+  for (unsigned int e = 0; e < cfg->Nel; e++)
+    for (unsigned int b = 0; b < cfg->Nblocks; b++)
+      for (unsigned int k = 0; k < Block[b].Nid; k++)
+        if (Block[b].id[k] == e) {
+          neb[(size_t)e * cfg->Nblocks + b] = Block[b].NatomElAll[k];
+          break;
+        }
+  const unsigned int nparts = cfg->Nblocks * (cfg->Nblocks + 1) / 2;
+  *I = new double[(size_t)(nparts + 1) * cfg->q.N];
+  check(xns_calc_int_partial_debye(context(), xyz.data(), NatomEl, cfg->Nel, cfg->Nblocks, neb.data(), q, cfg->q.N,
+                                   cfg->source, ff.empty() ? nullptr : ff.data(), SL.empty() ? nullptr : SL.data(),
+                                   cfg->PolarFactor, cfg->lambda, *I));
+  cout << "1D pattern calculation time: " << seconds_since(t1) << " s" << endl;
+}
+
+// calcPDFandDebye, CalcFunctions.cpp:912
+void calcPDFandDebye(double **I, double **PDF, const config *cfg, const unsigned int *NatomEl,
+                     const vector<vect3d<double> > *ra, vector<double *> FF, vector<double> SL, const double *q,
+                     unsigned int Ntot, int NumOMPthreads) {
+  (void)Ntot;
+  (void)NumOMPthreads;
+  chrono::steady_clock::time_point t1 = chrono::steady_clock::now();
+  vector<const double *> xyz = coords(ra, cfg->Nel), ff = ff_rows(cfg, FF);
+  const unsigned int P = cfg->Nel * (cfg->Nel + 1) / 2;
+  const bool want_pdf = cfg->scenario > Debye_hist;
+  const bool want_iq = cfg->scenario == Debye_hist || cfg->scenario == DebyePDF;
+  if (want_pdf) *PDF = new double[(size_t)(1 + P) * cfg->Nhist];
+  if (want_iq) *I = new double[cfg->q.N];
+  check(xns_calc_pdf_and_debye(context(), xyz.data(), NatomEl, cfg->Nel, cfg->Nhist, cfg->hist_bin, cfg->scenario,
+                               cfg->PDFtype, cfg->p0, want_iq ? q : nullptr, want_iq ? cfg->q.N : 0, cfg->source,
+                               ff.empty() ? nullptr : ff.data(), SL.empty() ? nullptr : SL.data(), cfg->PolarFactor,
+                               cfg->lambda, want_iq ? *I : nullptr, want_pdf ? *PDF : nullptr, nullptr));
+  cout << "Histogram, PDF and 1D pattern calculation time: " << seconds_since(t1) << " s" << endl;
+}
+
+// calcInt2D, CalcFunctions.cpp:969
+void calcInt2D(double ***I2D, double **I, const config *cfg, const unsigned int *NatomEl, const vector<vect3d<double> > *ra,
+               vector<double *> FF, vector<double> SL, const double *q, unsigned int Ntot, int NumOMPthreads) {
+  (void)Ntot;
+  (void)NumOMPthreads;
+  chrono::steady_clock::time_point t1 = chrono::steady_clock::now();
+  vector<const double *> xyz = coords(ra, cfg->Nel), ff = ff_rows(cfg, FF);
+  const unsigned int nq = cfg->q.N, nfi = cfg->Nfi;
+  vector<double> flat((size_t)nq * nfi);
+  *I = new double[nq];
+  const double emin[3] = {cfg->Euler.min.x, cfg->Euler.min.y, cfg->Euler.min.z};
+  const double emax[3] = {cfg->Euler.max.x, cfg->Euler.max.y, cfg->Euler.max.z};
+  const uint32_t en[3] = {cfg->Euler.N.x, cfg->Euler.N.y, cfg->Euler.N.z};
+  check(xns_calc_int_2d(context(), xyz.data(), NatomEl, cfg->Nel, q, nq, nfi, emin, emax, en, cfg->EulerConvention,
+                        cfg->lambda, cfg->source, ff.empty() ? nullptr : ff.data(), SL.empty() ? nullptr : SL.data(),
+                        cfg->PolarFactor, flat.data(), *I));
+  *I2D = new double *[nq];
+  for (unsigned int iq = 0; iq < nq; iq++) {
+    (*I2D)[iq] = new double[nfi];
+    memcpy((*I2D)[iq], flat.data() + (size_t)iq * nfi, sizeof(double) * nfi);
+  }
+  cout << "2D pattern calculation time: " << seconds_since(t1) << " s" << endl;
+}

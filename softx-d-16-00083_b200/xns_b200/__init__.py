@@ -1,0 +1,212 @@
+"""Python binding of the xns_b200 C ABI (include/xns_b200.h) over ctypes.
+
+The library is the in-tree build softx-d-16-00083_b200/lib/libxns_b200.so; importing this package
+fails loudly if it is missing, and every call raises XnsError on a non-zero status.  There is no CPU
+code path here: each function calls the CUDA library.
+
+Arrays follow the reference's layout (see the header): coordinates per element as (n_e, 3) float64
+arrays, element pairs a <= b in loop order, histograms element-pair major.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(_PKG, "lib", "libxns_b200.so")
+
+NEUTRON, XRAY = 0, 1
+RDF, PDF, RPDF = 0, 1, 2
+DEBYE_HIST, PDF_ONLY, DEBYE_PDF = 2, 3, 4
+
+
+class XnsError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("xns status %d: %s" % (status, msg))
+        self.status = status
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("xns_b200: %s is not built (run softx-d-16-00083_b200/build.py)" % LIB_PATH)
+    return C.CDLL(LIB_PATH)
+
+
+lib = _load()
+_p = C.c_void_p
+_u32 = C.c_uint32
+_dbl = C.c_double
+_int = C.c_int
+_PP = C.POINTER(C.c_void_p)
+
+lib.xns_create.argtypes = [_int, C.POINTER(_p)]
+lib.xns_destroy.argtypes = [_p]
+lib.xns_destroy.restype = None
+lib.xns_last_error.argtypes = [_p]
+lib.xns_last_error.restype = C.c_char_p
+lib.xns_status_string.argtypes = [_int]
+lib.xns_status_string.restype = C.c_char_p
+lib.xns_set_stream.argtypes = [_p, _p]
+lib.xns_last_kernel_ms.argtypes = [_p]
+lib.xns_last_kernel_ms.restype = _dbl
+lib.xns_kernel_launches.argtypes = [_p]
+lib.xns_kernel_launches.restype = C.c_uint64
+lib.xns_calc_hist.argtypes = [_p, _PP, _p, _u32, _u32, _dbl, _p]
+lib.xns_calc_int_1d_hist.argtypes = [_p, _p, _p, _u32, _u32, _dbl, _p, _u32, _int, _PP, _p, _int, _dbl, _p]
+lib.xns_calc_pdf.argtypes = [_p, _p, _p, _u32, _u32, _dbl, _int, _dbl, _p, _p]
+lib.xns_calc_pdf_and_debye.argtypes = [_p, _PP, _p, _u32, _u32, _dbl, _int, _int, _dbl, _p, _u32, _int, _PP, _p, _int,
+                                       _dbl, _p, _p, _p]
+lib.xns_calc_int_debye.argtypes = [_p, _PP, _p, _u32, _p, _u32, _int, _PP, _p, _int, _dbl, _p]
+lib.xns_calc_int_partial_debye.argtypes = [_p, _PP, _p, _u32, _u32, _p, _p, _u32, _int, _PP, _p, _int, _dbl, _p]
+lib.xns_calc_int_2d.argtypes = [_p, _PP, _p, _u32, _p, _u32, _u32, _p, _p, _p, _u32, _dbl, _int, _PP, _p, _int, _p, _p]
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_p)
+
+
+class _Elements:
+    """Keeps per-element contiguous float64 (n, 3) arrays alive and exposes the pointer table."""
+
+    def __init__(self, els):
+        self.arrays = [np.ascontiguousarray(e, dtype=np.float64).reshape(-1, 3) for e in els]
+        self.n_el = np.array([len(a) for a in self.arrays], dtype=np.uint32)
+        self.table = (C.c_void_p * len(self.arrays))(*[a.ctypes.data for a in self.arrays])
+        self.nel = len(self.arrays)
+        self.ntot = int(self.n_el.sum())
+
+
+def _rows(rows, nq):
+    """Per-element rows (X-ray form factors) -> pointer table; None stays None."""
+    if rows is None:
+        return None, None
+    arrs = [np.ascontiguousarray(r, dtype=np.float64).reshape(nq) for r in rows]
+    return arrs, (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+
+
+def _f64(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Context:
+    """One CUDA device.  Mirrors the reference's calc functions (CalcFunctions.cpp:546-1092)."""
+
+    def __init__(self, device=-1):
+        self._h = _p()
+        st = lib.xns_create(device, C.byref(self._h))
+        if st:
+            msg = lib.xns_last_error(self._h).decode()
+            lib.xns_destroy(self._h)
+            self._h = None
+            raise XnsError(st, msg)
+
+    def close(self):
+        if self._h:
+            lib.xns_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st:
+            raise XnsError(st, lib.xns_last_error(self._h).decode())
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def last_kernel_ms(self):
+        return lib.xns_last_kernel_ms(self._h)
+
+    @property
+    def kernel_launches(self):
+        return int(lib.xns_kernel_launches(self._h))
+
+    def set_stream(self, stream_ptr):
+        self._check(lib.xns_set_stream(self._h, stream_ptr))
+
+    # -- calc functions --------------------------------------------------------------------------
+    def calc_hist(self, elements, nhist, bin):
+        el = _Elements(elements)
+        out = np.zeros(el.nel * (el.nel + 1) // 2 * nhist, dtype=np.uint64)
+        self._check(lib.xns_calc_hist(self._h, el.table, _ptr(el.n_el), el.nel, nhist, bin, _ptr(out)))
+        return out
+
+    def calc_int_1d_hist(self, hist, n_el, nhist, bin, q, source, ff=None, sl=None, polar=False, lam=0.0):
+        hist = np.ascontiguousarray(hist, dtype=np.uint64)
+        n_el = np.ascontiguousarray(n_el, dtype=np.uint32)
+        q = _f64(q)
+        ffa, fft = _rows(ff, len(q))
+        sl = _f64(sl)
+        out = np.zeros(len(q))
+        self._check(lib.xns_calc_int_1d_hist(self._h, _ptr(hist), _ptr(n_el), len(n_el), nhist, bin, _ptr(q), len(q),
+                                             source, fft, _ptr(sl), int(polar), lam, _ptr(out)))
+        return out
+
+    def calc_pdf(self, hist, n_el, nhist, bin, pdftype, p0, sl):
+        hist = np.ascontiguousarray(hist, dtype=np.uint64)
+        n_el = np.ascontiguousarray(n_el, dtype=np.uint32)
+        sl = _f64(sl)
+        P = len(n_el) * (len(n_el) + 1) // 2
+        out = np.zeros((1 + P) * nhist)
+        self._check(lib.xns_calc_pdf(self._h, _ptr(hist), _ptr(n_el), len(n_el), nhist, bin, pdftype, p0, _ptr(sl),
+                                     _ptr(out)))
+        return out
+
+    def calc_pdf_and_debye(self, elements, nhist, bin, scenario, pdftype, p0, q, source, ff=None, sl=None, polar=False,
+                           lam=0.0, want_hist=False):
+        el = _Elements(elements)
+        P = el.nel * (el.nel + 1) // 2
+        q = _f64(q) if q is not None else np.zeros(1)
+        ffa, fft = _rows(ff, len(q))
+        sl = _f64(sl)
+        I = np.zeros(len(q)) if scenario != PDF_ONLY else None
+        pdf = np.zeros((1 + P) * nhist) if scenario != DEBYE_HIST else None
+        h = np.zeros(P * nhist, dtype=np.uint64) if want_hist else None
+        self._check(lib.xns_calc_pdf_and_debye(self._h, el.table, _ptr(el.n_el), el.nel, nhist, bin, scenario, pdftype,
+                                               p0, _ptr(q), len(q), source, fft, _ptr(sl), int(polar), lam, _ptr(I),
+                                               _ptr(pdf), _ptr(h)))
+        return I, pdf, h
+
+    def calc_int_debye(self, elements, q, source, ff=None, sl=None, polar=False, lam=0.0):
+        el = _Elements(elements)
+        q = _f64(q)
+        ffa, fft = _rows(ff, len(q))
+        sl = _f64(sl)
+        out = np.zeros(len(q))
+        self._check(lib.xns_calc_int_debye(self._h, el.table, _ptr(el.n_el), el.nel, _ptr(q), len(q), source, fft,
+                                           _ptr(sl), int(polar), lam, _ptr(out)))
+        return out
+
+    def calc_int_partial_debye(self, elements, n_el_block, q, source, ff=None, sl=None, polar=False, lam=0.0):
+        el = _Elements(elements)
+        neb = np.ascontiguousarray(n_el_block, dtype=np.uint32)  # (nel, nblocks)
+        nblocks = neb.shape[1]
+        q = _f64(q)
+        ffa, fft = _rows(ff, len(q))
+        sl = _f64(sl)
+        nparts = nblocks * (nblocks + 1) // 2
+        out = np.zeros(((1 + nparts) if nblocks > 1 else 1) * len(q))
+        self._check(lib.xns_calc_int_partial_debye(self._h, el.table, _ptr(el.n_el), el.nel, nblocks, _ptr(neb), _ptr(q),
+                                                   len(q), source, fft, _ptr(sl), int(polar), lam, _ptr(out)))
+        return out
+
+    def calc_int_2d(self, elements, q, nfi, euler_min, euler_max, euler_n, convention, lam, source, ff=None, sl=None,
+                    polar=False):
+        el = _Elements(elements)
+        q = _f64(q)
+        ffa, fft = _rows(ff, len(q))
+        sl = _f64(sl)
+        emin, emax = _f64(euler_min), _f64(euler_max)
+        en = np.ascontiguousarray(euler_n, dtype=np.uint32)
+        I2D = np.zeros((len(q), nfi))
+        I = np.zeros(len(q))
+        self._check(lib.xns_calc_int_2d(self._h, el.table, _ptr(el.n_el), el.nel, _ptr(q), len(q), nfi, _ptr(emin),
+                                        _ptr(emax), _ptr(en), convention, lam, source, fft, _ptr(sl), int(polar),
+                                        _ptr(I2D), _ptr(I)))
+        return I2D, I
