@@ -41,7 +41,8 @@ struct AtomPairSrc {
     xns_decode_tile(sp, nsp, w, &s, &I, &J);
     const SegPair g = sp[s];
     const uint32_t ib = I * DB_TI, jb = J * DB_TJ;
-    const uint32_t ni = min((uint32_t)DB_TI, g.na - ib), nj = min((uint32_t)DB_TJ, g.nb - jb);
+    // a "same" entry may name an a-tile past the segment's end (see schedule.cuh): it is empty
+    const uint32_t ni = ib < g.na ? min((uint32_t)DB_TI, g.na - ib) : 0u, nj = min((uint32_t)DB_TJ, g.nb - jb);
     const int tid = threadIdx.x;
     if (tid < (int)ni) {
       sxi[tid] = X[g.a0 + ib + tid];

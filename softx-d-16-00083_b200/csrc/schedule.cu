@@ -16,7 +16,9 @@ unsigned long long xns_build_schedule(const std::vector<Segment> &sa, const std:
     p.same = same[k];
     p.ta = (p.na + tile_a - 1) / tile_a;
     p.tb = (p.nb + tile_b - 1) / tile_b;
-    unsigned long long n = p.same ? (unsigned long long)p.ta * (p.ta + 1) / 2 : (unsigned long long)p.ta * p.tb;
+    p.ratio = tile_b / tile_a;
+    p.pad = 0;
+    unsigned long long n = p.same ? (unsigned long long)p.tb * (p.tb + 1) / 2 * p.ratio : (unsigned long long)p.ta * p.tb;
     if (p.same && p.na < 2) continue;
     p.tile_begin = total;
     total += n;

@@ -3,8 +3,11 @@
 #include "xns_internal.cuh"
 
 // Segment pairs are flattened into one index space of tile pairs: entry s owns tile pairs
-// [tile_begin, tile_begin + count).  A "same" entry enumerates the upper triangle I <= J of its
-// tiles (pairs i < j of one segment), any other entry the full TA x TB rectangle.
+// [tile_begin, tile_begin + count).  Tiles along a hold tile_a atoms, along b tile_b atoms, with
+// tile_b a multiple of tile_a.  A "same" entry (pairs i < j of one segment) enumerates the upper
+// triangle Ib <= J of tile_b-sized blocks, each split into tile_b/tile_a a-tiles, so the a-tile index
+// I = Ib * ratio + sub may point past the segment's end (an empty tile); any other entry enumerates the
+// full TA x TB rectangle.
 struct Segment {
   uint32_t start, count;
 };
@@ -30,12 +33,15 @@ __device__ __forceinline__ void xns_decode_tile(const SegPair *__restrict__ sp, 
   *s_out = lo;
   unsigned long long l = w - sp[lo].tile_begin;
   if (sp[lo].same) {
-    // l -> (I <= J): J = floor((sqrt(8l+1)-1)/2), I = l - J(J+1)/2
+    const uint32_t ratio = sp[lo].ratio;
+    const uint32_t sub = (uint32_t)(l % ratio);
+    l /= ratio;
+    // l -> (Ib <= J): J = floor((sqrt(8l+1)-1)/2), Ib = l - J(J+1)/2
     unsigned long long j = (unsigned long long)((sqrt(8.0 * (double)l + 1.0) - 1.0) * 0.5);
     while (j * (j + 1) / 2 > l) j--;
     while ((j + 1) * (j + 2) / 2 <= l) j++;
     *J = (uint32_t)j;
-    *I = (uint32_t)(l - j * (j + 1) / 2);
+    *I = (uint32_t)(l - j * (j + 1) / 2) * ratio + sub;
   } else {
     *I = (uint32_t)(l / sp[lo].tb);
     *J = (uint32_t)(l % sp[lo].tb);

@@ -53,6 +53,8 @@ struct SegPair {
   uint32_t cls;    // output class (element pair t for histograms; accumulator row for Debye)
   uint32_t same;
   uint32_t ta, tb; // tiles along a and b
+  uint32_t ratio;  // a-tiles per b-tile (tile_b / tile_a)
+  uint32_t pad;
   unsigned long long tile_begin;  // prefix over the schedule
 };
 
