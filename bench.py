@@ -62,9 +62,9 @@ def npairs(els):
     return n * (n - 1) // 2
 
 
-def config_block(els, nh, extra=None):
+def config_block(els, nh, extra=None, cells=CELLS):
     c = {"workload": "DebyePDF rock-salt nanocube %d^3 cells a=%.2f A, %d atoms, hist bin %.3f A (%d bins x 3 pairs), "
-                     "rPDF, I(q) %d q in [%.1f,%.1f)" % (CELLS, A, sum(len(e) for e in els), BIN, nh, NQ, QMIN, QMAX),
+                     "rPDF, I(q) %d q in [%.1f,%.1f)" % (cells, A, sum(len(e) for e in els), BIN, nh, NQ, QMIN, QMAX),
          "atoms": int(sum(len(e) for e in els)), "pairs_per_step": int(npairs(els)), "nhist": int(nh), "nq": NQ,
          "l2": "flushed (512 MB write) before every timed step"}
     if extra:
@@ -202,7 +202,7 @@ def ours(args, rank, world, local_rank):
     stream = torch.cuda.current_stream(dev)
     ctx.set_stream(stream.cuda_stream)
 
-    els, nh, q, p0 = workload(rank)
+    els, nh, q, p0 = workload(rank, args.cells)
     n_el = np.array([len(e) for e in els], dtype=np.uint32)
     P = 3
     pairs = npairs(els)
@@ -317,7 +317,7 @@ def ours(args, rank, world, local_rank):
                                                                 "reductions (I(q))",
             "data": "synthetic (seeded)",
             "patterns_per_s": world / (ms_step * 1e-3),
-            "config": config_block(els, nh, {"parallelism": "replicas x%d (one structure per rank)" % world}),
+            "config": config_block(els, nh, {"parallelism": "replicas x%d (one structure per rank)" % world}, args.cells),
             "stages_ms": {"histogram": hist_avg, "pdf": pdf_ms / args.steps, "iq": iq_ms / args.steps},
             "roofline": {"kernel": "hist_tiles_kernel", "bound": "fp64", "achieved": achieved, "peak": peak.value,
                          "unit": "TFLOP/s", "frac": achieved / peak.value if peak.value else None, "traffic": None,
@@ -341,6 +341,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cells", type=int, default=CELLS,
+                    help="cube edge in unit cells (default 30, the benchmark; smaller only for profiler captures)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

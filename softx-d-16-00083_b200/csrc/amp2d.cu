@@ -7,23 +7,23 @@
 // then I2D *= 1/(Ntot N_orient), the polarisation factor, and I(q) = mean over phi (:1066-1076).
 //
 // One thread per mesh point; atoms are staged through shared memory in tiles shared by the CTA.
-// The phase (R^T qv).r is formed and reduced mod 2pi in FP64 (it reaches ~10^3 rad for 10^6-atom
-// crystallites, where an FP32 phase would carry ~1e-4 rad of error); the sine and cosine of the
-// reduced phase come from the MUFU unit.  Tile sums run in FP32 (<= 256 terms) and are added to
-// FP64 amplitude totals (compensated block accumulation).
+// The phase (R^T qv).r is formed and reduced in FP64 (it reaches ~10^3 rad for 10^6-atom
+// crystallites, where an FP32 phase would carry ~1e-4 rad of error) and its sine and cosine come from
+// the accurate polynomial of xmath.cuh (on a lattice the MUFU approximation's error adds coherently).
+// Tile sums run in FP32 (<= 256 terms) and are added to FP64 amplitude totals (compensated block
+// accumulation).
 #include <math.h>
 #include <string.h>
 
 #include <algorithm>
 
+#include "xmath.cuh"
 #include "xns_internal.cuh"
 
 namespace {
 
 constexpr int A2_THREADS = 256;
 constexpr int A2_TILE = 256;
-constexpr double TWO_PI = 6.283185307179586476925286766559;
-constexpr double INV_TWO_PI = 0.15915494309189533576888376337251;
 
 __global__ void __launch_bounds__(A2_THREADS) amp2d_polar_kernel(
     const double *__restrict__ X, const double *__restrict__ Y, const double *__restrict__ Z,
@@ -60,10 +60,8 @@ __global__ void __launch_bounds__(A2_THREADS) amp2d_polar_kernel(
         if (valid) {
           float tr = 0.f, ti = 0.f;
           for (uint32_t j = 0; j < n; j++) {
-            const double ph = __fma_rn(w2, sz[j], __fma_rn(w1, sy[j], w0 * sx[j]));
-            const double k = rint(ph * INV_TWO_PI);
             float s, c;
-            __sincosf((float)__fma_rn(-k, TWO_PI, ph), &s, &c);
+            xns_math::xns_sincos(__fma_rn(w2, sz[j], __fma_rn(w1, sy[j], w0 * sx[j])), &s, &c);
             tr += c;
             ti += s;
           }

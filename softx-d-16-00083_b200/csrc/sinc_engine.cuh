@@ -5,33 +5,33 @@
 //
 // Records (r, w) arrive in tiles of up to SE_TILE produced cooperatively by a Source in shared
 // memory.  A lane owns a chunk of M consecutive q values, a slot of lanes walks the tile's records.
-// On a uniform mesh q_k = q0 + k dq the lane seeds s_{-1} = sin(q_{k0-1} r) w/r and
-// s_0 = sin(q_{k0} r) w/r (phase reduced mod 2pi in FP64, MUFU sine of the float remainder) and runs
-// the Chebyshev recurrence s_{k+1} = 2cos(dq r) s_k - s_{k-1}: one FFMA per term for the sine and
-// one FADD for the sum, no transcendental.  2cos(dq r) = 2 - 4 sin^2(dq r / 2) keeps its rounding
-// relative to the small quantity 1 - cos for small dq r.  Sums run in FP32 over one tile
-// (<= SE_TILE/slots records per lane) and are added to per-thread FP64 totals in shared memory after
-// every tile (compensated block accumulation); CTAs then reduce in FP64 in the epilogue.  1/q_k is
-// applied in the epilogue.  A mesh that is not uniform uses a direct sine per term (DIRECT).
+// On a uniform mesh q_k = q0 + k dq the lane seeds s_0 = sin(q_{k0} r) w/r and
+// s_{-1} = sin(q_{k0} r - dq r) w/r from an accurate sine and cosine of the FP64 phase (xmath.cuh;
+// the MUFU approximations would add coherently over the distance shells of a crystal) and runs the
+// Chebyshev recurrence s_{k+1} = 2cos(dq r) s_k - s_{k-1}: one FFMA per term for the sine and one
+// FADD for the sum, no transcendental.  The rounding of 2cos(dq r) makes the phase drift by at most
+// M * 2^-23 / (2 sin(dq r)) over a chunk, pseudo-random from pair to pair.  Sums run in FP32 over one
+// tile (<= SE_TILE/slots records per lane) and are added to per-thread FP64 totals in shared memory
+// after every tile (compensated block accumulation); CTAs then reduce in FP64 in the epilogue.  1/q_k
+// is applied in the epilogue.  A mesh that is not uniform takes an accurate sine per term (DIRECT).
 #pragma once
 #include <math.h>
 
 #include <algorithm>
 
+#include "xmath.cuh"
 #include "xns_internal.cuh"
 
 namespace xns_sinc {
 
 constexpr int SE_THREADS = 256;
 constexpr int SE_TILE = 2048;
-constexpr double TWO_PI = 6.283185307179586476925286766559;
-constexpr double INV_TWO_PI = 0.15915494309189533576888376337251;
 
 struct PairRec {
   double r;      // distance (FP64)
   float w_r;     // weight / r; 0 for a record that does not count
   float c2;      // 2 cos(dq r)
-  float theta;   // dq r
+  float s_th;    // sin(dq r)
   float pad;
 };
 
@@ -39,20 +39,15 @@ __device__ __forceinline__ PairRec make_rec(double r, double w, double dq) {
   PairRec rec;
   rec.r = r;
   rec.w_r = (float)(w / r);
-  float th = (float)(dq * r);
-  float h = sinf(0.5f * th);
-  rec.c2 = 2.f - 4.f * h * h;
-  rec.theta = th;
+  float s, c;
+  xns_math::xns_sincos(dq * r, &s, &c);
+  rec.c2 = 2.f * c;
+  rec.s_th = s;
   rec.pad = 0.f;
   return rec;
 }
 
 __device__ __forceinline__ PairRec null_rec() { return PairRec{1.0, 0.f, 2.f, 0.f, 0.f}; }
-
-__device__ __forceinline__ float sin_reduced(double x) {
-  double n = rint(x * INV_TWO_PI);
-  return __sinf((float)__fma_rn(-n, TWO_PI, x));
-}
 
 struct SincParams {
   double q0, dq;      // uniform mesh
@@ -111,13 +106,15 @@ __global__ void __launch_bounds__(SE_THREADS, 2) sinc_tiles_kernel(SincParams p,
         if (A.w_r == 0.f && B.w_r == 0.f) continue;
         if (DIRECT) {
 #pragma unroll
-          for (int k = 0; k < M; k++) blk[k] += sin_reduced(qd[k] * A.r) * A.w_r + sin_reduced(qd[k] * B.r) * B.w_r;
+          for (int k = 0; k < M; k++)
+            blk[k] += xns_math::xns_sin(qd[k] * A.r) * A.w_r + xns_math::xns_sin(qd[k] * B.r) * B.w_r;
         } else {
-          double xa = qk0 * A.r, xb = qk0 * B.r;
-          double na = rint(xa * INV_TWO_PI), nb = rint(xb * INV_TWO_PI);
-          float ra = (float)__fma_rn(-na, TWO_PI, xa), rb = (float)__fma_rn(-nb, TWO_PI, xb);
-          float a0 = __sinf(ra) * A.w_r, am = __sinf(ra - A.theta) * A.w_r;
-          float b0 = __sinf(rb) * B.w_r, bm = __sinf(rb - B.theta) * B.w_r;
+          // seeds: sin and cos of q_{k0} r, then sin(q_{k0} r - dq r) by the angle-difference formula
+          float sa, csa, sb, csb;
+          xns_math::xns_sincos(qk0 * A.r, &sa, &csa);
+          xns_math::xns_sincos(qk0 * B.r, &sb, &csb);
+          float a0 = sa * A.w_r, am = fmaf(sa, 0.5f * A.c2, -csa * A.s_th) * A.w_r;
+          float b0 = sb * B.w_r, bm = fmaf(sb, 0.5f * B.c2, -csb * B.s_th) * B.w_r;
           const float ca = A.c2, cb = B.c2;
           blk[0] += a0 + b0;
 #pragma unroll
