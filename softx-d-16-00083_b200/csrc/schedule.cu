@@ -19,7 +19,6 @@ unsigned long long xns_build_schedule(const std::vector<Segment> &sa, const std:
     p.ratio = tile_b / tile_a;
     p.pad = 0;
     unsigned long long n = p.same ? (unsigned long long)p.tb * (p.tb + 1) / 2 * p.ratio : (unsigned long long)p.ta * p.tb;
-    if (p.same && p.na < 2) continue;
     p.tile_begin = total;
     total += n;
     out->push_back(p);

@@ -5,12 +5,15 @@
 //
 // Records (r, w) arrive in tiles of up to SE_TILE produced cooperatively by a Source in shared
 // memory.  A lane owns a chunk of M consecutive q values, a slot of lanes walks the tile's records.
-// On a uniform mesh q_k = q0 + k dq the lane seeds s_0 = sin(q_{k0} r) w/r and
-// s_{-1} = sin(q_{k0} r - dq r) w/r from an accurate sine and cosine of the FP64 phase (xmath.cuh;
-// the MUFU approximations would add coherently over the distance shells of a crystal) and runs the
-// Chebyshev recurrence s_{k+1} = 2cos(dq r) s_k - s_{k-1}: one FFMA per term for the sine and one
-// FADD for the sum, no transcendental.  The rounding of 2cos(dq r) makes the phase drift by at most
-// M * 2^-23 / (2 sin(dq r)) over a chunk, pseudo-random from pair to pair.  Sums run in FP32 over one
+// On a uniform mesh q_k = q0 + k dq the lane seeds s_0 = sin(q_{k0} r) w/r and the difference
+// d_0 = s_0 - s_{-1} = 2 sin(t/2) cos(q_{k0} r - t/2) w/r (t = dq r) from an accurate sine and cosine
+// of the FP64 phase (xmath.cuh; the MUFU approximations would add coherently over the distance shells
+// of a crystal) and runs the sine recurrence in Reinsch's difference form,
+//   d_{k+1} = d_k - lam s_k,  s_{k+1} = s_k + d_{k+1},  lam = 4 sin^2(t/2),
+// which is the Chebyshev recurrence s_{k+1} = 2cos(t) s_k - s_{k-1} with 2cos(t) kept as 2 - lam: lam
+// carries full relative precision even for small t, so the phase does not drift the way a rounded
+// 2cos(t) (error 2^-24 / sin t per step) would on fine q meshes.  Three FP32 instructions per
+// (record, q) term (FFMA, FADD, and the FADD of the sum), no transcendental.  Sums run in FP32 over one
 // tile (<= SE_TILE/slots records per lane) and are added to per-thread FP64 totals in shared memory
 // after every tile (compensated block accumulation); CTAs then reduce in FP64 in the epilogue.  1/q_k
 // is applied in the epilogue.  A mesh that is not uniform takes an accurate sine per term (DIRECT).
@@ -30,9 +33,9 @@ constexpr int SE_TILE = 2048;
 struct PairRec {
   double r;      // distance (FP64)
   float w_r;     // weight / r; 0 for a record that does not count
-  float c2;      // 2 cos(dq r)
-  float s_th;    // sin(dq r)
-  float pad;
+  float lam;     // 4 sin^2(dq r / 2) = 2 - 2 cos(dq r)
+  float h2;      // 2 sin(dq r / 2)
+  float ch;      // cos(dq r / 2)
 };
 
 __device__ __forceinline__ PairRec make_rec(double r, double w, double dq) {
@@ -40,14 +43,14 @@ __device__ __forceinline__ PairRec make_rec(double r, double w, double dq) {
   rec.r = r;
   rec.w_r = (float)(w / r);
   float s, c;
-  xns_math::xns_sincos(dq * r, &s, &c);
-  rec.c2 = 2.f * c;
-  rec.s_th = s;
-  rec.pad = 0.f;
+  xns_math::xns_sincos(0.5 * dq * r, &s, &c);
+  rec.lam = 4.f * s * s;
+  rec.h2 = 2.f * s;
+  rec.ch = c;
   return rec;
 }
 
-__device__ __forceinline__ PairRec null_rec() { return PairRec{1.0, 0.f, 2.f, 0.f, 0.f}; }
+__device__ __forceinline__ PairRec null_rec() { return PairRec{1.0, 0.f, 0.f, 0.f, 1.f}; }
 
 struct SincParams {
   double q0, dq;      // uniform mesh
@@ -109,23 +112,21 @@ __global__ void __launch_bounds__(SE_THREADS, 2) sinc_tiles_kernel(SincParams p,
           for (int k = 0; k < M; k++)
             blk[k] += xns_math::xns_sin(qd[k] * A.r) * A.w_r + xns_math::xns_sin(qd[k] * B.r) * B.w_r;
         } else {
-          // seeds: sin and cos of q_{k0} r, then sin(q_{k0} r - dq r) by the angle-difference formula
+          // seeds: s_0 = sin(x), d_0 = s_0 - s_{-1} = 2 sin(t/2) cos(x - t/2) with x = q_{k0} r, t = dq r
           float sa, csa, sb, csb;
           xns_math::xns_sincos(qk0 * A.r, &sa, &csa);
           xns_math::xns_sincos(qk0 * B.r, &sb, &csb);
-          float a0 = sa * A.w_r, am = fmaf(sa, 0.5f * A.c2, -csa * A.s_th) * A.w_r;
-          float b0 = sb * B.w_r, bm = fmaf(sb, 0.5f * B.c2, -csb * B.s_th) * B.w_r;
-          const float ca = A.c2, cb = B.c2;
-          blk[0] += a0 + b0;
+          float a = sa * A.w_r, da = A.h2 * fmaf(csa, A.ch, sa * (0.5f * A.h2)) * A.w_r;
+          float b = sb * B.w_r, db = B.h2 * fmaf(csb, B.ch, sb * (0.5f * B.h2)) * B.w_r;
+          const float la = A.lam, lb = B.lam;
+          blk[0] += a + b;
 #pragma unroll
           for (int k = 1; k < M; k++) {
-            float an = fmaf(ca, a0, -am);
-            float bn = fmaf(cb, b0, -bm);
-            blk[k] += an + bn;
-            am = a0;
-            a0 = an;
-            bm = b0;
-            b0 = bn;
+            da = fmaf(-la, a, da);
+            db = fmaf(-lb, b, db);
+            a += da;
+            b += db;
+            blk[k] += a + b;
           }
         }
       }

@@ -23,6 +23,11 @@ enum ScratchSlot {
   SLOT_OUT2,
   SLOT_FLAGS,           // error counters
   SLOT_AUX,
+  SLOT_HSORT,           // histogram plan: cell-sorted coordinates and per-atom cell ids
+  SLOT_HCELL,           // histogram plan: per-cell counts, offsets, cursors
+  SLOT_HTILE,           // histogram plan: tiles (atom ranges with bounding boxes)
+  SLOT_HLIST,           // histogram plan: tile pairs sorted by (element pair, distance bucket)
+  SLOT_HKEY,            // histogram plan: bucket counts / offsets and small tables
   SLOT_COUNT
 };
 

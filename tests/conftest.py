@@ -37,6 +37,15 @@ def rel_err(a, b):
     return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)))
 
 
+def rel_err_floor(a, b, floor_frac):
+    """Max relative error with the denominator floored at floor_frac * median|b|: near-zero points of an
+    interference pattern (|A|^2 of a sum of N unit phasors that nearly cancel) carry the absolute
+    error of the phasor sum, not a relative one."""
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    floor = floor_frac * float(np.median(np.abs(b)))
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), floor)))
+
+
 @pytest.fixture(scope="session")
 def oracle():
     from oracle import Oracle

@@ -4,14 +4,15 @@ relative tolerances (FP32 arithmetic with FP64 reductions against the reference'
 import numpy as np
 import pytest
 
-from conftest import golden_names, load_golden, rel_err, split_elements
+from conftest import golden_names, load_golden, rel_err, rel_err_floor, split_elements
 
 from xns_b200 import synth
 
 pytestmark = pytest.mark.gpu
 
 TOL_I = 1e-5       # I(q) of the plain Debye / histogram paths, max relative error
-TOL_2D = 1e-5      # 2D intensity, max relative error
+TOL_2D = 1e-5      # 2D intensity, max relative error with the denominator floored at 1e-2 x median
+FLOOR_2D = 1e-2
 
 
 @pytest.mark.parametrize("name", golden_names("hist"))
@@ -27,6 +28,17 @@ def test_hist_vs_oracle(gpu_ctx, oracle, cells, bin, seed):
     els = synth.rocksalt_cube(cells=cells, seed=seed)
     nh = synth.hist_size(els, bin)
     assert np.array_equal(gpu_ctx.calc_hist(els, nh, bin), oracle.hist(els, nh, bin))
+
+
+def test_hist_sparse_element_and_sphere(gpu_ctx, oracle):
+    """A 5 % substituent spreads its few atoms over the whole crystallite: its tile pairs are wider
+    than the shared-memory window and take the direct path; a sphere exercises partly filled cells."""
+    els = synth.fcc_crystallite(cells=9, subst=0.05, seed=6)
+    nh = synth.hist_size(els, 0.001)
+    assert np.array_equal(gpu_ctx.calc_hist(els, nh, 0.001), oracle.hist(els, nh, 0.001))
+    sph = synth.fcc_sphere(n=6000, seed=7)
+    nh = synth.hist_size(sph, 0.001)
+    assert np.array_equal(gpu_ctx.calc_hist(sph, nh, 0.001), oracle.hist(sph, nh, 0.001))
 
 
 def test_hist_edge_cases(gpu_ctx, oracle):
@@ -128,5 +140,5 @@ def test_2d_golden(gpu_ctx, name):
     els = split_elements(g["xyz"], g["n_el"])
     I2D, I = gpu_ctx.calc_int_2d(els, g["q"], int(g["nfi"]), g["emin"], g["emax"], g["en"], int(g["conv"]),
                                  float(g["lam"]), int(g["source"]), ff=g.get("ff"), sl=g.get("sl"), polar=bool(g["polar"]))
-    assert rel_err(I2D, g["I2D"]) < TOL_2D
+    assert rel_err_floor(I2D, g["I2D"], FLOOR_2D) < TOL_2D
     assert rel_err(I, g["I"]) < TOL_2D
