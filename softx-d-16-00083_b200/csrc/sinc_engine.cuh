@@ -13,9 +13,9 @@
 // which is the Chebyshev recurrence s_{k+1} = 2cos(t) s_k - s_{k-1} with 2cos(t) kept as 2 - lam: lam
 // carries full relative precision even for small t, so the phase does not drift the way a rounded
 // 2cos(t) (error 2^-24 / sin t per step) would on fine q meshes.  Three FP32 instructions per
-// (record, q) term (FFMA, FADD, and the FADD of the sum), no transcendental.  Sums run in FP32 over one
-// tile (<= SE_TILE/slots records per lane) and are added to per-thread FP64 totals in shared memory
-// after every tile (compensated block accumulation); CTAs then reduce in FP64 in the epilogue.  1/q_k
+// (record, q) term (FFMA, FADD, and the FADD of the sum), no transcendental.  Sums run in FP32 over
+// SE_FP32_PAIRS record pairs and are then added to per-thread FP64 totals in shared memory
+// (compensated block accumulation); CTAs then reduce in FP64 in the epilogue.  1/q_k
 // is applied in the epilogue.  A mesh that is not uniform takes an accurate sine per term (DIRECT).
 #pragma once
 #include <math.h>
@@ -29,6 +29,11 @@ namespace xns_sinc {
 
 constexpr int SE_THREADS = 256;
 constexpr int SE_TILE = 2048;
+// Record pairs a lane sums in FP32 before adding the sums to its FP64 totals.  A lane adds each
+// record's term to a running FP32 sum, so the rounding error grows with the length of that sum; with
+// the large cancellation at the minima of I(q) (sum of |terms| ~10^3 x the result) 8 pairs keep the
+// FP32 summation error within ~3x of the FP32 rounding of the terms themselves.
+constexpr int SE_FP32_PAIRS = 8;
 
 struct PairRec {
   double r;      // distance (FP64)
@@ -102,11 +107,21 @@ __global__ void __launch_bounds__(SE_THREADS, 2) sinc_tiles_kernel(SincParams p,
       float blk[M];
 #pragma unroll
       for (int k = 0; k < M; k++) blk[k] = 0.f;
+      int nblk = 0;  // record pairs in blk
       for (int e = slot; e < n; e += 2 * nslots) {
         const PairRec A = pr[e];
         const int e2 = e + nslots;
         const PairRec B = e2 < n ? pr[e2] : null_rec();
         if (A.w_r == 0.f && B.w_r == 0.f) continue;
+        if (nblk == SE_FP32_PAIRS) {  // FP32 sums stay short: move them to the FP64 totals
+#pragma unroll
+          for (int k = 0; k < M; k++) {
+            acc64[k * SE_THREADS + tid] += (double)blk[k];
+            blk[k] = 0.f;
+          }
+          nblk = 0;
+        }
+        nblk++;
         if (DIRECT) {
 #pragma unroll
           for (int k = 0; k < M; k++)
