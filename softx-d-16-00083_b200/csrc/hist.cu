@@ -282,8 +282,8 @@ struct HistParams {
 
 // One warp counts the pairs of one tile pair: the I tile is staged in the warp's shared memory, the J
 // tile sits in registers (atoms lane and lane + 32), the warp walks i.
-template <class Count>
-__device__ __forceinline__ unsigned count_tile_pair(const HistParams &p, const TilePair tp, double *wI, Count count) {
+template <bool SAME, class Count>
+__device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const TilePair tp, double *wI, Count count) {
   const uint32_t lane = threadIdx.x & 31;
   const Tile TI = p.tiles[tp.I], TJ = p.tiles[tp.J];
   const uint32_t ni = TI.count, nj = TJ.count;
@@ -298,23 +298,48 @@ __device__ __forceinline__ unsigned count_tile_pair(const HistParams &p, const T
   const double x1 = j1 < nj ? p.X[TJ.start + j1] : 0.0, y1 = j1 < nj ? p.Y[TJ.start + j1] : 0.0,
                z1 = j1 < nj ? p.Z[TJ.start + j1] : 0.0;
   __syncwarp();
-  const bool same = tp.I == tp.J;
+  const double nh1 = (double)p.nhist - 1.0;
   unsigned bad = 0;
-  for (uint32_t i = 0; i < ni; i++) {
-    const double xi = wI[i], yi = wI[TILE_MAX + i], zi = wI[2 * TILE_MAX + i];
-    if (j0 < nj && (!same || i < j0)) {
-      const uint32_t k = ref_bin(ref_dist2(xi, yi, zi, x0, y0, z0), p.bin, p.inv_bin, p.margin, p.nhist);
-      if (k < p.nhist) count(k);
-      else bad++;
+  // rows i and i+1 against columns j0 and j1: four independent FP64 chains per iteration, no branch
+  // until the rare exact fallback.  SAME (a tile against itself) keeps only i < j.
+  const bool c0 = j0 < nj, c1 = j1 < nj;
+  for (uint32_t i = 0; i < ni; i += 2) {
+    const uint32_t i1 = min(i + 1, ni - 1);
+    const double xa = wI[i], ya = wI[TILE_MAX + i], za = wI[2 * TILE_MAX + i];
+    const double xb = wI[i1], yb = wI[TILE_MAX + i1], zb = wI[2 * TILE_MAX + i1];
+    const bool r1 = i + 1 < ni;
+    bool v0 = c0, v1 = c1, v2 = c0 && r1, v3 = c1 && r1;
+    if (SAME) {
+      v0 = v0 && i < j0;
+      v1 = v1 && i < j1;
+      v2 = v2 && i + 1 < j0;
+      v3 = v3 && i + 1 < j1;
     }
-    if (j1 < nj && (!same || i < j1)) {
-      const uint32_t k = ref_bin(ref_dist2(xi, yi, zi, x1, y1, z1), p.bin, p.inv_bin, p.margin, p.nhist);
-      if (k < p.nhist) count(k);
-      else bad++;
+    const double d0 = ref_dist2(xa, ya, za, x0, y0, z0), d1 = ref_dist2(xa, ya, za, x1, y1, z1);
+    const double d2 = ref_dist2(xb, yb, zb, x0, y0, z0), d3 = ref_dist2(xb, yb, zb, x1, y1, z1);
+    uint32_t k0, k1, k2, k3;
+    const bool f0 = ref_bin_fast(d0, p.inv_bin, p.margin, nh1, &k0), f1 = ref_bin_fast(d1, p.inv_bin, p.margin, nh1, &k1);
+    const bool f2 = ref_bin_fast(d2, p.inv_bin, p.margin, nh1, &k2), f3 = ref_bin_fast(d3, p.inv_bin, p.margin, nh1, &k3);
+    if (!((f0 || !v0) && (f1 || !v1) && (f2 || !v2) && (f3 || !v3))) {
+      // a distance within the margin of a bin edge (or outside the estimate's range): exact path;
+      // a bin beyond the histogram is reported, not counted
+      if (v0 && !f0) { k0 = ref_bin(d0, p.bin, p.inv_bin, p.margin, p.nhist); if (k0 >= p.nhist) { v0 = false; bad++; } }
+      if (v1 && !f1) { k1 = ref_bin(d1, p.bin, p.inv_bin, p.margin, p.nhist); if (k1 >= p.nhist) { v1 = false; bad++; } }
+      if (v2 && !f2) { k2 = ref_bin(d2, p.bin, p.inv_bin, p.margin, p.nhist); if (k2 >= p.nhist) { v2 = false; bad++; } }
+      if (v3 && !f3) { k3 = ref_bin(d3, p.bin, p.inv_bin, p.margin, p.nhist); if (k3 >= p.nhist) { v3 = false; bad++; } }
     }
+    if (v0) count(k0);
+    if (v1) count(k1);
+    if (v2) count(k2);
+    if (v3) count(k3);
   }
   __syncwarp();
   return bad;
+}
+
+template <class Count>
+__device__ __forceinline__ unsigned count_tile_pair(const HistParams &p, const TilePair tp, double *wI, Count count) {
+  return tp.I == tp.J ? count_tile_pair_t<true>(p, tp, wI, count) : count_tile_pair_t<false>(p, tp, wI, count);
 }
 
 // Adds window bins [lo, hi) to the global histogram and clears them (all threads of the CTA).
@@ -569,7 +594,6 @@ int xns_hist_device(xns_ctx *ctx, const DevCoords &dc, uint32_t nhist, double bi
   hp.nel = nel;
   hp.wide_begin = n_narrow;
   hp.wide_end = (uint32_t)ntp;
-  if ((st = xns_stage_begin(ctx, STAGE_HIST))) return st;
   if (!ranges.empty()) {
     void *vr, *vrh;
     if ((st = xns_scratch(ctx, SLOT_SEGPAIRS, sizeof(CtaRange) * ranges.size() + sizeof(SegPair) * sched.size(), &vr)))
@@ -582,9 +606,11 @@ int xns_hist_device(xns_ctx *ctx, const DevCoords &dc, uint32_t nhist, double bi
     hp.ranges = (const CtaRange *)vr;
     const size_t smem = sizeof(uint32_t) * WIN + sizeof(double) * 3 * TILE_MAX * HW_WARPS;
     XNS_CUDA(ctx, cudaFuncSetAttribute(hist_window_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if ((st = xns_stage_begin(ctx, STAGE_HIST))) return st;
     hist_window_kernel<<<(unsigned)ranges.size(), HW_THREADS, smem, ctx->stream>>>(hp);
     XNS_LAUNCHED(ctx);
   }
+  if (ranges.empty() && (st = xns_stage_begin(ctx, STAGE_HIST))) return st;
   if (hp.wide_end > hp.wide_begin) {
     hist_wide_kernel<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(hp);
     XNS_LAUNCHED(ctx);

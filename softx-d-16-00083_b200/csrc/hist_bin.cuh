@@ -52,6 +52,26 @@ __device__ __forceinline__ uint32_t ref_bin(double d2, double bin, double inv_bi
   return (uint32_t)q;
 }
 
+// The estimate of ref_bin without branches: k is valid when the return value is true.  Callers run
+// several of these side by side (independent FP64 chains) and send the rare false ones to ref_bin.
+__device__ __forceinline__ bool ref_bin_fast(double d2, double inv_bin, double margin, double nhist_m1, uint32_t *k) {
+  const double MAGIC = 6755399441055744.0;
+  const int hi = __double2hiint(d2);
+  const bool in_range = (unsigned)(hi - (897 << 20)) < (unsigned)((1151 - 897) << 20);
+  // rsqrt.approx (what rsqrtf compiles to; 2 ulp): the flush-to-zero form is one MUFU instruction, and
+  // in_range keeps its argument a normal float
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(trunc_to_float(d2)));
+  const double yd = float_to_double_exact(y);
+  const double r0 = __dmul_rn(d2, yd);
+  const double res = __fma_rn(-r0, r0, d2);
+  const double t = __dmul_rn(__fma_rn(res, 0.5 * yd, r0), inv_bin);
+  const double u = __dadd_rn(t, MAGIC);
+  const double d = __dsub_rn(t, __dsub_rn(u, MAGIC));
+  *k = (uint32_t)__double2loint(u) - (d < 0.0 ? 1u : 0u);
+  return in_range && t < nhist_m1 && fabs(d) >= margin;
+}
+
 __device__ __forceinline__ double ref_dist2(double xi, double yi, double zi, double xj, double yj, double zj) {
   double dx = __dsub_rn(xi, xj), dy = __dsub_rn(yi, yj), dz = __dsub_rn(zi, zj);
   return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
