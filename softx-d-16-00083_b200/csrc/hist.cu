@@ -31,7 +31,7 @@ using namespace xns_hist;
 
 namespace {
 
-constexpr int CELL_TARGET = 48;      // mean atoms per cell over an element's bounding box
+constexpr int CELL_TARGET = 56;      // mean atoms per cell over an element's bounding box
 constexpr int TILE_MAX = 64;         // atoms per tile
 constexpr int MAX_CELLS_AXIS = 256;
 constexpr int HW_WARPS = 16;
@@ -342,17 +342,36 @@ __device__ __forceinline__ unsigned count_tile_pair(const HistParams &p, const T
   return tp.I == tp.J ? count_tile_pair_t<true>(p, tp, wI, count) : count_tile_pair_t<false>(p, tp, wI, count);
 }
 
-// Adds window bins [lo, hi) to the global histogram and clears them (all threads of the CTA).
-__device__ __forceinline__ void flush_window(uint32_t *win, unsigned long long *h, uint32_t lo, uint32_t hi, uint32_t nhist) {
-  hi = min(hi, nhist);
-  for (uint32_t k = lo + threadIdx.x; k < hi; k += HW_THREADS) {
-    const uint32_t s = k % WIN;
+// Slot s of the window holds bin B + s.  flush_window adds slots [lo, hi) (bins B + lo ...) to the
+// global histogram and clears them (all threads of the CTA).
+__device__ __forceinline__ void flush_window(uint32_t *win, unsigned long long *h, uint32_t B, uint32_t lo, uint32_t hi,
+                                             uint32_t nhist) {
+  hi = min(hi, nhist > B ? nhist - B : 0u);
+  for (uint32_t s = lo + threadIdx.x; s < hi; s += HW_THREADS) {
     const uint32_t v = win[s];
     if (v) {
-      atomicAdd(h + k, (unsigned long long)v);
+      atomicAdd(h + B + s, (unsigned long long)v);
       win[s] = 0;
     }
   }
+}
+
+// Moves the window from B to nb > B: bins [B, nb) leave (flushed), bins [nb, B + WIN) move down to
+// slots [0, B + WIN - nb), the vacated top slots are cleared.  Called by all threads between barriers.
+__device__ __forceinline__ void slide_window(uint32_t *win, unsigned long long *h, uint32_t B, uint32_t nb, uint32_t nhist) {
+  const uint32_t delta = nb - B;
+  flush_window(win, h, B, 0, min(delta, WIN), nhist);
+  if (delta >= WIN) return;  // everything left; the flush cleared it
+  __syncthreads();
+  // shift down by delta in chunks: a chunk's reads lie above every slot written so far
+  for (uint32_t c = 0; c < WIN - delta; c += HW_THREADS) {
+    const uint32_t s = c + threadIdx.x;
+    const uint32_t v = s < WIN - delta ? win[s + delta] : 0u;
+    __syncthreads();
+    if (s < WIN - delta) win[s] = v;
+    __syncthreads();
+  }
+  for (uint32_t s = WIN - delta + threadIdx.x; s < WIN; s += HW_THREADS) win[s] = 0;
 }
 
 __global__ void __launch_bounds__(HW_THREADS, 1) hist_window_kernel(HistParams p) {
@@ -371,22 +390,25 @@ __global__ void __launch_bounds__(HW_THREADS, 1) hist_window_kernel(HistParams p
     for (uint32_t e = r; e < min(r + HW_WARPS, rg.end); e++) kmax = max(kmax, p.list[e].kmax);
     if (kmax >= B + WIN) {
       const uint32_t nb = p.list[r].kmin / BUCKET * BUCKET;
-      __syncthreads();
-      flush_window(win, h, B, min(nb, B + WIN), p.nhist);
-      B = nb;
-      __syncthreads();
+      if (nb > B) {
+        __syncthreads();
+        slide_window(win, h, B, nb, p.nhist);
+        B = nb;
+        __syncthreads();
+      }
     }
     const uint32_t e = r + (threadIdx.x >> 5);
     if (e < rg.end) {
       const uint32_t base = B;
       bad += count_tile_pair(p, p.list[e], wI, [&](uint32_t k) {
-        if (k - base < WIN) atomicAdd(win + k % WIN, 1u);
+        const uint32_t s = k - base;
+        if (s < WIN) atomicAdd(win + s, 1u);
         else atomicAdd(h + k, 1ull);  // outside the window (a round spanning two buckets): count directly
       });
     }
   }
   __syncthreads();
-  flush_window(win, h, B, B + WIN, p.nhist);
+  flush_window(win, h, B, 0, WIN, p.nhist);
   if (bad) atomicAdd(p.n_bad, bad);
 }
 
