@@ -9,39 +9,11 @@
 // shared sinc engine (sinc_engine.cuh).
 #include <string.h>
 
+#include "bin_source.cuh"
 #include "sinc_engine.cuh"
 
 using namespace xns_sinc;
 
-namespace {
-
-struct BinSrc {
-  const unsigned long long *hist;
-  uint32_t nhist;
-  uint32_t tiles_per_pair;
-  double bin;
-
-  __device__ uint32_t cls(unsigned long long w) const { return (uint32_t)(w / tiles_per_pair); }
-
-  __device__ int fill(unsigned long long w, PairRec *pr, void *, double dq) const {
-    const uint32_t t = (uint32_t)(w / tiles_per_pair);
-    const uint32_t b0 = (uint32_t)(w % tiles_per_pair) * SE_TILE;
-    const unsigned long long *h = hist + (size_t)t * nhist;
-    for (int e = threadIdx.x; e < SE_TILE; e += SE_THREADS) {
-      const uint32_t k = b0 + e;
-      PairRec rec = null_rec();
-      if (k < nhist) {
-        unsigned long long n = h[k];
-        if (n) rec = make_rec(((double)k + 0.5) * bin, (double)n, dq);
-      }
-      pr[e] = rec;
-    }
-    __syncthreads();
-    return SE_TILE;
-  }
-};
-
-}  // namespace
 
 int xns_hist_iq_device(xns_ctx *ctx, const unsigned long long *d_hist, const uint32_t *n_el, uint32_t nel, uint32_t nhist,
                        double bin, const double *q, uint32_t nq, const double *d_w, int polar, double lambda, double *d_I) {
