@@ -33,6 +33,7 @@ extern "C" {
 #define XNS_ERR_NODEV 3    /* no sm_100 device / library not built for it */
 #define XNS_ERR_RANGE 4    /* a pair distance fell beyond the histogram (reference: out-of-bounds write) */
 #define XNS_ERR_NOMEM 5    /* device allocation failed */
+#define XNS_ERR_LIMIT 6    /* a size beyond the fixed limits of xns_int_1d_hist_noalloc */
 
 /* typedefs.h:50-56 */
 #define XNS_NEUTRON 0
@@ -124,6 +125,27 @@ int xns_pdf_and_debye_device(xns_ctx *ctx, const double *xyz_dev, const uint32_t
                              double bin, int scenario, int pdftype, double p0, const double *q, uint32_t nq, int source,
                              const double *const *ff, const double *sl, int polar, double lambda, double *I_dev,
                              double *pdf_dev, uint64_t *hist_dev);
+
+/* ---- allocation-free entry point ------------------------------------------------------------------ */
+
+/* Histogram -> I(q) that allocates no device memory.  No counterpart in the reference: it serves
+ * callers that cannot call cudaMalloc -- a plugin whose host framework owns all device memory and
+ * hands it buffers, or a service whose memory budget is fixed at start-up.  The caller passes the
+ * histogram (hist_dev: P*nhist u64) and the output (I_dev: nq doubles) as device buffers it owns; the
+ * result equals xns_calc_int_1d_hist's.  Intermediates live in one file-scope device array of
+ * XNS_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until exit.  Limits: at most
+ * XNS_NOALLOC_MAX_ELEMENTS elements, XNS_NOALLOC_MAX_Q q points, and (P + nel + 1) * nq * 8 bytes plus
+ * one CTA's P * nq * 8 bytes of partial sums within the array; larger sizes return XNS_ERR_LIMIT.
+ * Runs on the current device and the given stream (NULL = default stream) and returns without
+ * waiting for the GPU.  The first call on a device looks up the array's device address: make it before
+ * any stream capture.  Calls share the array: calls that overlap on the GPU (other streams, other host
+ * threads) race on it. */
+#define XNS_NOALLOC_SCRATCH_BYTES (16u << 20)
+#define XNS_NOALLOC_MAX_ELEMENTS 16
+#define XNS_NOALLOC_MAX_Q 8192
+int xns_int_1d_hist_noalloc(const uint64_t *hist_dev, const uint32_t *n_el, uint32_t nel, uint32_t nhist, double bin,
+                            const double *q, uint32_t nq, int source, const double *const *ff, const double *sl, int polar,
+                            double lambda, double *I_dev, void *stream);
 
 /* ---- utilities (no reference counterpart) -------------------------------------------------------- */
 

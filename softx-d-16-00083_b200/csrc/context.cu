@@ -170,6 +170,7 @@ const char *xns_status_string(int status) {
     case XNS_ERR_NODEV: return "no compute capability 10.x device";
     case XNS_ERR_RANGE: return "pair distance beyond the histogram";
     case XNS_ERR_NOMEM: return "device memory allocation failed";
+    case XNS_ERR_LIMIT: return "size beyond the allocation-free entry point's fixed limits";
     default: return "unknown status";
   }
 }
