@@ -334,6 +334,154 @@ def ours(args, rank, world, local_rank):
     return 0
 
 
+# ---- secondary workloads (one GPU): the other measurement rows of the hot path -------------------
+def _measure(ctx, call, steps, warmup, stage):
+    """Runs call() warmup + steps times; returns (mean event time of the whole call in ms, mean
+    kernel-only stage time in ms, kernels launched in the timed calls, clocks)."""
+    import torch
+    from xns_b200 import lib
+    lib.xns_last_stage_ms.argtypes = [__import__("ctypes").c_void_p, __import__("ctypes").c_int]
+    lib.xns_last_stage_ms.restype = __import__("ctypes").c_double
+    for _ in range(warmup):
+        call()
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    clocks = Clocks(0)
+    clocks.start()
+    l0 = ctx.kernel_launches
+    tot = kern = 0.0
+    for _ in range(steps):
+        flush.fill_(1.0)
+        ev0.record(stream)
+        call()
+        ev1.record(stream)
+        ev1.synchronize()
+        tot += ev0.elapsed_time(ev1)
+        kern += lib.xns_last_stage_ms(ctx.handle, stage)
+    return tot / steps, kern / steps, ctx.kernel_launches - l0, clocks.stop()
+
+
+def _fma_peaks(ctx):
+    import ctypes as C
+    from xns_b200 import lib
+    lib.xns_measure_fma_peak.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
+    p64, p32 = C.c_double(0), C.c_double(0)
+    lib.xns_measure_fma_peak(ctx.handle, 1, C.byref(p64))
+    lib.xns_measure_fma_peak(ctx.handle, 0, C.byref(p32))
+    return p64.value, p32.value
+
+
+def debye_workload(args):
+    """Config 1: exact Debye double sum, fcc sphere a = 4.078 A cropped to 5000 atoms, Gaussian
+    displacement 0.05 A, neutron b = 7.63 fm, 1024 q in [0.1, 10).  Metric atom-pairs/s per pattern;
+    roofline: FP32 pipe at 4 flops per (pair, q) term."""
+    import torch
+    import xns_b200
+    from xns_b200 import synth
+    torch.cuda.set_device(0)
+    ctx = xns_b200.Context(0)
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    els = synth.fcc_sphere(n=5000, a=4.078, sigma=0.05, seed=0)
+    q = synth.q_mesh(0.1, 10.0, 1024)
+    n = 5000
+    pairs = n * (n - 1) // 2
+    ms, kms, launches, clk = _measure(ctx, lambda: ctx.calc_int_debye(els, q, xns_b200.NEUTRON, sl=[7.63]), args.steps,
+                                      args.warmup, 3)
+    p64, p32 = _fma_peaks(ctx)
+    achieved = 4.0 * pairs * len(q) / (kms * 1e-3) / 1e12
+    line = {"metric": "atom-pairs/s", "value": pairs / (kms * 1e-3), "unit": "pairs/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": kms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 terms, f64 reductions", "data": "synthetic (seeded)", "patterns_per_s": 1e3 / kms,
+            "config": {"workload": "exact Debye, fcc sphere 5000 atoms a=4.078 A sigma=0.05 A, neutron, 1024 q in [0.1,10)",
+                       "pairs_per_step": pairs, "nq": len(q), "l2": "flushed (512 MB write) before every timed step"},
+            "roofline": {"kernel": "sinc_tiles_kernel<AtomPairSrc>", "bound": "fp32", "achieved": achieved, "peak": p32,
+                         "unit": "TFLOP/s", "frac": achieved / p32, "traffic": None, "flops_per_term": 4,
+                         "peak_source": "measured in-process (FFMA loop, xns_measure_fma_peak)"},
+            "e2e": {"value": pairs / (ms * 1e-3), "unit": "pairs/s", "ms_per_step": ms, "h2d_bytes_per_step": n * 24 + 8 * 1024,
+                    "d2h_bytes_per_step": 8 * 1024},
+            "gpu_launches": int(launches), "clocks": clk}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as orc
+        cores = os.cpu_count() or 1
+        try:
+            R, kind = orc.Reference(threads=cores), "reference"
+        except FileNotFoundError:
+            R, kind = orc.Oracle(), "port"
+        m = 1500
+        while True:
+            sub = [els[0][:m]]
+            t = time.perf_counter()
+            R.int_debye(sub, q, 0, sl=[7.63])
+            dt = time.perf_counter() - t
+            if dt > 3.0 or m >= n:
+                break
+            m = min(n, int(m * min(2.0, max(1.2, (8.0 / max(dt, 1e-3)) ** 0.5))))
+        sp = m * (m - 1) // 2
+        line["cpu_baseline"] = {"value": sp / dt, "unit": "pairs/s", "cores": cores, "kind": kind,
+                                "sample": "calcIntDebye on the first %d atoms of the sphere, 1024 q, %.2f s" % (m, dt)}
+    print(json.dumps(line))
+    ctx.close()
+    return 0
+
+
+def twod_workload(args):
+    """Config 3: 2D amplitude of a 1,000,188-atom fcc crystallite (a = 3.61 A, 63^3 cells, 5 % second
+    species, seeded random orientation), X-ray form factors from seeded 4-Gaussian coefficients, on the
+    reference's polar mesh of 1024 q in [0.05, 8) x 1024 phi with lambda = 0.01 A (a nearly flat
+    detector plane), one orientation.  Metric (atom, mesh point) terms per second."""
+    import torch
+    import xns_b200
+    from xns_b200 import synth
+    torch.cuda.set_device(0)
+    ctx = xns_b200.Context(0)
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    els = synth.fcc_crystallite(cells=args.cells2d, a=3.61, subst=0.05, seed=0)
+    n = sum(len(e) for e in els)
+    nq = nfi = args.mesh2d
+    q = synth.q_mesh(0.05, 8.0, nq)
+    ff = synth.ff_on_mesh(synth.ff_coefficients(2, seed=3), q)
+    call = lambda: ctx.calc_int_2d(els, q, nfi, [0, 0, 0], [0, 0, 0], [1, 1, 1], 5, 0.01, xns_b200.XRAY, ff=ff)  # noqa
+    ms, kms, launches, clk = _measure(ctx, call, args.steps, min(args.warmup, 1), 4)
+    terms = n * nq * nfi
+    p64, p32 = _fma_peaks(ctx)
+    line = {"metric": "terms/s", "value": terms / (kms * 1e-3), "unit": "(atom, q-point) terms/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": min(args.warmup, 1), "ms_per_step": kms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 phase, f32 sincos and sums, f64 totals",
+            "data": "synthetic (seeded)", "patterns_per_s": 1e3 / kms,
+            "config": {"workload": "2D polar mesh %dx%d, fcc crystallite %d atoms, X-ray" % (nq, nfi, n), "atoms": n,
+                       "terms_per_step": terms},
+            "roofline": {"kernel": "amp2d_polar_kernel", "bound": "fp64",
+                         "achieved": 10.0 * terms / (kms * 1e-3) / 1e12, "peak": p64, "unit": "TFLOP/s",
+                         "frac": 10.0 * terms / (kms * 1e-3) / 1e12 / p64, "traffic": None,
+                         "flops_per_term": "10 FP64 (phase 6 + quadrant reduction 4)",
+                         "peak_source": "measured in-process (DFMA loop, xns_measure_fma_peak)"},
+            "e2e": {"value": terms / (ms * 1e-3), "unit": "(atom, q-point) terms/s", "ms_per_step": ms,
+                    "h2d_bytes_per_step": n * 24, "d2h_bytes_per_step": nq * nfi * 8 + nq * 8},
+            "gpu_launches": int(launches), "clocks": clk}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as orc
+        cores = os.cpu_count() or 1
+        try:
+            R, kind = orc.Reference(threads=cores), "reference"
+        except FileNotFoundError:
+            R, kind = orc.Oracle(), "port"
+        # the reference parallelises over q rows: one row per core, a 64-point phi mesh (the work per term
+        # does not depend on the mesh)
+        rows, nfi_s = cores, 64
+        t = time.perf_counter()
+        R.int_2d(els, q[:rows], nfi_s, [0, 0, 0], [0, 0, 0], [1, 1, 1], 5, 0.01, xns_b200.XRAY, ff=ff[:, :rows])
+        dt = time.perf_counter() - t
+        line["cpu_baseline"] = {"value": n * rows * nfi_s / dt, "unit": "(atom, q-point) terms/s", "cores": cores,
+                                "kind": kind, "sample": "calcInt2D on %d q rows x %d phi, all %d atoms, %.2f s"
+                                                        % (rows, nfi_s, n, dt)}
+    print(json.dumps(line))
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -343,10 +491,18 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cells", type=int, default=CELLS,
                     help="cube edge in unit cells (default 30, the benchmark; smaller only for profiler captures)")
+    ap.add_argument("--workload", default="histogram", choices=["histogram", "debye", "2d"],
+                    help="histogram (default, the headline: config 2); debye (config 1) and 2d (config 3) run on one GPU")
+    ap.add_argument("--cells2d", type=int, default=63, help="2d workload: crystallite edge in fcc cells (63: 1e6 atoms)")
+    ap.add_argument("--mesh2d", type=int, default=1024, help="2d workload: q and phi points")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == "debye" and args.impl == "ours":
+        return debye_workload(args)
+    if args.workload == "2d" and args.impl == "ours":
+        return twod_workload(args)
     if args.impl == "reference":
         return reference_arm(args, rank, world)
     if world > 1:
