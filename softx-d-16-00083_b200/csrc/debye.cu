@@ -17,7 +17,7 @@ using namespace xns_sinc;
 
 namespace {
 
-constexpr int DB_TI = 32, DB_TJ = 64;
+constexpr int DB_TI = 16, DB_TJ = 96;
 static_assert(DB_TI * DB_TJ == SE_TILE, "tile pair must fill one record tile");
 
 struct AtomPairSrc {
@@ -32,7 +32,7 @@ struct AtomPairSrc {
     return sp[s].cls;
   }
 
-  // stage: 6 * 64 doubles
+  // stage: 3 * (DB_TI + DB_TJ) doubles
   __device__ int fill(unsigned long long w, PairRec *pr, void *stage, double dq) const {
     double *sxi = (double *)stage, *syi = sxi + DB_TI, *szi = syi + DB_TI;
     double *sxj = szi + DB_TI, *syj = sxj + DB_TJ, *szj = syj + DB_TJ;
@@ -49,10 +49,10 @@ struct AtomPairSrc {
       syi[tid] = Y[g.a0 + ib + tid];
       szi[tid] = Z[g.a0 + ib + tid];
     }
-    if (tid >= 64 && tid - 64 < (int)nj) {
-      sxj[tid - 64] = X[g.b0 + jb + tid - 64];
-      syj[tid - 64] = Y[g.b0 + jb + tid - 64];
-      szj[tid - 64] = Z[g.b0 + jb + tid - 64];
+    for (int t = tid - DB_TI; t >= 0 && t < (int)nj; t += SE_THREADS) {
+      sxj[t] = X[g.b0 + jb + t];
+      syj[t] = Y[g.b0 + jb + t];
+      szj[t] = Z[g.b0 + jb + t];
     }
     __syncthreads();
     for (int e = tid; e < SE_TILE; e += SE_THREADS) {

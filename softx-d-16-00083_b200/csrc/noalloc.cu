@@ -85,8 +85,8 @@ int device_setup(int dev, DeviceSetup *out) {
     if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess) return XNS_ERR_CUDA;
     if (major != 10) return XNS_ERR_NODEV;
     if (cudaDeviceGetAttribute(&s.num_sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return XNS_ERR_CUDA;
-    if (prepare<32, false>(&s.per_sm_uniform) != cudaSuccess) return XNS_ERR_CUDA;
-    if (prepare<16, true>(&s.per_sm_direct) != cudaSuccess) return XNS_ERR_CUDA;
+    if (prepare<SE_M_UNIFORM, false>(&s.per_sm_uniform) != cudaSuccess) return XNS_ERR_CUDA;
+    if (prepare<SE_M_DIRECT, true>(&s.per_sm_direct) != cudaSuccess) return XNS_ERR_CUDA;
     s.scratch = (unsigned char *)ptr;
     s.ready = true;
   }
@@ -170,17 +170,17 @@ extern "C" int xns_int_1d_hist_noalloc(const uint64_t *hist_dev, const uint32_t 
   p.ntiles = ntiles;
   p.partial = partial;
   BinSrc src{(const unsigned long long *)hist_dev, nhist, tpp, bin};
-  const int M = uniform ? 32 : 16;
+  const int M = uniform ? SE_M_UNIFORM : SE_M_DIRECT;
   const uint32_t chunks = (nq + M - 1) / M;
   int lanes = 1;
   while (lanes < (int)chunks) lanes <<= 1;
   if (lanes > SE_THREADS) return XNS_ERR_LIMIT;
   if (uniform) {
-    const size_t smem = sizeof(double) * 32 * SE_THREADS + sizeof(PairRec) * SE_TILE;
-    sinc_tiles_kernel<32, false, BinSrc><<<(unsigned)grid, SE_THREADS, smem, s>>>(p, src, lanes);
+    const size_t smem = sizeof(double) * SE_M_UNIFORM * SE_THREADS + sizeof(PairRec) * SE_TILE;
+    sinc_tiles_kernel<SE_M_UNIFORM, false, BinSrc><<<(unsigned)grid, SE_THREADS, smem, s>>>(p, src, lanes);
   } else {
-    const size_t smem = sizeof(double) * 16 * SE_THREADS + sizeof(PairRec) * SE_TILE;
-    sinc_tiles_kernel<16, true, BinSrc><<<(unsigned)grid, SE_THREADS, smem, s>>>(p, src, lanes);
+    const size_t smem = sizeof(double) * SE_M_DIRECT * SE_THREADS + sizeof(PairRec) * SE_TILE;
+    sinc_tiles_kernel<SE_M_DIRECT, true, BinSrc><<<(unsigned)grid, SE_THREADS, smem, s>>>(p, src, lanes);
   }
   if (cudaGetLastError() != cudaSuccess) return XNS_ERR_CUDA;
   sinc_epilogue_kernel<<<(nq + 127) / 128, 128, 0, s>>>(partial, (int)grid, P, nel, 1, 1, tab, tab + P, w, tab + 2 * P, q0, dq,

@@ -12,11 +12,12 @@
 //   d_{k+1} = d_k - lam s_k,  s_{k+1} = s_k + d_{k+1},  lam = 4 sin^2(t/2),
 // which is the Chebyshev recurrence s_{k+1} = 2cos(t) s_k - s_{k-1} with 2cos(t) kept as 2 - lam: lam
 // carries full relative precision even for small t, so the phase does not drift the way a rounded
-// 2cos(t) (error 2^-24 / sin t per step) would on fine q meshes.  Three FP32 instructions per
-// (record, q) term (FFMA, FADD, and the FADD of the sum), no transcendental.  Sums run in FP32 over
-// SE_FP32_PAIRS record pairs and are then added to per-thread FP64 totals in shared memory
-// (compensated block accumulation); CTAs then reduce in FP64 in the epilogue.  1/q_k
-// is applied in the epilogue.  A mesh that is not uniform takes an accurate sine per term (DIRECT).
+// 2cos(t) (error 2^-24 / sin t per step) would on fine q meshes.  A lane runs four records side by
+// side: per (record, q) term one FFMA and one FADD for the sine, plus 3/4 FADD for the pairwise sum of
+// the four, no transcendental.  Sums run in FP32 over SE_FP32_GROUPS groups and are then added to
+// per-thread FP64 totals in shared memory (compensated block accumulation); CTAs then reduce in FP64
+// in the epilogue.  1/q_k is applied in the epilogue.  A mesh that is not uniform takes an accurate
+// sine per term (DIRECT).
 #pragma once
 #include <math.h>
 
@@ -27,13 +28,17 @@
 
 namespace xns_sinc {
 
-constexpr int SE_THREADS = 256;
-constexpr int SE_TILE = 2048;
-// Record pairs a lane sums in FP32 before adding the sums to its FP64 totals.  A lane adds each
-// record's term to a running FP32 sum, so the rounding error grows with the length of that sum; with
-// the large cancellation at the minima of I(q) (sum of |terms| ~10^3 x the result) 8 pairs keep the
-// FP32 summation error within ~3x of the FP32 rounding of the terms themselves.
-constexpr int SE_FP32_PAIRS = 8;
+constexpr int SE_THREADS = 128;
+constexpr int SE_TILE = 1536;
+// q values per lane: M_UNIFORM for the recurrence (a seed costs ~30 instructions, the recurrence 2.75
+// per term), M_DIRECT for the per-term sine of a non-uniform mesh.
+constexpr int SE_M_UNIFORM = 64;
+constexpr int SE_M_DIRECT = 16;
+// Record groups (4 records each) a lane sums in FP32 before adding the sums to its FP64 totals.  A
+// lane adds each group's terms to a running FP32 sum, so the rounding error grows with the length of
+// that sum; with the large cancellation at the minima of I(q) (sum of |terms| ~10^3 x the result) 16
+// records keep the FP32 summation error within ~3x of the FP32 rounding of the terms themselves.
+constexpr int SE_FP32_GROUPS = 4;
 
 struct PairRec {
   double r;      // distance (FP64)
@@ -107,13 +112,14 @@ __global__ void __launch_bounds__(SE_THREADS, 2) sinc_tiles_kernel(SincParams p,
       float blk[M];
 #pragma unroll
       for (int k = 0; k < M; k++) blk[k] = 0.f;
-      int nblk = 0;  // record pairs in blk
-      for (int e = slot; e < n; e += 2 * nslots) {
-        const PairRec A = pr[e];
-        const int e2 = e + nslots;
-        const PairRec B = e2 < n ? pr[e2] : null_rec();
-        if (A.w_r == 0.f && B.w_r == 0.f) continue;
-        if (nblk == SE_FP32_PAIRS) {  // FP32 sums stay short: move them to the FP64 totals
+      int nblk = 0;  // record groups in blk
+      // a lane takes four records per step: e, e + S, e + 2S, e + 3S (S = slots)
+      for (int e = slot; e < n; e += 4 * nslots) {
+        PairRec R[4];
+#pragma unroll
+        for (int g = 0; g < 4; g++) R[g] = e + g * nslots < n ? pr[e + g * nslots] : null_rec();
+        if (R[0].w_r == 0.f && R[1].w_r == 0.f && R[2].w_r == 0.f && R[3].w_r == 0.f) continue;
+        if (nblk == SE_FP32_GROUPS) {  // FP32 sums stay short: move them to the FP64 totals
 #pragma unroll
           for (int k = 0; k < M; k++) {
             acc64[k * SE_THREADS + tid] += (double)blk[k];
@@ -124,24 +130,32 @@ __global__ void __launch_bounds__(SE_THREADS, 2) sinc_tiles_kernel(SincParams p,
         nblk++;
         if (DIRECT) {
 #pragma unroll
-          for (int k = 0; k < M; k++)
-            blk[k] += xns_math::xns_sin(qd[k] * A.r) * A.w_r + xns_math::xns_sin(qd[k] * B.r) * B.w_r;
+          for (int k = 0; k < M; k++) {
+            float t = 0.f;
+#pragma unroll
+            for (int g = 0; g < 4; g++) t += xns_math::xns_sin(qd[k] * R[g].r) * R[g].w_r;
+            blk[k] += t;
+          }
         } else {
           // seeds: s_0 = sin(x), d_0 = s_0 - s_{-1} = 2 sin(t/2) cos(x - t/2) with x = q_{k0} r, t = dq r
-          float sa, csa, sb, csb;
-          xns_math::xns_sincos(qk0 * A.r, &sa, &csa);
-          xns_math::xns_sincos(qk0 * B.r, &sb, &csb);
-          float a = sa * A.w_r, da = A.h2 * fmaf(csa, A.ch, sa * (0.5f * A.h2)) * A.w_r;
-          float b = sb * B.w_r, db = B.h2 * fmaf(csb, B.ch, sb * (0.5f * B.h2)) * B.w_r;
-          const float la = A.lam, lb = B.lam;
-          blk[0] += a + b;
+          float s[4], d[4], lam[4];
+#pragma unroll
+          for (int g = 0; g < 4; g++) {
+            float sx, cx;
+            xns_math::xns_sincos(qk0 * R[g].r, &sx, &cx);
+            s[g] = sx * R[g].w_r;
+            d[g] = R[g].h2 * fmaf(cx, R[g].ch, sx * (0.5f * R[g].h2)) * R[g].w_r;
+            lam[g] = R[g].lam;
+          }
+          blk[0] += (s[0] + s[1]) + (s[2] + s[3]);
 #pragma unroll
           for (int k = 1; k < M; k++) {
-            da = fmaf(-la, a, da);
-            db = fmaf(-lb, b, db);
-            a += da;
-            b += db;
-            blk[k] += a + b;
+#pragma unroll
+            for (int g = 0; g < 4; g++) {
+              d[g] = fmaf(-lam[g], s[g], d[g]);
+              s[g] += d[g];
+            }
+            blk[k] += (s[0] + s[1]) + (s[2] + s[3]);
           }
         }
       }
@@ -198,13 +212,13 @@ int launch_sinc(xns_ctx *ctx, const SincParams &p, const Src &src, int lanes, si
 // Chooses M and the lanes per slot for nq and launches; DIRECT when the mesh is not uniform.
 template <class Src>
 int run_sinc(xns_ctx *ctx, SincParams p, const Src &src, size_t stage_bytes, bool uniform, int *grid_out) {
-  const int M = uniform ? 32 : 16;
+  const int M = uniform ? SE_M_UNIFORM : SE_M_DIRECT;
   const uint32_t chunks = (p.nq + M - 1) / M;
   int lanes = 1;
   while (lanes < (int)chunks) lanes <<= 1;
   if (lanes > SE_THREADS) return xns_fail(ctx, XNS_ERR_ARG, "too many q points for one call");
-  if (uniform) return launch_sinc<32, false>(ctx, p, src, lanes, stage_bytes, grid_out);
-  return launch_sinc<16, true>(ctx, p, src, lanes, stage_bytes, grid_out);
+  if (uniform) return launch_sinc<SE_M_UNIFORM, false>(ctx, p, src, lanes, stage_bytes, grid_out);
+  return launch_sinc<SE_M_DIRECT, true>(ctx, p, src, lanes, stage_bytes, grid_out);
 }
 
 // Uploads pair_a, pair_b, n_el_block and the q mesh for the epilogue and runs it.
