@@ -104,7 +104,13 @@ def test_partial_debye_golden(gpu_ctx):
     g = load_golden("partial__rocksalt_3blocks")
     els = split_elements(g["xyz"], g["n_el"])
     I = gpu_ctx.calc_int_partial_debye(els, g["n_el_block"], g["q"], int(g["source"]), sl=g["sl"])
-    assert rel_err(I, g["I"]) < TOL_I
+    nq = len(g["q"])
+    rows, want = I.reshape(-1, nq), g["I"].reshape(-1, nq)
+    assert rel_err(rows[0], want[0]) < TOL_I  # the total
+    # the parts: a cross-block part oscillates around zero, so its error is measured against 1 % of the
+    # row's median magnitude where the part itself is smaller
+    for r, w in zip(rows[1:], want[1:]):
+        assert rel_err_floor(r, w, FLOOR_2D) < TOL_I
 
 
 @pytest.mark.parametrize("name", golden_names("pdf"))
