@@ -147,6 +147,26 @@ int xns_int_1d_hist_noalloc(const uint64_t *hist_dev, const uint32_t *n_el, uint
                             const double *q, uint32_t nq, int source, const double *const *ff, const double *sl, int polar,
                             double lambda, double *I_dev, void *stream);
 
+/* ---- split-precision tensor-core transform -------------------------------------------------------- */
+
+/* The histogram -> I(q) contraction of calcInt1DHist (CalcFunctions.cpp:855-864) for ncols histogram
+ * columns at once, on the tensor cores in split-BF16 (3 products, FP32 accumulation, FP64 cross-CTA
+ * sums):  G[c*nq + i] = sum_k hist[c*nh + k] * sin(q_i r_k) / (q_i r_k),  r_k = (k + 0.5) * bin.
+ * No weights, no self term and no 1/N: the column-level kernel the batched entry points build on.
+ * Relative error of G against FP64 below 1e-4 (typically 1e-5).  The sinc matrix is cached in the
+ * context for the last (q mesh, bin, nh / 64) and rebuilt when they change. */
+int xns_hist_transform_bf16x3(xns_ctx *ctx, const uint64_t *hist, uint32_t ncols, uint32_t nh, double bin,
+                              const double *q, uint32_t nq, double *G);
+
+/* The same G with exact accumulation on the BF16 tensor cores: the sinc matrix (FP64, with the
+ * reference's +1e-8 in the denominator) as four base-256 integer digits, the counts as two or three
+ * base-256 digits, all digit products summed exactly (integers below 2^24 in the FP32 accumulator,
+ * flushed to FP64 every 128 bins).  G carries the FP64 sinc's error plus < 2.4e-10 per matrix
+ * element, so I(q) stays within 1e-5 of FP64 even at the deep minima of small particles, where the
+ * FP32-accumulated bf16x3 form loses precision.  Counts below 2^24 (XNS_ERR_LIMIT beyond). */
+int xns_hist_transform_exact(xns_ctx *ctx, const uint64_t *hist, uint32_t ncols, uint32_t nh, double bin,
+                             const double *q, uint32_t nq, double *G);
+
 /* ---- utilities (no reference counterpart) -------------------------------------------------------- */
 
 /* Measured FMA-pipe throughput of this device in TFLOP/s (an FMA counts 2 flops): FP64 when fp64 != 0,

@@ -175,13 +175,13 @@ __global__ void __launch_bounds__(SE_THREADS, 2) sinc_tiles_kernel(SincParams p,
 // Reduction of the per-CTA FP64 partial sums plus the calc-function epilogue: 1/q, weights, self
 // term, 1/Ntot, polarisation factor and the sum over parts (CalcFunctions.cpp:592-625 and 733-755 for
 // the Debye sums, :872-906 for the histogram transform).  Classes are part * P + t.
-// out: [total | parts] when nparts > 1, else [total].
+// out: [total | parts] when nparts > 1, else [total].  over_q: the partial sums still need the 1/q.
 __global__ void sinc_epilogue_kernel(const double *__restrict__ partial, int grid, uint32_t ncls, uint32_t nel,
                                      uint32_t nparts, uint32_t nblocks, const uint32_t *__restrict__ pair_a,
                                      const uint32_t *__restrict__ pair_b, const double *__restrict__ w,
                                      const uint32_t *__restrict__ n_el_block, double q0, double dq,
                                      const double *__restrict__ qmesh, uint32_t nq, uint32_t ntot, int polar, double lambda,
-                                     double *__restrict__ out);
+                                     int over_q, double *__restrict__ out);
 
 // Launches sinc_tiles_kernel with the persistent grid and zeroed partial sums; returns the status
 // and the grid size used.
@@ -221,10 +221,12 @@ int run_sinc(xns_ctx *ctx, SincParams p, const Src &src, size_t stage_bytes, boo
   return launch_sinc<SE_M_DIRECT, true>(ctx, p, src, lanes, stage_bytes, grid_out);
 }
 
-// Uploads pair_a, pair_b, n_el_block and the q mesh for the epilogue and runs it.
+// Uploads pair_a, pair_b, n_el_block and the q mesh for the epilogue and runs it.  partial: grid x ncls
+// x nq sums (null: the engine's per-CTA partials); over_q: the sums are sum w sin(q r)/r and still
+// need the 1/q (the engine's), otherwise they are already sum w sin(q r)/(q r + 1e-8).
 int sinc_epilogue(xns_ctx *ctx, int grid, uint32_t ncls, uint32_t nel, uint32_t nblocks, const uint32_t *n_el_block,
                   const double *q, uint32_t nq, bool uniform, double q0, double dq, const double *d_w, uint32_t ntot,
-                  int polar, double lambda, double *d_out);
+                  int polar, double lambda, double *d_out, const double *partial = nullptr, bool over_q = true);
 // The q mesh as a device array (valid until the next call on the context).
 int sinc_upload_q(xns_ctx *ctx, const double *q, uint32_t nq, const double **d_q);
 

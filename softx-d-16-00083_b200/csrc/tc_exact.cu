@@ -1,0 +1,430 @@
+// Exact-accumulation sinc transform on the BF16 tensor cores: integer digits (tcgen05 kind::f16).
+//
+//   G[c][q] = sum_k n_c[k] * sin(q r_k) / (q r_k + 1e-8),   r_k = (k + 0.5) * bin
+//
+// (the calcInt1DHist contraction, CalcFunctions.cpp:855-864).  The split-BF16 transform (tc_gemm.cu)
+// accumulates real products in FP32, and its rounding grows with the running sum; at the low-q minima
+// of a small particle's I(q) that sum is 1e5-1e6 times the result, which puts the error above 1e-4 of
+// I(q).  Here both operands are written as small integers, which BF16 holds exactly (|x| <= 256):
+//   S[q][k] = sum_{i<4}  d_i / (128 * 256^i),  d_i in [-128, 128]  (S in FP64; residual < 2.4e-10)
+//   n[k]    = sum_{j<NH} e_j * 256^j,          e_j in [0, 255]     (counts < 2^(8 NH), exact)
+//   G       = sum_{i,j} 256^(j-i) / 128 * (d_i . e_j)
+// A product of digits is an integer below 2^15 and a level v = j - i gains at most 3 of them per k,
+// so over a chunk of CH_K = 128 k every partial sum is an integer below 2^24 and the FP32 tensor-memory
+// accumulator holds it exactly.  All 4*NH digit products are kept; products of one level share one
+// accumulator (4 + NH - 1 levels of 64 columns), and every chunk the accumulators are read, combined
+// in FP64 (Horner over the levels, exact: below 2^53) and added to per-thread FP64 sums, which go to
+// the output with FP64 atomics when the CTA's part of an output tile ends.
+//
+// Tile 128 q x 64 columns x 64 k, one CTA per SM, 2 stages of {4 S-digit tiles, NH count-digit
+// tiles}; warp 0 loads (cp.async.bulk), warp 1 issues the MMAs, warps 2-9 drain tensor memory (two
+// warps per 32-lane quarter, 32 columns each).  Waits are bounded as in tc_gemm.cu.
+#include <algorithm>
+
+#include "tc_gemm.cuh"
+#include "tc_ptx.cuh"
+
+using namespace xns_ptx;
+
+namespace {
+
+constexpr int XM = 128, XN = 64, XK = 64;  // tile: q rows, columns, k (one 128-byte swizzle row of BF16)
+constexpr int NDS = 4;                     // digits of the sinc matrix
+constexpr int XA = XM * XK * 2;            // 16 KB per S-digit tile
+constexpr int XB = XN * XK * 2;            // 8 KB per count-digit tile
+constexpr int XSTAGES = 2;
+constexpr int CH_TILES = 2;                // k tiles per exact chunk (CH_K = 128)
+constexpr int XTHREADS = 320;
+constexpr uint32_t XTMEM_COLS = 512;
+
+template <int NH>
+struct Exact {
+  static constexpr int NL = NDS + NH - 1;  // levels NH-1 .. -(NDS-1)
+  static constexpr int STAGE = NDS * XA + NH * XB;
+  static constexpr int SMEM = XSTAGES * STAGE + 1024;
+  static_assert(NL * XN <= (int)XTMEM_COLS, "levels must fit in tensor memory");
+};
+
+struct XArgs {
+  const uint8_t *A;  // NDS digit planes of MT*KT tiles, plane stride a_plane bytes
+  const uint8_t *B;  // NH digit planes of NT*KT tiles, plane stride b_plane bytes
+  size_t a_plane, b_plane;
+  uint32_t MT, NT, KT;
+  double *out;
+  uint32_t ldo, m_valid, n_valid;
+  int *err;
+};
+
+template <int NH>
+__global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) {
+  using E = Exact<NH>;
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ __align__(8) unsigned long long bars[2 * XSTAGES + 3];
+  __shared__ uint32_t tmem_sh;
+  __shared__ int abort_sh;
+  const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
+  const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[XSTAGES]);
+  const uint32_t tfull = smem_u32(&bars[2 * XSTAGES]), tempty = smem_u32(&bars[2 * XSTAGES + 1]);
+  const uint32_t drain = smem_u32(&bars[2 * XSTAGES + 2]);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  volatile int *abort = &abort_sh;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < XSTAGES; s++) {
+      mbar_init(full0 + 8 * s, 1);
+      mbar_init(empty0 + 8 * s, 1);
+    }
+    mbar_init(tfull, 1);
+    mbar_init(tempty, XTHREADS - 64);
+    mbar_init(drain, 1);
+    abort_sh = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_sh)),
+                 "r"(XTMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_sh;
+
+  const unsigned long long KT = g.KT;
+  const unsigned long long units = (unsigned long long)g.NT * g.MT * KT;
+  const unsigned long long u0 = units * blockIdx.x / gridDim.x, u1 = units * (blockIdx.x + 1) / gridDim.x;
+
+  if (warp == 0) {
+    if (lane == 0) {  // loader
+      uint32_t fills[XSTAGES] = {};
+      unsigned long long i = 0;
+      for (unsigned long long u = u0; u < u1; ++u, ++i) {
+        const uint32_t s = (uint32_t)(i % XSTAGES), k = (uint32_t)(i / XSTAGES);
+        if (k > 0 && !mbar_wait(empty0 + 8 * s, (k - 1) & 1u, abort, WAIT_LIMIT_NS)) {
+          abort_sh = 1;
+          atomicOr(g.err, 1);
+          break;
+        }
+        const uint32_t kt = (uint32_t)(u % KT);
+        const unsigned long long r = u / KT;
+        const uint32_t mt = (uint32_t)(r % g.MT), nt = (uint32_t)(r / g.MT);
+        const uint32_t dst = base + s * E::STAGE, bar = full0 + 8 * s;
+        const size_t ao = ((size_t)mt * g.KT + kt) * XA, bo = ((size_t)nt * g.KT + kt) * XB;
+        mbar_expect_tx(bar, (uint32_t)E::STAGE);
+#pragma unroll
+        for (int d = 0; d < NDS; d++) bulk_g2s(dst + d * XA, g.A + d * g.a_plane + ao, XA, bar);
+#pragma unroll
+        for (int e = 0; e < NH; e++) bulk_g2s(dst + NDS * XA + e * XB, g.B + e * g.b_plane + bo, XB, bar);
+        fills[s] = k + 1;
+      }
+      if (*abort)
+        for (int s = 0; s < XSTAGES; s++)
+          if (fills[s]) mbar_wait(full0 + 8 * s, (fills[s] - 1) & 1u, nullptr, DRAIN_LIMIT_NS);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {  // MMA issuer
+      // kind::f16: F32 accumulator (1), BF16 A and B (1, 1), K-major, N = 64, M = 128
+      const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(XN >> 3) << 17) | ((uint32_t)(XM >> 4) << 24);
+      uint32_t chunk = 0;  // chunks handed to the drain warps so far
+      bool issued = false;
+      unsigned long long i = 0;
+      uint32_t in_chunk = 0;
+      for (unsigned long long u = u0; u < u1; ++u, ++i) {
+        const uint32_t s = (uint32_t)(i % XSTAGES), k = (uint32_t)(i / XSTAGES);
+        const bool seg_first = (u == u0) || (u % KT == 0);
+        const bool seg_last = (u + 1 == u1) || ((u + 1) % KT == 0);
+        const bool first = seg_first || in_chunk == 0;
+        if (first && chunk > 0) {  // the drain warps have read the previous chunk
+          if (!mbar_wait(tempty, (chunk - 1) & 1u, abort, WAIT_LIMIT_NS)) {
+            abort_sh = 1;
+            atomicOr(g.err, 1);
+            break;
+          }
+          tc_fence_after();
+        }
+        if (!mbar_wait(full0 + 8 * s, k & 1u, abort, WAIT_LIMIT_NS)) {
+          abort_sh = 1;
+          atomicOr(g.err, 1);
+          break;
+        }
+        tc_fence_after();
+        const uint32_t a0 = base + s * E::STAGE, b0 = a0 + NDS * XA;
+#pragma unroll
+        for (int ks = 0; ks < XK / 16; ks++) {
+          const uint32_t off = ks * 32;
+          uint32_t written = 0;
+#pragma unroll
+          for (int di = 0; di < NDS; di++) {
+#pragma unroll
+            for (int ej = 0; ej < NH; ej++) {
+              const int lev = (NH - 1) - (ej - di);  // 0 = top level
+              const uint32_t acc = (first && ks == 0 && !(written & (1u << lev))) ? 0u : 1u;
+              written |= 1u << lev;
+              tc_mma(tmem + lev * XN, sw128_desc(a0 + di * XA + off), sw128_desc(b0 + ej * XB + off), idesc, acc);
+            }
+          }
+        }
+        issued = true;
+        tc_commit(empty0 + 8 * s);
+        in_chunk++;
+        if (seg_last || in_chunk == CH_TILES) {
+          tc_commit(tfull);
+          chunk++;
+          in_chunk = 0;
+        }
+      }
+      if (*abort && issued) {
+        tc_commit(drain);
+        mbar_wait(drain, 0, nullptr, DRAIN_LIMIT_NS);
+      }
+    }
+  } else {  // drain: warp w reads TMEM lanes 32*(w%4) .. +31, columns 32*h .. +31
+    const uint32_t wq = warp & 3, h = (uint32_t)(warp - 2) >> 2;
+    const uint32_t lane_addr = tmem + ((wq * 32u) << 16) + h * 32u;
+    double sum[32];
+#pragma unroll
+    for (int j = 0; j < 32; j++) sum[j] = 0.0;
+    uint32_t chunk = 0, in_chunk = 0;
+    for (unsigned long long u = u0; u < u1; ++u) {
+      const bool seg_last = (u + 1 == u1) || ((u + 1) % KT == 0);
+      in_chunk++;
+      if (!(seg_last || in_chunk == CH_TILES)) continue;
+      in_chunk = 0;
+      const bool ok = mbar_wait(tfull, chunk & 1u, abort, WAIT_LIMIT_NS);
+      if (__any_sync(0xffffffffu, !ok)) {
+        abort_sh = 1;
+        if (lane == 0) atomicOr(g.err, 1);
+        break;
+      }
+      tc_fence_after();
+#pragma unroll
+      for (int c = 0; c < 32; c += 16) {
+        double t[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++) t[j] = 0.0;
+#pragma unroll
+        for (int lev = 0; lev < E::NL; lev++) {  // Horner over the levels, top first
+          uint32_t rr[16];
+          tc_ld16_raw(lane_addr + lev * XN + c, rr);
+#pragma unroll
+          for (int j = 0; j < 16; j++) t[j] = t[j] * 256.0 + (double)__uint_as_float(rr[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 16; j++) sum[c + j] += t[j];
+      }
+      tc_fence_before();
+      mbar_arrive(tempty);
+      chunk++;
+      if (seg_last) {
+        const unsigned long long r = u / KT;
+        const uint32_t mt = (uint32_t)(r % g.MT), nt = (uint32_t)(r / g.MT);
+        const uint32_t m = mt * XM + wq * 32 + lane;
+        // level l holds 256^(NH-1-l)/128; Horner gave 256^(NL-1-l): scale 256^(NH-NL)/128
+        const double scale = 1.0 / (128.0 * 16777216.0);  // NL - NH = NDS - 1 = 3 -> 256^-3
+        if (m < g.m_valid) {
+#pragma unroll
+          for (int j = 0; j < 32; j++) {
+            const uint32_t n = nt * XN + h * 32 + j;
+            if (n < g.n_valid) atomicAdd(g.out + (size_t)n * g.ldo + m, sum[j] * scale);
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < 32; j++) sum[j] = 0.0;
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(XTMEM_COLS) : "memory");
+}
+
+// Byte offset of the 16-byte chunk ch of row `row` in a K-major 128-byte-swizzled tile.
+__device__ __forceinline__ uint32_t chunk_offset(uint32_t row, uint32_t ch) {
+  return (row >> 3) * 1024u + (row & 7u) * 128u + (((ch ^ row) & 7u) << 4);
+}
+
+__device__ __forceinline__ uint4 pack8(const float *v) {
+  __align__(16) __nv_bfloat16 b[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) b[i] = __float2bfloat16_rn(v[i]);  // integers |v| <= 256: exact
+  return *(const uint4 *)b;
+}
+
+// One CTA of 128 threads per (mt, kt) tile; a thread makes the 64 k of one row.  sin(x_k) comes from
+// one FP64 sincos at the row's first bin and the rotation by delta = q * bin (4 FMAs per bin; the
+// drift over 64 bins is ~1e-14, far below the 2.4e-10 digit residual).
+__global__ void pack_sinc_digits_kernel(const double *__restrict__ q, uint32_t nq, double bin, uint32_t nh, uint32_t KT,
+                                        uint8_t *__restrict__ A, size_t a_plane) {
+  const uint32_t tile = blockIdx.x, mt = tile / KT, kt = tile % KT;
+  const uint32_t row = threadIdx.x, m = mt * XM + row, kbase = kt * XK;
+  const double qm = m < nq ? q[m] : 0.0;
+  double s, c, sd, cd;
+  sincos(((kbase + 0.5) * bin) * qm, &s, &c);
+  sincos(bin * qm, &sd, &cd);
+  for (uint32_t ch = 0; ch < XK / 8; ch++) {
+    float dig[NDS][8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const uint32_t k = kbase + ch * 8 + i;
+      double v = 0.0;
+      if (m < nq && k < nh) {
+        const double x = ((k + 0.5) * bin) * qm;  // qrij = rij * q[iq] (CalcFunctions.cpp:858-861)
+        v = s / (x + 0.00000001);
+      }
+      double r = v * 128.0;
+#pragma unroll
+      for (int d = 0; d < NDS; d++) {
+        const double di = rint(r);
+        dig[d][i] = (float)di;
+        r = (r - di) * 256.0;
+      }
+      const double s1 = __fma_rn(s, cd, c * sd), c1 = __fma_rn(c, cd, -(s * sd));
+      s = s1;
+      c = c1;
+    }
+    const size_t off = (size_t)tile * XA + chunk_offset(row, ch);
+#pragma unroll
+    for (int d = 0; d < NDS; d++) *(uint4 *)(A + d * a_plane + off) = pack8(dig[d]);
+  }
+}
+
+// One CTA per (nt, kt) tile of XN rows (histogram columns).  Sets *overflow when a count needs more
+// than NH digits.
+template <int NH>
+__global__ void pack_count_digits_kernel(const unsigned long long *__restrict__ hist, uint32_t ncols, uint32_t nh,
+                                         size_t ldh, uint32_t KT, uint8_t *__restrict__ B, size_t b_plane,
+                                         int *overflow) {
+  const uint32_t tile = blockIdx.x, nt = tile / KT, kt = tile % KT;
+  for (uint32_t c = threadIdx.x; c < XN * 8; c += blockDim.x) {
+    const uint32_t row = c >> 3, ch = c & 7, n = nt * XN + row, k0 = kt * XK + ch * 8;
+    float dig[NH][8];
+    bool big = false;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const uint32_t k = k0 + i;
+      const unsigned long long v = (n < ncols && k < nh) ? hist[(size_t)n * ldh + k] : 0ull;
+      big |= (v >> (8 * NH)) != 0;
+#pragma unroll
+      for (int e = 0; e < NH; e++) dig[e][i] = (float)((v >> (8 * e)) & 255u);
+    }
+    if (big) atomicOr(overflow, 1);
+    const size_t off = (size_t)tile * XB + chunk_offset(row, ch);
+#pragma unroll
+    for (int e = 0; e < NH; e++) *(uint4 *)(B + e * b_plane + off) = pack8(dig[e]);
+  }
+}
+
+__global__ void max_count_kernel(const unsigned long long *__restrict__ hist, uint32_t ncols, uint32_t nh, size_t ldh,
+                                 unsigned long long *out) {
+  unsigned long long m = 0;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < (size_t)ncols * nh; t += (size_t)gridDim.x * blockDim.x)
+    m = max(m, hist[(t / nh) * ldh + t % nh]);
+  for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
+template <int NH>
+int run_exact(xns_ctx *ctx, const unsigned long long *d_hist, uint32_t ncols, uint32_t nh, size_t ldh, uint32_t MT,
+              uint32_t KT, const uint8_t *A, size_t a_plane, double *d_G, uint32_t nq, int *flags) {
+  using E = Exact<NH>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    XNS_CUDA(ctx, cudaFuncSetAttribute(sinc_exact_kernel<NH>, cudaFuncAttributeMaxDynamicSharedMemorySize, E::SMEM));
+    attr_set = true;
+  }
+  int st;
+  const uint32_t NT = (ncols + XN - 1) / XN;
+  const size_t b_plane = (size_t)NT * KT * XB;
+  void *B;
+  if ((st = xns_scratch(ctx, SLOT_TC_B, NH * b_plane, &B))) return st;
+  pack_count_digits_kernel<NH><<<NT * KT, 256, 0, ctx->stream>>>(d_hist, ncols, nh, ldh, KT, (uint8_t *)B, b_plane,
+                                                                  flags + 1);
+  XNS_LAUNCHED(ctx);
+  XArgs g{};
+  g.A = A;
+  g.B = (const uint8_t *)B;
+  g.a_plane = a_plane;
+  g.b_plane = b_plane;
+  g.MT = MT;
+  g.NT = NT;
+  g.KT = KT;
+  g.out = d_G;
+  g.ldo = nq;
+  g.m_valid = nq;
+  g.n_valid = ncols;
+  g.err = flags;
+  const unsigned long long units = (unsigned long long)NT * MT * KT;
+  const unsigned grid = (unsigned)std::min<unsigned long long>((unsigned long long)ctx->num_sms, units);
+  sinc_exact_kernel<NH><<<grid, XTHREADS, E::SMEM, ctx->stream>>>(g);
+  XNS_LAUNCHED(ctx);
+  return XNS_OK;
+}
+
+}  // namespace
+
+int xns_tc_hist_transform_exact(xns_ctx *ctx, const unsigned long long *d_hist, uint32_t ncols, uint32_t nh, size_t ldh,
+                                double bin, const double *q, uint32_t nq, double *d_G) {
+  if (!ncols || !nq) return XNS_OK;
+  const uint32_t MT = (nq + XM - 1) / XM, KT = (nh + XK - 1) / XK;
+  int st;
+  void *flags;
+  if ((st = xns_scratch(ctx, SLOT_FLAGS, 64, &flags))) return st;
+  XNS_CUDA(ctx, cudaMemsetAsync(flags, 0, 16, ctx->stream));
+  // the largest count picks the number of count digits (one small read-back)
+  unsigned long long *d_max = (unsigned long long *)((char *)flags + 8);
+  max_count_kernel<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(d_hist, ncols, nh, ldh, d_max);
+  XNS_LAUNCHED(ctx);
+  unsigned long long maxc = 0;
+  XNS_CUDA(ctx, cudaMemcpyAsync(&maxc, d_max, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (maxc >> 24) return xns_fail(ctx, XNS_ERR_LIMIT, "exact transform: a bin count reaches 2^24");
+  // sinc digits: rebuilt only when the q mesh, the bin width or the K extent change
+  const size_t a_plane = (size_t)MT * KT * XA;
+  void *A;
+  const bool same = ctx->x_bin == bin && ctx->x_kt == KT && ctx->x_q.size() == nq &&
+                    std::equal(q, q + nq, ctx->x_q.begin()) && ctx->slot_size[SLOT_X_A] >= NDS * a_plane;
+  if ((st = xns_scratch(ctx, SLOT_X_A, NDS * a_plane, &A))) return st;
+  if (!same) {
+    void *dq;
+    if ((st = xns_scratch(ctx, SLOT_QMESH, sizeof(double) * nq, &dq))) return st;
+    XNS_CUDA(ctx, cudaMemcpyAsync(dq, q, sizeof(double) * nq, cudaMemcpyHostToDevice, ctx->stream));
+    pack_sinc_digits_kernel<<<MT * KT, XM, 0, ctx->stream>>>((const double *)dq, nq, bin, nh, KT, (uint8_t *)A, a_plane);
+    XNS_LAUNCHED(ctx);
+    ctx->x_q.assign(q, q + nq);
+    ctx->x_bin = bin;
+    ctx->x_kt = KT;
+  }
+  XNS_CUDA(ctx, cudaMemsetAsync(d_G, 0, sizeof(double) * ncols * nq, ctx->stream));
+  st = (maxc >> 16) ? run_exact<3>(ctx, d_hist, ncols, nh, ldh, MT, KT, (const uint8_t *)A, a_plane, d_G, nq, (int *)flags)
+                    : run_exact<2>(ctx, d_hist, ncols, nh, ldh, MT, KT, (const uint8_t *)A, a_plane, d_G, nq, (int *)flags);
+  if (st) return st;
+  int err[2] = {0, 0};
+  XNS_CUDA(ctx, cudaMemcpyAsync(err, flags, sizeof(err), cudaMemcpyDeviceToHost, ctx->stream));
+  XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (err[0]) return xns_fail(ctx, XNS_ERR_CUDA, "exact transform: a pipeline wait ran out of time");
+  if (err[1]) return xns_fail(ctx, XNS_ERR_LIMIT, "exact transform: a bin count exceeds the digit range");
+  return XNS_OK;
+}
+
+// Host-buffer entry: as xns_hist_transform_bf16x3, with exact digit accumulation.
+extern "C" int xns_hist_transform_exact(xns_ctx *ctx, const uint64_t *hist, uint32_t ncols, uint32_t nh, double bin,
+                                        const double *q, uint32_t nq, double *G) {
+  if (!ctx) return XNS_ERR_ARG;
+  if (!hist || !q || !G || !ncols || !nh || !nq) return xns_fail(ctx, XNS_ERR_ARG, "transform: null or empty argument");
+  int st;
+  void *dh, *dG;
+  if ((st = xns_scratch(ctx, SLOT_HIST, sizeof(uint64_t) * ncols * nh, &dh))) return st;
+  if ((st = xns_scratch(ctx, SLOT_TC_OUT, sizeof(double) * ncols * nq, &dG))) return st;
+  XNS_CUDA(ctx, cudaMemcpyAsync(dh, hist, sizeof(uint64_t) * ncols * nh, cudaMemcpyHostToDevice, ctx->stream));
+  if ((st = xns_timer_start(ctx))) return st;
+  if ((st = xns_stage_begin(ctx, STAGE_IQ))) return st;
+  if ((st = xns_tc_hist_transform_exact(ctx, (const unsigned long long *)dh, ncols, nh, nh, bin, q, nq, (double *)dG)))
+    return st;
+  if ((st = xns_stage_end(ctx, STAGE_IQ))) return st;
+  if ((st = xns_timer_stop(ctx))) return st;
+  XNS_CUDA(ctx, cudaMemcpyAsync(G, dG, sizeof(double) * ncols * nq, cudaMemcpyDeviceToHost, ctx->stream));
+  XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return XNS_OK;
+}

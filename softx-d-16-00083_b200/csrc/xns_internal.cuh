@@ -28,6 +28,12 @@ enum ScratchSlot {
   SLOT_HTILE,           // histogram plan: tiles (atom ranges with bounding boxes)
   SLOT_HLIST,           // histogram plan: tile pairs sorted by (element pair, distance bucket)
   SLOT_HKEY,            // histogram plan: bucket counts / offsets and small tables
+  SLOT_TC_A,            // split-BF16 sinc matrix (hi and lo planes, tensor-core tile order)
+  SLOT_TC_B,            // split-BF16 histogram columns (hi and lo planes)
+  SLOT_TC_OUT,          // FP64 sinc-transform output (columns x q)
+  SLOT_X_A,             // integer-digit planes of the sinc matrix (exact transform)
+  SLOT_BATCH,           // batched ensemble: coordinates, schedules and per-structure tables
+  SLOT_BATCH_HIST,      // batched ensemble: histograms
   SLOT_COUNT
 };
 
@@ -49,6 +55,14 @@ struct xns_ctx {
   size_t slot_size[SLOT_COUNT] = {};
   void *pinned = nullptr;  // pinned host staging
   size_t pinned_size = 0;
+  // the sinc matrix held in SLOT_TC_A was built for this q mesh, bin width and K extent
+  std::vector<double> tc_q;
+  double tc_bin = 0;
+  uint32_t tc_kt = 0;
+  // the same for the integer-digit sinc planes in SLOT_X_A
+  std::vector<double> x_q;
+  double x_bin = 0;
+  uint32_t x_kt = 0;
 };
 
 // One entry of the tile-pair schedule: atoms [a0, a0+na) against [b0, b0+nb) of the SoA arrays.

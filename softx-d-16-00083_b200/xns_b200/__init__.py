@@ -59,6 +59,8 @@ lib.xns_calc_pdf_and_debye.argtypes = [_p, _PP, _p, _u32, _u32, _dbl, _int, _int
 lib.xns_calc_int_debye.argtypes = [_p, _PP, _p, _u32, _p, _u32, _int, _PP, _p, _int, _dbl, _p]
 lib.xns_calc_int_partial_debye.argtypes = [_p, _PP, _p, _u32, _u32, _p, _p, _u32, _int, _PP, _p, _int, _dbl, _p]
 lib.xns_calc_int_2d.argtypes = [_p, _PP, _p, _u32, _p, _u32, _u32, _p, _p, _p, _u32, _dbl, _int, _PP, _p, _int, _p, _p]
+lib.xns_hist_transform_bf16x3.argtypes = [_p, _p, _u32, _u32, _dbl, _p, _u32, _p]
+lib.xns_hist_transform_exact.argtypes = [_p, _p, _u32, _u32, _dbl, _p, _u32, _p]
 
 
 def _ptr(a):
@@ -157,6 +159,16 @@ class Context:
         self._check(lib.xns_calc_pdf(self._h, _ptr(hist), _ptr(n_el), len(n_el), nhist, bin, pdftype, p0, _ptr(sl),
                                      _ptr(out)))
         return out
+
+    def hist_transform(self, hist, bin, q, scheme="exact"):
+        """G[c, i] = sum_k hist[c, k] sin(q_i r_k)/(q_i r_k) on the tensor cores: scheme "bf16x3" (split
+        BF16, FP32 accumulation) or "exact" (integer digits, exact accumulation)."""
+        hist = np.ascontiguousarray(np.atleast_2d(hist), dtype=np.uint64)
+        q = _f64(q)
+        G = np.zeros((hist.shape[0], len(q)))
+        fn = {"bf16x3": lib.xns_hist_transform_bf16x3, "exact": lib.xns_hist_transform_exact}[scheme]
+        self._check(fn(self._h, _ptr(hist), hist.shape[0], hist.shape[1], bin, _ptr(q), len(q), _ptr(G)))
+        return G
 
     def calc_pdf_and_debye(self, elements, nhist, bin, scenario, pdftype, p0, q, source, ff=None, sl=None, polar=False,
                            lam=0.0, want_hist=False):
