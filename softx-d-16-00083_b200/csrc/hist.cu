@@ -1,23 +1,28 @@
 // Pair-distance histogram (replaces calcHist, CalcFunctions.cpp:757-809, and calcHistKernel,
-// CalcFunctionsCUDA.cu:814-920).
+// CalcFunctionsCUDA.cu:814-920), for one structure or a set of independent structures at once.
 //
-// Counts are bit-identical to the reference's (exact FP64 bin decision, hist_bin.cuh).  At the
-// reference's 0.001 A bins a 2e5-atom structure has ~3e5 bins per element pair: far more than a shared
-// memory histogram holds, and one global atomic per pair leaves the kernel bound by L2 atomics.  So
-// the pairs are ordered by distance first:
+// Counts are bit-identical to the reference's.  At the reference's 0.001 A bins a 2e5-atom structure
+// has ~3e5 bins per element pair: far more than a shared-memory histogram holds, and one global atomic
+// per pair leaves the kernel bound by L2 atomics.  So the pairs are ordered by distance first:
 //   1. atoms of each element are counting-sorted into cubic cells of ~CELL_TARGET atoms
-//      (cell_count / cell_scan / cell_scatter kernels); each cell is cut into tiles of <= 64 atoms
-//      with a bounding box (tile_build / tile_bbox);
-//   2. every tile pair (upper triangle within an element, all pairs across elements) gets the bin
-//      range [kmin, kmax] its bounding boxes allow, and is counting-sorted by (element pair,
-//      kmin / BUCKET) (pair_key / key_scan / pair_scatter);
-//   3. hist_window_kernel: one CTA per SM walks a contiguous run of that list, one tile pair per warp,
-//      and counts into a WIN-bin u32 window of shared memory that slides up the distance axis (bins
-//      that leave the window are added to the u64 global histogram once per CTA);
+//      (cell_count / scan / cell_scatter kernels); each cell is cut into tiles of <= 64 atoms with a
+//      bounding box (tile_build / tile_bbox);
+//   2. every tile pair (upper triangle within an element, all pairs across elements of the same
+//      structure) gets the bin range [kmin, kmax] its bounding boxes allow, and is counting-sorted by
+//      (class, kmin / BUCKET), a class being one element pair of one structure (pair_key / scan /
+//      pair_scatter);
+//   3. the sorted list is cut into runs of one class; hist_window_kernel is persistent (one CTA per
+//      SM) and takes runs from a work queue, largest first, one tile pair per warp, counting into a
+//      WIN-bin u32 window of shared memory that slides up the distance axis (bins that leave the
+//      window are added to the u64 global histogram once per run);
 //   4. hist_wide_kernel: tile pairs whose range is wider than the window (sparse elements) count
 //      straight into the global histogram.
-// Atom order inside a cell and list order inside a bucket come from atomics, but counts do not depend
-// on either.
+//
+// Bin decision, per pair: an FP32 estimate of r/bin from tile-local offsets, with a proven error bound
+// (count_tile_pair_t); pairs whose estimate lies within that bound of a bin edge (about 9 % at 0.001 A
+// bins and 1e5-bin distances), or near the last bin, are queued in per-lane rings and binned exactly
+// with FP64 in the reference's operation order (hist_bin.cuh).  Atom order inside a cell and list order
+// inside a bucket come from atomics, but counts do not depend on either.
 #include <math.h>
 #include <string.h>
 
@@ -25,6 +30,7 @@
 #include <cmath>
 
 #include "hist_bin.cuh"
+#include "hist_set.cuh"
 #include "schedule.cuh"
 
 using namespace xns_hist;
@@ -36,9 +42,12 @@ constexpr int TILE_MAX = 64;         // atoms per tile
 constexpr int MAX_CELLS_AXIS = 256;
 constexpr int HW_WARPS = 16;
 constexpr int HW_THREADS = 32 * HW_WARPS;
-constexpr uint32_t WIN = 50 * 1024;  // window bins
+constexpr uint32_t WIN = 39 * 1024;  // window bins
 constexpr uint32_t BUCKET = 1024;    // distance bucket of the tile-pair sort, in bins
 constexpr int SCAN_THREADS = 1024;
+constexpr int RING = 256;            // deferred pairs per warp: 8 per lane (u16 entries i << 6 | j)
+// per warp: FP64 I and J tiles, FP32 I-tile offsets, the rings (bytes)
+constexpr int WARP_STAGE = 2 * 3 * TILE_MAX * 8 + 3 * TILE_MAX * 4 + RING * 2;
 
 struct Tile {
   uint32_t start, count, elem, pad;
@@ -55,6 +64,11 @@ struct ElemGrid {
 };
 struct CtaRange {
   uint32_t begin, end, type, pad;
+};
+// Class of an element's pairs: structure's first class, element index within the structure, the
+// structure's element count.
+struct ElemCls {
+  uint32_t cls_base, local, nel_s, pad;
 };
 
 // doubles -> u64 keys with the same order, for atomicMin / atomicMax
@@ -166,6 +180,12 @@ __global__ void cell_scatter_kernel(const double *__restrict__ X, const double *
   }
 }
 
+// dst[i] = src[idx[i]]
+__global__ void gather_u32_kernel(const uint32_t *__restrict__ src, const uint32_t *__restrict__ idx, uint32_t n,
+                                  uint32_t *__restrict__ dst) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[idx[i]];
+}
+
 // Cells -> tiles: a cell of n atoms becomes ceil(n/64) tiles of near-equal size.
 __global__ void tile_build_kernel(const uint32_t *__restrict__ cnt, const uint32_t *__restrict__ cell_off,
                                   const uint32_t *__restrict__ tile_off, uint32_t ncells, const ElemGrid *__restrict__ eg,
@@ -173,8 +193,12 @@ __global__ void tile_build_kernel(const uint32_t *__restrict__ cnt, const uint32
   for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < ncells; c += gridDim.x * blockDim.x) {
     const uint32_t n = cnt[c];
     if (!n) continue;
-    uint32_t e = 0;
-    while (e + 1 < nel && c >= eg[e + 1].base) e++;
+    uint32_t lo = 0, hi = nel - 1;  // last element whose first cell is <= c
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      if (eg[mid].base <= c) lo = mid;
+      else hi = mid - 1;
+    }
     const uint32_t nt = (n + TILE_MAX - 1) / TILE_MAX;
     uint32_t s = cell_off[c];
     for (uint32_t t = 0; t < nt; t++) {
@@ -182,7 +206,7 @@ __global__ void tile_build_kernel(const uint32_t *__restrict__ cnt, const uint32
       Tile tl;
       tl.start = s;
       tl.count = cnt_t;
-      tl.elem = e;
+      tl.elem = lo;
       tl.pad = 0;
       tiles[tile_off[c] + t] = tl;
       s += cnt_t;
@@ -235,7 +259,7 @@ struct KeyParams {
   unsigned long long ntp;
   const Tile *tiles;
   double inv_bin;
-  uint32_t nhist, nbuckets, nkeys;  // key = t * nbuckets + bucket; nkeys - 1 = the wide key
+  uint32_t nhist, nbuckets, nkeys;  // key = class * nbuckets + bucket; nkeys - 1 = the wide key
 };
 
 __device__ __forceinline__ uint32_t pair_key(const KeyParams &p, unsigned long long w, TilePair *tp) {
@@ -273,40 +297,139 @@ struct HistParams {
   const Tile *tiles;
   const TilePair *list;
   const CtaRange *ranges;
-  unsigned long long *hist;
+  const ElemCls *ecls;
+  unsigned int *queue;      // next run for the persistent window kernel
+  unsigned long long *hist; // classes x nhist
   unsigned int *n_bad;
   double bin, inv_bin, margin;
-  uint32_t nhist, nel;
+  uint32_t nhist, nranges;
   uint32_t wide_begin, wide_end;
 };
 
-// One warp counts the pairs of one tile pair: the I tile is staged in the warp's shared memory, the J
-// tile sits in registers (atoms lane and lane + 32), the warp walks i.
-template <bool SAME, class Count>
-__device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const TilePair tp, double *wI, Count count) {
+// One warp counts the pairs of one tile pair: both tiles' FP64 coordinates and the I tile's FP32
+// offsets are staged in the warp's shared memory (stage: WARP_STAGE bytes), the J tile's FP32 offsets
+// sit in registers (atoms lane and lane + 32), the warp walks i two rows at a time (four independent
+// chains).  SAME (a tile against itself) keeps only i < j.
+//
+// FP32 estimate of r/bin: dh is the tile-centre offset (c_I - c_J)/bin rounded to float, dl its low
+// part; the I offsets are (x_i - c_I)/bin and the J offsets (x_j - c_J)/bin - dl, rounded to float.
+// Error bound (bins; u = 2^-24, E_I / E_J the tiles' largest half extent in bins): each axis
+// |dx - dx_true| <= u|dx| + C, C = u(2 E_I + 3 E_J + 2) + 2^-40 |D|; d2 by FMAs adds 3u relative;
+// rsqrt.approx (2 ulp) followed by one Newton step leaves u + O(u^2) relative to sqrt(d2); so
+// |r - r_true| <= 4.3 u r + 1.74 C.  With m = 6 u r + 2 C, any r whose distance d to the nearest
+// integer is >= m has floor(r) equal to the reference's bin (whose own FP64 rounding is below 1e-10
+// bins).  r + 1.5*2^23 rounds r to an integer in the low mantissa bits (r < 2^22), which gives
+// round(r) and d without a conversion.  Pairs with d < m, near or beyond the last bin, or outside the
+// CTA's window go to the lane's ring and are binned exactly with FP64 from the staged coordinates
+// (hist_bin.cuh) once some lane holds four.
+template <bool SAME, bool WINDOW>
+__device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const TilePair tp, uint8_t *stage,
+                                                      uint32_t *win, uint32_t base, unsigned long long *h) {
+  double *wI = reinterpret_cast<double *>(stage), *wJ = wI + 3 * TILE_MAX;
+  float *wIf = reinterpret_cast<float *>(wJ + 3 * TILE_MAX);
+  uint16_t *ring = reinterpret_cast<uint16_t *>(wIf + 3 * TILE_MAX);
   const uint32_t lane = threadIdx.x & 31;
   const Tile TI = p.tiles[tp.I], TJ = p.tiles[tp.J];
   const uint32_t ni = TI.count, nj = TJ.count;
+  const double ib = p.inv_bin;
+  double cI[3], cJ[3], EI = 0, EJ = 0, Dm = 0;
+  float dh[3], dl[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    cI[k] = 0.5 * (TI.lo[k] + TI.hi[k]);
+    cJ[k] = 0.5 * (TJ.lo[k] + TJ.hi[k]);
+    EI = fmax(EI, 0.5 * (TI.hi[k] - TI.lo[k]) * ib + 1.0);
+    EJ = fmax(EJ, 0.5 * (TJ.hi[k] - TJ.lo[k]) * ib + 1.0);
+    const double D = (cI[k] - cJ[k]) * ib;
+    dh[k] = (float)D;
+    dl[k] = (float)(D - (double)dh[k]);
+    Dm = fmax(Dm, fabs(D));
+  }
+  const float m0 = (float)(2.0 * (ldexp(2.0 * EI + 3.0 * EJ + 2.0, -24) + ldexp(Dm, -40))) + 1e-6f;
+  const float mr = 6.0f * 5.9604645e-8f;
   for (uint32_t i = lane; i < ni; i += 32) {
-    wI[i] = p.X[TI.start + i];
-    wI[TILE_MAX + i] = p.Y[TI.start + i];
-    wI[2 * TILE_MAX + i] = p.Z[TI.start + i];
+    const double x = p.X[TI.start + i], y = p.Y[TI.start + i], z = p.Z[TI.start + i];
+    wI[i] = x;
+    wI[TILE_MAX + i] = y;
+    wI[2 * TILE_MAX + i] = z;
+    wIf[i] = (float)((x - cI[0]) * ib);
+    wIf[TILE_MAX + i] = (float)((y - cI[1]) * ib);
+    wIf[2 * TILE_MAX + i] = (float)((z - cI[2]) * ib);
   }
   const uint32_t j0 = lane, j1 = lane + 32;
-  const double x0 = j0 < nj ? p.X[TJ.start + j0] : 0.0, y0 = j0 < nj ? p.Y[TJ.start + j0] : 0.0,
-               z0 = j0 < nj ? p.Z[TJ.start + j0] : 0.0;
-  const double x1 = j1 < nj ? p.X[TJ.start + j1] : 0.0, y1 = j1 < nj ? p.Y[TJ.start + j1] : 0.0,
-               z1 = j1 < nj ? p.Z[TJ.start + j1] : 0.0;
-  __syncwarp();
-  const double nh1 = (double)p.nhist - 1.0;
-  unsigned bad = 0;
-  // rows i and i+1 against columns j0 and j1: four independent FP64 chains per iteration, no branch
-  // until the rare exact fallback.  SAME (a tile against itself) keeps only i < j.
   const bool c0 = j0 < nj, c1 = j1 < nj;
+  float xj0 = 0.f, yj0 = 0.f, zj0 = 0.f, xj1 = 0.f, yj1 = 0.f, zj1 = 0.f;
+  if (c0) {
+    const double x = p.X[TJ.start + j0], y = p.Y[TJ.start + j0], z = p.Z[TJ.start + j0];
+    wJ[j0] = x;
+    wJ[TILE_MAX + j0] = y;
+    wJ[2 * TILE_MAX + j0] = z;
+    xj0 = (float)((x - cJ[0]) * ib) - dl[0];
+    yj0 = (float)((y - cJ[1]) * ib) - dl[1];
+    zj0 = (float)((z - cJ[2]) * ib) - dl[2];
+  }
+  if (c1) {
+    const double x = p.X[TJ.start + j1], y = p.Y[TJ.start + j1], z = p.Z[TJ.start + j1];
+    wJ[j1] = x;
+    wJ[TILE_MAX + j1] = y;
+    wJ[2 * TILE_MAX + j1] = z;
+    xj1 = (float)((x - cJ[0]) * ib) - dl[0];
+    yj1 = (float)((y - cJ[1]) * ib) - dl[1];
+    zj1 = (float)((z - cJ[2]) * ib) - dl[2];
+  }
+  __syncwarp();
+  const float MAGIC = 12582912.0f;                              // 1.5 * 2^23
+  const float lim = fminf((float)p.nhist - 1.0f, 4194303.0f);  // the last bin and beyond: exact path
+  const int tbase = __float_as_int(MAGIC) + (int)base;          // slot = bits(r + MAGIC) - tbase - (d < 0)
+  uint16_t *lq = ring + lane;                                   // this lane's ring: entry s at lq[32 s]
+  uint32_t qw = 0, cnt = 0;                                     // next write slot (mod 8), pending entries
+  unsigned bad = 0;
+  auto drain_one = [&]() {  // lanes with a pending entry bin their oldest exactly
+    if (cnt) {
+      const uint32_t e = lq[((qw - cnt) & 7u) << 5];
+      cnt--;
+      const uint32_t a = e >> 6, b = e & 63u;
+      const double d2 = ref_dist2(wI[a], wI[TILE_MAX + a], wI[2 * TILE_MAX + a], wJ[b], wJ[TILE_MAX + b],
+                                  wJ[2 * TILE_MAX + b]);
+      const uint32_t k = ref_bin(d2, p.bin, p.inv_bin, p.margin, p.nhist);
+      if (k >= p.nhist) {
+        bad++;
+      } else if (WINDOW && k - base < WIN) {
+        atomicAdd(win + (k - base), 1u);
+      } else {
+        atomicAdd(h + k, 1ull);
+      }
+    }
+  };
+#define XNS_PAIR(XA, YA, ZA, XJ, YJ, ZJ, VALID, II, JJ)                                   \
+  {                                                                                         \
+    const float dx = dh[0] + (XA - XJ), dy = dh[1] + (YA - YJ), dz = dh[2] + (ZA - ZJ);    \
+    const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));                                   \
+    float y;                                                                                \
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(d2));                                \
+    const float r0 = d2 * y; /* NaN for d2 == 0: not fast */                                \
+    const float r = fmaf(fmaf(-r0, r0, d2), 0.5f * y, r0); /* one Newton step */            \
+    const float t = r + MAGIC;                                                              \
+    const float d = r - (t - MAGIC);                                                        \
+    const float m = fmaf(r, mr, m0);                                                        \
+    const uint32_t slot = (uint32_t)(__float_as_int(t) - tbase) - (d < 0.f ? 1u : 0u);      \
+    const bool fast = (VALID) && fabsf(d) >= m && r < lim && (!WINDOW || slot < WIN);      \
+    if (WINDOW) {                                                                           \
+      /* branch-free: a lane without a fast pair adds 0 to its own spare slot */            \
+      atomicAdd(win + (fast ? slot : WIN + lane), fast ? 1u : 0u);                          \
+    } else if (fast) {                                                                      \
+      atomicAdd(h + slot, 1ull);                                                            \
+    }                                                                                       \
+    /* branch-free push: the write to the next free slot is harmless when nothing is pushed */ \
+    const uint32_t push = ((VALID) && !fast) ? 1u : 0u;                                     \
+    lq[qw << 5] = (uint16_t)(((II) << 6) | (JJ));                                           \
+    qw = (qw + push) & 7u;                                                                  \
+    cnt += push;                                                                            \
+  }
   for (uint32_t i = 0; i < ni; i += 2) {
     const uint32_t i1 = min(i + 1, ni - 1);
-    const double xa = wI[i], ya = wI[TILE_MAX + i], za = wI[2 * TILE_MAX + i];
-    const double xb = wI[i1], yb = wI[TILE_MAX + i1], zb = wI[2 * TILE_MAX + i1];
+    const float xa = wIf[i], ya = wIf[TILE_MAX + i], za = wIf[2 * TILE_MAX + i];
+    const float xb = wIf[i1], yb = wIf[TILE_MAX + i1], zb = wIf[2 * TILE_MAX + i1];
     const bool r1 = i + 1 < ni;
     bool v0 = c0, v1 = c1, v2 = c0 && r1, v3 = c1 && r1;
     if (SAME) {
@@ -315,31 +438,23 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
       v2 = v2 && i + 1 < j0;
       v3 = v3 && i + 1 < j1;
     }
-    const double d0 = ref_dist2(xa, ya, za, x0, y0, z0), d1 = ref_dist2(xa, ya, za, x1, y1, z1);
-    const double d2 = ref_dist2(xb, yb, zb, x0, y0, z0), d3 = ref_dist2(xb, yb, zb, x1, y1, z1);
-    uint32_t k0, k1, k2, k3;
-    const bool f0 = ref_bin_fast(d0, p.inv_bin, p.margin, nh1, &k0), f1 = ref_bin_fast(d1, p.inv_bin, p.margin, nh1, &k1);
-    const bool f2 = ref_bin_fast(d2, p.inv_bin, p.margin, nh1, &k2), f3 = ref_bin_fast(d3, p.inv_bin, p.margin, nh1, &k3);
-    if (!((f0 || !v0) && (f1 || !v1) && (f2 || !v2) && (f3 || !v3))) {
-      // a distance within the margin of a bin edge (or outside the estimate's range): exact path;
-      // a bin beyond the histogram is reported, not counted
-      if (v0 && !f0) { k0 = ref_bin(d0, p.bin, p.inv_bin, p.margin, p.nhist); if (k0 >= p.nhist) { v0 = false; bad++; } }
-      if (v1 && !f1) { k1 = ref_bin(d1, p.bin, p.inv_bin, p.margin, p.nhist); if (k1 >= p.nhist) { v1 = false; bad++; } }
-      if (v2 && !f2) { k2 = ref_bin(d2, p.bin, p.inv_bin, p.margin, p.nhist); if (k2 >= p.nhist) { v2 = false; bad++; } }
-      if (v3 && !f3) { k3 = ref_bin(d3, p.bin, p.inv_bin, p.margin, p.nhist); if (k3 >= p.nhist) { v3 = false; bad++; } }
-    }
-    if (v0) count(k0);
-    if (v1) count(k1);
-    if (v2) count(k2);
-    if (v3) count(k3);
+    XNS_PAIR(xa, ya, za, xj0, yj0, zj0, v0, i, j0)
+    XNS_PAIR(xa, ya, za, xj1, yj1, zj1, v1, i, j1)
+    XNS_PAIR(xb, yb, zb, xj0, yj0, zj0, v2, i + 1, j0)
+    XNS_PAIR(xb, yb, zb, xj1, yj1, zj1, v3, i + 1, j1)
+    // a ring holds 8: after this every lane holds at most 3, and the next step adds at most 4
+    while (__any_sync(0xffffffffu, cnt >= 4)) drain_one();
   }
-  __syncwarp();
+#undef XNS_PAIR
+  while (__any_sync(0xffffffffu, cnt > 0)) drain_one();
   return bad;
 }
 
-template <class Count>
-__device__ __forceinline__ unsigned count_tile_pair(const HistParams &p, const TilePair tp, double *wI, Count count) {
-  return tp.I == tp.J ? count_tile_pair_t<true>(p, tp, wI, count) : count_tile_pair_t<false>(p, tp, wI, count);
+template <bool WINDOW>
+__device__ __forceinline__ unsigned count_tile_pair(const HistParams &p, const TilePair tp, uint8_t *stage, uint32_t *win,
+                                                    uint32_t base, unsigned long long *h) {
+  return tp.I == tp.J ? count_tile_pair_t<true, WINDOW>(p, tp, stage, win, base, h)
+                      : count_tile_pair_t<false, WINDOW>(p, tp, stage, win, base, h);
 }
 
 // Slot s of the window holds bin B + s.  flush_window adds slots [lo, hi) (bins B + lo ...) to the
@@ -374,96 +489,114 @@ __device__ __forceinline__ void slide_window(uint32_t *win, unsigned long long *
   for (uint32_t s = WIN - delta + threadIdx.x; s < WIN; s += HW_THREADS) win[s] = 0;
 }
 
+// Persistent: each CTA takes runs (one class, a contiguous stretch of the sorted list) from the queue.
+// The window is empty between runs (the final flush clears every slot below nhist, and slots at or
+// above nhist are never written).
 __global__ void __launch_bounds__(HW_THREADS, 1) hist_window_kernel(HistParams p) {
-  extern __shared__ uint32_t win[];  // WIN bins, then HW_WARPS staging areas of 3 x 64 doubles
-  double *wI = reinterpret_cast<double *>(win + WIN) + (threadIdx.x >> 5) * 3 * TILE_MAX;
-  const CtaRange rg = p.ranges[blockIdx.x];
-  if (rg.begin >= rg.end) return;
-  unsigned long long *h = p.hist + (size_t)rg.type * p.nhist;
+  extern __shared__ uint32_t win[];  // WIN bins, 32 spare slots, then WARP_STAGE bytes per warp
+  uint8_t *stage = reinterpret_cast<uint8_t *>(win + WIN + 32) + (threadIdx.x >> 5) * WARP_STAGE;
+  __shared__ uint32_t run;
   for (uint32_t s = threadIdx.x; s < WIN; s += HW_THREADS) win[s] = 0;
-  uint32_t B = p.list[rg.begin].kmin / BUCKET * BUCKET;
-  __syncthreads();
   unsigned bad = 0;
-  for (uint32_t r = rg.begin; r < rg.end; r += HW_WARPS) {
-    // the round's entries must fit the window [B, B + WIN): slide it when the farthest one does not
-    uint32_t kmax = 0;
-    for (uint32_t e = r; e < min(r + HW_WARPS, rg.end); e++) kmax = max(kmax, p.list[e].kmax);
-    if (kmax >= B + WIN) {
-      const uint32_t nb = p.list[r].kmin / BUCKET * BUCKET;
-      if (nb > B) {
-        __syncthreads();
-        slide_window(win, h, B, nb, p.nhist);
-        B = nb;
-        __syncthreads();
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) run = atomicAdd(p.queue, 1u);
+    __syncthreads();
+    const uint32_t ri = run;
+    if (ri >= p.nranges) break;
+    const CtaRange rg = p.ranges[ri];
+    unsigned long long *h = p.hist + (size_t)rg.type * p.nhist;
+    uint32_t B = p.list[rg.begin].kmin / BUCKET * BUCKET;
+    for (uint32_t r = rg.begin; r < rg.end; r += HW_WARPS) {
+      // the round's entries must fit the window [B, B + WIN): slide it when the farthest one does not
+      uint32_t kmax = 0;
+      for (uint32_t e = r; e < min(r + HW_WARPS, rg.end); e++) kmax = max(kmax, p.list[e].kmax);
+      if (kmax >= B + WIN) {
+        const uint32_t nb = p.list[r].kmin / BUCKET * BUCKET;
+        if (nb > B) {
+          __syncthreads();
+          slide_window(win, h, B, nb, p.nhist);
+          B = nb;
+          __syncthreads();
+        }
+      }
+      const uint32_t e = r + (threadIdx.x >> 5);
+      if (e < rg.end) {
+        bad += count_tile_pair<true>(p, p.list[e], stage, win, B, h);
       }
     }
-    const uint32_t e = r + (threadIdx.x >> 5);
-    if (e < rg.end) {
-      const uint32_t base = B;
-      bad += count_tile_pair(p, p.list[e], wI, [&](uint32_t k) {
-        const uint32_t s = k - base;
-        if (s < WIN) atomicAdd(win + s, 1u);
-        else atomicAdd(h + k, 1ull);  // outside the window (a round spanning two buckets): count directly
-      });
-    }
+    __syncthreads();
+    flush_window(win, h, B, 0, WIN, p.nhist);
   }
-  __syncthreads();
-  flush_window(win, h, B, 0, WIN, p.nhist);
   if (bad) atomicAdd(p.n_bad, bad);
 }
 
 __global__ void __launch_bounds__(256) hist_wide_kernel(HistParams p) {
-  __shared__ double stage[8 * 3 * TILE_MAX];
-  double *wI = stage + (threadIdx.x >> 5) * 3 * TILE_MAX;
+  __shared__ __align__(16) uint8_t stage_all[8 * WARP_STAGE];
+  uint8_t *stage = stage_all + (threadIdx.x >> 5) * WARP_STAGE;
   unsigned bad = 0;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t e = p.wide_begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); e < p.wide_end; e += nw) {
     const TilePair tp = p.list[e];
-    const uint32_t a = min(p.tiles[tp.I].elem, p.tiles[tp.J].elem), b = max(p.tiles[tp.I].elem, p.tiles[tp.J].elem);
-    unsigned long long *h = p.hist + (size_t)(a * p.nel - a * (a - 1) / 2 + (b - a)) * p.nhist;
-    bad += count_tile_pair(p, tp, wI, [&](uint32_t k) { atomicAdd(h + k, 1ull); });
+    const ElemCls ea = p.ecls[p.tiles[tp.I].elem], eb = p.ecls[p.tiles[tp.J].elem];
+    const uint32_t a = min(ea.local, eb.local), b = max(ea.local, eb.local), n = ea.nel_s;
+    unsigned long long *h = p.hist + (size_t)(ea.cls_base + a * n - a * (a - 1) / 2 + (b - a)) * p.nhist;
+    bad += count_tile_pair<false>(p, tp, stage, nullptr, 0, h);
   }
   if (bad) atomicAdd(p.n_bad, bad);
 }
 
 }  // namespace
 
-int xns_hist_device(xns_ctx *ctx, const DevCoords &dc, uint32_t nhist, double bin, unsigned long long *d_hist) {
-  const uint32_t nel = (uint32_t)dc.n_el.size();
+int xns_hist_set(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, unsigned long long *d_hist) {
+  const uint32_t nel = (uint32_t)hs.el_n.size();
   if (nhist == 0 || !(bin > 0)) return xns_fail(ctx, XNS_ERR_ARG, "histogram: nhist == 0 or bin <= 0");
-  const uint32_t P = xns_npairs(nel);
+  if (nel == 0) return xns_fail(ctx, XNS_ERR_ARG, "histogram: no elements");
+  // classes: structure s owns P(nel_s) consecutive classes
+  std::vector<ElemCls> ecls(nel);
+  uint32_t C = 0;
+  for (const HistStruct &s : hs.st) {
+    for (uint32_t l = 0; l < s.nel; l++) ecls[s.e0 + l] = {C, l, s.nel, 0};
+    C += xns_npairs(s.nel);
+  }
   int st;
-  XNS_CUDA(ctx, cudaMemsetAsync(d_hist, 0, sizeof(unsigned long long) * (size_t)P * nhist, ctx->stream));
+  XNS_CUDA(ctx, cudaMemsetAsync(d_hist, 0, sizeof(unsigned long long) * (size_t)C * nhist, ctx->stream));
   void *flags;
   if ((st = xns_scratch(ctx, SLOT_FLAGS, 64, &flags))) return st;
   XNS_CUDA(ctx, cudaMemsetAsync(flags, 0, 64, ctx->stream));
-  if (dc.ntot < 2) return XNS_OK;
+  uint32_t ntot = 0;
+  for (uint32_t e = 0; e < nel; e++) ntot = std::max(ntot, hs.el_off[e] + hs.el_n[e]);
+  if (ntot < 2) return XNS_OK;
 
   // -- element bounding boxes -> cell grids
-  void *vkey, *vh;
-  const size_t small_bytes = sizeof(ElemGrid) * nel + 2 * 3 * sizeof(unsigned long long) * nel + 64;
-  if ((st = xns_scratch(ctx, SLOT_AUX, small_bytes, &vkey))) return st;
-  ElemGrid *d_eg = (ElemGrid *)vkey;
-  unsigned long long *d_bmin = (unsigned long long *)(d_eg + nel), *d_bmax = d_bmin + 3 * nel;
-  if ((st = xns_pinned(ctx, small_bytes, &vh))) return st;
+  void *vaux, *vh;
+  const size_t aux_bytes = (sizeof(ElemGrid) + sizeof(ElemCls) + 6 * sizeof(unsigned long long) + 2 * sizeof(uint32_t)) * nel + 64;
+  if ((st = xns_scratch(ctx, SLOT_AUX, aux_bytes, &vaux))) return st;
+  ElemGrid *d_eg = (ElemGrid *)vaux;
+  ElemCls *d_ecls = (ElemCls *)(d_eg + nel);
+  unsigned long long *d_bmin = (unsigned long long *)(d_ecls + nel), *d_bmax = d_bmin + 3 * nel;
+  uint32_t *d_ebase = (uint32_t *)(d_bmax + 3 * nel), *d_estart = d_ebase + nel;
+  if ((st = xns_pinned(ctx, aux_bytes, &vh))) return st;
   XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   std::vector<ElemGrid> eg(nel);
   for (uint32_t e = 0; e < nel; e++) {
     memset(&eg[e], 0, sizeof(ElemGrid));
-    eg[e].atom0 = dc.off_el[e];
-    eg[e].natoms = dc.n_el[e];
+    eg[e].atom0 = hs.el_off[e];
+    eg[e].natoms = hs.el_n[e];
   }
   memcpy(vh, eg.data(), sizeof(ElemGrid) * nel);
-  XNS_CUDA(ctx, cudaMemcpyAsync(d_eg, vh, sizeof(ElemGrid) * nel, cudaMemcpyHostToDevice, ctx->stream));
+  memcpy((char *)vh + sizeof(ElemGrid) * nel, ecls.data(), sizeof(ElemCls) * nel);
+  XNS_CUDA(ctx, cudaMemcpyAsync(d_eg, vh, (sizeof(ElemGrid) + sizeof(ElemCls)) * nel, cudaMemcpyHostToDevice, ctx->stream));
   XNS_CUDA(ctx, cudaMemsetAsync(d_bmin, 0xff, 3 * sizeof(unsigned long long) * nel, ctx->stream));
   XNS_CUDA(ctx, cudaMemsetAsync(d_bmax, 0, 3 * sizeof(unsigned long long) * nel, ctx->stream));
-  elem_bbox_kernel<<<dim3(std::max(1, ctx->num_sms / (int)nel), nel), 256, 0, ctx->stream>>>(dc.x, dc.y, dc.z, d_eg, d_bmin,
+  elem_bbox_kernel<<<dim3(std::max(1, ctx->num_sms / (int)nel), nel), 256, 0, ctx->stream>>>(hs.x, hs.y, hs.z, d_eg, d_bmin,
                                                                                              d_bmax);
   XNS_LAUNCHED(ctx);
-  std::vector<unsigned long long> bb(6 * nel);
+  std::vector<unsigned long long> bb(6 * (size_t)nel);
   XNS_CUDA(ctx, cudaMemcpyAsync(bb.data(), d_bmin, 6 * sizeof(unsigned long long) * nel, cudaMemcpyDeviceToHost, ctx->stream));
   XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   uint32_t ncells = 0;
+  std::vector<uint32_t> ebase(nel);
   for (uint32_t e = 0; e < nel; e++) {
     ElemGrid &g = eg[e];
     g.base = ncells;
@@ -471,7 +604,7 @@ int xns_hist_device(xns_ctx *ctx, const DevCoords &dc, uint32_t nhist, double bi
     double ext[3], vol = 1;
     for (int k = 0; k < 3; k++) {
       g.o[k] = ord_value(bb[3 * e + k]);
-      ext[k] = ord_value(bb[3 * nel + 3 * e + k]) - g.o[k];
+      ext[k] = ord_value(bb[3 * (size_t)nel + 3 * e + k]) - g.o[k];
       if (!(ext[k] >= 0) || !std::isfinite(ext[k])) return xns_fail(ctx, XNS_ERR_ARG, "histogram: non-finite coordinates");
     }
     const double emax = std::max(ext[0], std::max(ext[1], ext[2]));
@@ -489,27 +622,31 @@ int xns_hist_device(xns_ctx *ctx, const DevCoords &dc, uint32_t nhist, double bi
   if ((st = xns_scratch(ctx, SLOT_HCELL, sizeof(uint32_t) * (4 * (size_t)ncells + 8), &vcell))) return st;
   uint32_t *d_cnt = (uint32_t *)vcell, *d_coff = d_cnt + ncells, *d_toff = d_coff + ncells, *d_cur = d_toff + ncells,
            *d_tot = d_cur + ncells;
-  if ((st = xns_scratch(ctx, SLOT_HSORT, (sizeof(double) * 3 + sizeof(uint32_t)) * (size_t)dc.ntot, &vsort))) return st;
-  double *Xs = (double *)vsort, *Ys = Xs + dc.ntot, *Zs = Ys + dc.ntot;
-  uint32_t *d_cid = (uint32_t *)(Zs + dc.ntot);
+  if ((st = xns_scratch(ctx, SLOT_HSORT, (sizeof(double) * 3 + sizeof(uint32_t)) * (size_t)ntot, &vsort))) return st;
+  double *Xs = (double *)vsort, *Ys = Xs + ntot, *Zs = Ys + ntot;
+  uint32_t *d_cid = (uint32_t *)(Zs + ntot);
+  for (uint32_t e = 0; e < nel; e++) ebase[e] = std::min(eg[e].base, ncells - 1);
   memcpy(vh, eg.data(), sizeof(ElemGrid) * nel);
+  memcpy((char *)vh + sizeof(ElemGrid) * nel, ebase.data(), sizeof(uint32_t) * nel);
   XNS_CUDA(ctx, cudaMemcpyAsync(d_eg, vh, sizeof(ElemGrid) * nel, cudaMemcpyHostToDevice, ctx->stream));
+  XNS_CUDA(ctx, cudaMemcpyAsync(d_ebase, (char *)vh + sizeof(ElemGrid) * nel, sizeof(uint32_t) * nel,
+                                cudaMemcpyHostToDevice, ctx->stream));
   XNS_CUDA(ctx, cudaMemsetAsync(d_cnt, 0, sizeof(uint32_t) * ncells, ctx->stream));
   XNS_CUDA(ctx, cudaMemsetAsync(d_cur, 0, sizeof(uint32_t) * ncells, ctx->stream));
   const int gx = std::max(1, ctx->num_sms * 4 / (int)nel);
-  cell_count_kernel<<<dim3(gx, nel), 256, 0, ctx->stream>>>(dc.x, dc.y, dc.z, d_eg, d_cid, d_cnt);
+  cell_count_kernel<<<dim3(gx, nel), 256, 0, ctx->stream>>>(hs.x, hs.y, hs.z, d_eg, d_cid, d_cnt);
   XNS_LAUNCHED(ctx);
   scan_kernel<<<1, SCAN_THREADS, 0, ctx->stream>>>(d_cnt, ncells, d_coff, d_toff, d_tot);
   XNS_LAUNCHED(ctx);
-  cell_scatter_kernel<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(dc.x, dc.y, dc.z, dc.ntot, d_cid, d_coff, d_cur, Xs, Ys, Zs);
+  cell_scatter_kernel<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(hs.x, hs.y, hs.z, ntot, d_cid, d_coff, d_cur, Xs, Ys, Zs);
   XNS_LAUNCHED(ctx);
-  // tiles per element: read the tile offsets at the element boundaries
+  // tiles per element: the tile offsets at the element boundaries
+  gather_u32_kernel<<<(nel + 255) / 256, 256, 0, ctx->stream>>>(d_toff, d_ebase, nel, d_estart);
+  XNS_LAUNCHED(ctx);
   std::vector<uint32_t> tstart(nel + 1);
   uint32_t totals[2];
   XNS_CUDA(ctx, cudaMemcpyAsync(totals, d_tot, sizeof(totals), cudaMemcpyDeviceToHost, ctx->stream));
-  for (uint32_t e = 0; e < nel; e++)
-    if (eg[e].base < ncells)
-      XNS_CUDA(ctx, cudaMemcpyAsync(&tstart[e], d_toff + eg[e].base, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  XNS_CUDA(ctx, cudaMemcpyAsync(tstart.data(), d_estart, sizeof(uint32_t) * nel, cudaMemcpyDeviceToHost, ctx->stream));
   XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   const uint32_t ntiles = totals[1];
   for (uint32_t e = 0; e < nel; e++)
@@ -523,17 +660,19 @@ int xns_hist_device(xns_ctx *ctx, const DevCoords &dc, uint32_t nhist, double bi
   tile_bbox_kernel<<<(ntiles + 7) / 8, 256, 0, ctx->stream>>>(Xs, Ys, Zs, d_tiles, ntiles);
   XNS_LAUNCHED(ctx);
 
-  // -- tile pairs sorted by (element pair, distance bucket)
+  // -- tile pairs sorted by (class, distance bucket)
   std::vector<Segment> sa, sb;
   std::vector<uint32_t> cls, same;
-  uint32_t t = 0;
-  for (uint32_t a = 0; a < nel; a++)
-    for (uint32_t b = a; b < nel; b++, t++) {
-      sa.push_back({tstart[a], tstart[a + 1] - tstart[a]});
-      sb.push_back({tstart[b], tstart[b + 1] - tstart[b]});
-      cls.push_back(t);
-      same.push_back(a == b);
-    }
+  for (const HistStruct &s : hs.st) {
+    uint32_t t = ecls[s.e0].cls_base;
+    for (uint32_t a = s.e0; a < s.e0 + s.nel; a++)
+      for (uint32_t b = a; b < s.e0 + s.nel; b++, t++) {
+        sa.push_back({tstart[a], tstart[a + 1] - tstart[a]});
+        sb.push_back({tstart[b], tstart[b + 1] - tstart[b]});
+        cls.push_back(t);
+        same.push_back(a == b);
+      }
+  }
   std::vector<SegPair> sched;
   const unsigned long long ntp = xns_build_schedule(sa, sb, cls, same, 1, 1, &sched);
   if (ntp >= (1ull << 32)) return xns_fail(ctx, XNS_ERR_ARG, "histogram: too many tile pairs");
@@ -548,7 +687,9 @@ int xns_hist_device(xns_ctx *ctx, const DevCoords &dc, uint32_t nhist, double bi
   kp.inv_bin = 1.0 / bin;
   kp.nhist = nhist;
   kp.nbuckets = nhist / BUCKET + 1;
-  kp.nkeys = P * kp.nbuckets + 1;
+  const unsigned long long nkeys = (unsigned long long)C * kp.nbuckets + 1;
+  if (nkeys >= (1ull << 31)) return xns_fail(ctx, XNS_ERR_ARG, "histogram: too many classes x distance buckets");
+  kp.nkeys = (uint32_t)nkeys;
   void *vk, *vl;
   if ((st = xns_scratch(ctx, SLOT_HKEY, sizeof(uint32_t) * (3 * (size_t)kp.nkeys + 8), &vk))) return st;
   uint32_t *d_kcnt = (uint32_t *)vk, *d_koff = d_kcnt + kp.nkeys, *d_kcur = d_koff + kp.nkeys, *d_ktot = d_kcur + kp.nkeys;
@@ -563,76 +704,62 @@ int xns_hist_device(xns_ctx *ctx, const DevCoords &dc, uint32_t nhist, double bi
   XNS_LAUNCHED(ctx);
   pair_scatter_kernel<<<kgrid, 256, 0, ctx->stream>>>(kp, d_koff, d_kcur, d_list);
   XNS_LAUNCHED(ctx);
-  // split the sorted list into CTA ranges, one element pair per CTA, in proportion to its pairs
+  // cut the sorted list into runs of one class: about 4 runs per SM over the whole list, so that the
+  // queue balances uneven classes; a CTA's u32 window counts at most 64*64*entries pairs per bin, so a
+  // run stays below 2^19 entries
   std::vector<uint32_t> koff(kp.nkeys);
   XNS_CUDA(ctx, cudaMemcpyAsync(koff.data(), d_koff, sizeof(uint32_t) * kp.nkeys, cudaMemcpyDeviceToHost, ctx->stream));
   XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   const uint32_t n_narrow = koff[kp.nkeys - 1];
-  // a CTA's u32 window counts at most 64*64*entries pairs per bin: keep that below 2^31
-  const uint32_t max_per_cta = (1u << 19);
-  const int G = std::max<int>(ctx->num_sms, (int)((n_narrow + max_per_cta - 1) / max_per_cta));
-  // CTAs per element pair in proportion to its entries (largest remainders get the spare CTAs), so
-  // that one wave of G CTAs covers the list
-  std::vector<uint32_t> nty(P), gty(P, 0);
-  int used = 0;
-  for (uint32_t ty = 0; ty < P; ty++) {
-    nty[ty] = koff[(ty + 1) * kp.nbuckets] - koff[ty * kp.nbuckets];
-    if (nty[ty]) {
-      gty[ty] = std::max(1u, (uint32_t)((double)G * nty[ty] / std::max(n_narrow, 1u)));
-      used += gty[ty];
-    }
-  }
-  while (used < G) {
-    uint32_t best = 0;
-    double most = -1;
-    for (uint32_t ty = 0; ty < P; ty++)
-      if (nty[ty] && (double)nty[ty] / gty[ty] > most) {
-        most = (double)nty[ty] / gty[ty];
-        best = ty;
-      }
-    if (most < 0) break;
-    gty[best]++;
-    used++;
-  }
+  const uint32_t L = std::min<uint32_t>(1u << 19, std::max<uint32_t>(64, (n_narrow + 4 * ctx->num_sms - 1) / (4 * ctx->num_sms)));
   std::vector<CtaRange> ranges;
-  for (uint32_t ty = 0; ty < P; ty++) {
-    if (!nty[ty]) continue;
-    const uint32_t b0 = koff[ty * kp.nbuckets], b1 = b0 + nty[ty];
-    const uint32_t L = (nty[ty] + gty[ty] - 1) / gty[ty];
-    for (uint32_t s = b0; s < b1; s += L) ranges.push_back({s, std::min(b1, s + L), ty, 0});
+  for (uint32_t c = 0; c < C; c++) {
+    const uint32_t b0 = koff[(size_t)c * kp.nbuckets], b1 = koff[(size_t)(c + 1) * kp.nbuckets];
+    for (uint32_t s = b0; s < b1; s += L) ranges.push_back({s, std::min(b1, s + L), c, 0});
   }
+  std::stable_sort(ranges.begin(), ranges.end(),
+                   [](const CtaRange &a, const CtaRange &b) { return a.end - a.begin > b.end - b.begin; });
   HistParams hp;
   hp.X = Xs;
   hp.Y = Ys;
   hp.Z = Zs;
   hp.tiles = d_tiles;
   hp.list = d_list;
+  hp.ecls = d_ecls;
+  hp.queue = (unsigned int *)flags + 1;
   hp.hist = d_hist;
   hp.n_bad = (unsigned int *)flags;
   hp.bin = bin;
   hp.inv_bin = 1.0 / bin;
   hp.margin = (double)nhist * ldexp(1.0, -37);
   hp.nhist = nhist;
-  hp.nel = nel;
+  hp.nranges = (uint32_t)ranges.size();
   hp.wide_begin = n_narrow;
   hp.wide_end = (uint32_t)ntp;
+  hp.ranges = nullptr;
   if (!ranges.empty()) {
     void *vr, *vrh;
     if ((st = xns_scratch(ctx, SLOT_SEGPAIRS, sizeof(CtaRange) * ranges.size() + sizeof(SegPair) * sched.size(), &vr)))
       return st;
-    // the schedule is no longer needed once the list is built; its slot now holds the CTA ranges
+    // the schedule is no longer needed once the list is built; its slot now holds the runs
     if ((st = xns_pinned(ctx, sizeof(CtaRange) * ranges.size(), &vrh))) return st;
     XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     memcpy(vrh, ranges.data(), sizeof(CtaRange) * ranges.size());
     XNS_CUDA(ctx, cudaMemcpyAsync(vr, vrh, sizeof(CtaRange) * ranges.size(), cudaMemcpyHostToDevice, ctx->stream));
     hp.ranges = (const CtaRange *)vr;
-    const size_t smem = sizeof(uint32_t) * WIN + sizeof(double) * 3 * TILE_MAX * HW_WARPS;
-    XNS_CUDA(ctx, cudaFuncSetAttribute(hist_window_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    if ((st = xns_stage_begin(ctx, STAGE_HIST))) return st;
-    hist_window_kernel<<<(unsigned)ranges.size(), HW_THREADS, smem, ctx->stream>>>(hp);
+  }
+  if ((st = xns_stage_begin(ctx, STAGE_HIST))) return st;
+  if (!ranges.empty()) {
+    const size_t smem = sizeof(uint32_t) * (WIN + 32) + (size_t)WARP_STAGE * HW_WARPS;
+    static bool attr = false;
+    if (!attr) {
+      XNS_CUDA(ctx, cudaFuncSetAttribute(hist_window_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      attr = true;
+    }
+    const unsigned grid = (unsigned)std::min<size_t>((size_t)ctx->num_sms, ranges.size());
+    hist_window_kernel<<<grid, HW_THREADS, smem, ctx->stream>>>(hp);
     XNS_LAUNCHED(ctx);
   }
-  if (ranges.empty() && (st = xns_stage_begin(ctx, STAGE_HIST))) return st;
   if (hp.wide_end > hp.wide_begin) {
     hist_wide_kernel<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(hp);
     XNS_LAUNCHED(ctx);
@@ -643,6 +770,17 @@ int xns_hist_device(xns_ctx *ctx, const DevCoords &dc, uint32_t nhist, double bi
   XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   if (bad) return xns_fail(ctx, XNS_ERR_RANGE, "histogram: " + std::to_string(bad) + " pair distances fall beyond nhist bins");
   return XNS_OK;
+}
+
+int xns_hist_device(xns_ctx *ctx, const DevCoords &dc, uint32_t nhist, double bin, unsigned long long *d_hist) {
+  HistSet hs;
+  hs.x = dc.x;
+  hs.y = dc.y;
+  hs.z = dc.z;
+  hs.el_off = dc.off_el;
+  hs.el_n = dc.n_el;
+  hs.st.push_back({0, (uint32_t)dc.n_el.size()});
+  return xns_hist_set(ctx, hs, nhist, bin, d_hist);
 }
 
 extern "C" int xns_calc_hist(xns_ctx *ctx, const double *const *xyz_el, const uint32_t *n_el, uint32_t nel, uint32_t nhist,
