@@ -426,6 +426,87 @@ def debye_workload(args):
     return 0
 
 
+def batch_workload(args):
+    """Config 4: an ensemble of fcc spheres (a = 4.078 A), atom counts log-uniform in [1e3, 2e5], each
+    with its own Gaussian displacement sigma in [0.02, 0.1] A; 0.001 A bins, 4096 q in [0.1, 25),
+    neutron b = 7.63 fm.  Metric: patterns (I(q) of one structure) per second of the batched pass
+    (one plan, one persistent histogram launch, one exact tensor-core transform), next to the plain
+    path (one Debye_hist call per structure)."""
+    import torch
+    import xns_b200
+    from xns_b200 import synth
+    torch.cuda.set_device(0)
+    ctx = xns_b200.Context(0)
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    structs, ns, sig = synth.sphere_ensemble(count=args.batch_count, seed=0)
+    bin = 0.001
+    nh = max(synth.hist_size(s, bin) for s in structs)
+    q = synth.q_mesh(0.1, 25.0, 4096)
+    sl = [[7.63]] * len(structs)
+    pairs = int(sum(int(n) * (int(n) - 1) // 2 for n in ns))
+    steps, warmup = args.steps, args.warmup
+    chosen = lambda: ctx.calc_batch_debye_hist(structs, nh, bin, q, xns_b200.NEUTRON, sl=sl)  # noqa: E731
+    ms_c, kms_c, launches_c, clk = _measure(ctx, chosen, steps, warmup, 0)
+    def plain():  # the common bin count keeps the transform's sinc planes cached between structures
+        for s in structs:
+            ctx.calc_pdf_and_debye(s, nh, bin, xns_b200.DEBYE_HIST, 0, 0.0, q, xns_b200.NEUTRON, sl=[7.63])
+
+    ms_p, _, launches_p, _ = _measure(ctx, plain, max(1, steps // 2), 1, 0)
+    b = ctx.batch(structs, nh, bin, q, xns_b200.NEUTRON, sl=sl, autotune=True)
+    I, h = b.run(want_hist=True)
+    reps = []
+    for _ in range(3):
+        b.run()
+        reps.append(b.last_ms)
+    ct, wb, tms = b.tuning()
+    b.close()
+    # per-pattern error for the smallest, a median and the largest structure: against the reference's
+    # FP64 transform (calcInt1DHist, its summation order) on the same histograms, and against an
+    # extended-precision (x87 80-bit) sum on 128 q points that include the deepest minima -- at those
+    # minima the sequential FP64 sum itself is off by up to ~1e-5 for 2e5-atom particles
+    errs = {}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as orc
+        O = orc.Oracle()
+        for s in sorted({int(np.argmin(ns)), int(np.argsort(ns)[len(ns) // 2]), int(np.argmax(ns))}):
+            hs = h[s * nh:(s + 1) * nh]
+            Io = O.int_1d_hist(hs, [int(ns[s])], nh, bin, q, 0, sl=[7.63])
+            sel = np.unique(np.concatenate([np.argsort(np.abs(Io))[:64], np.linspace(0, len(q) - 1, 64).astype(int)]))
+            k = np.nonzero(hs)[0]
+            r = (k.astype(np.longdouble) + 0.5) * np.longdouble(bin)
+            hk = hs[k].astype(np.longdouble)
+            G = np.zeros(len(sel), dtype=np.longdouble)
+            for c in range(0, len(sel), 8):
+                x = np.outer(q[sel[c:c + 8]].astype(np.longdouble), r)
+                G[c:c + 8] = (np.sin(x) / (x + np.longdouble(1e-8))) @ hk
+            Ix = np.asarray((int(ns[s]) * np.longdouble(7.63) ** 2 + 2 * np.longdouble(7.63) ** 2 * G) / int(ns[s]),
+                            dtype=np.float64)
+            errs["%d atoms" % ns[s]] = {"vs_reference_fp64": float(np.max(np.abs(I[s] - Io) / np.abs(Io))),
+                                        "vs_extended_128q": float(np.max(np.abs(I[s][sel] - Ix) / np.abs(Ix))),
+                                        "reference_fp64_vs_extended_128q": float(np.max(np.abs(Io[sel] - Ix) / np.abs(Ix)))}
+    line = {"metric": "patterns/s", "value": len(structs) / (ms_c * 1e-3), "unit": "patterns/s", "n_gpus": 1,
+            "steps": steps, "warmup": warmup, "ms_per_step": ms_c, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 distances + u64 counts (histogram), integer-digit tensor-core transform",
+            "data": "synthetic (seeded)",
+            "config": {"workload": "%d fcc spheres a=4.078 A, %d-%d atoms (log-uniform), sigma 0.02-0.1 A, bin 0.001 A "
+                                   "(%d bins), 4096 q in [0.1,25), neutron" % (len(structs), ns.min(), ns.max(), nh),
+                       "structures": len(structs), "atoms": int(ns.sum()), "pairs_per_step": pairs,
+                       "l2": "flushed (512 MB write) before every timed step"},
+            "pairs_per_s": pairs / (ms_c * 1e-3),
+            "plain": {"patterns_per_s": len(structs) / (ms_p * 1e-3), "ms_per_step": ms_p,
+                      "path": "one xns_calc_pdf_and_debye (Debye_hist) call per structure"},
+            "speedup_vs_plain": ms_p / ms_c,
+            "graph_replay_ms": min(reps), "autotune": {"cell_target": ct, "window_bins": wb, "hist_ms": tms},
+            "max_rel_err_vs_fp64": errs,
+            "e2e": {"value": len(structs) / (ms_c * 1e-3), "unit": "patterns/s", "ms_per_step": ms_c,
+                    "h2d_bytes_per_step": int(ns.sum()) * 24 + 8 * len(q), "d2h_bytes_per_step": 8 * len(q) * len(structs)},
+            "gpu_launches": int(launches_c), "clocks": clk}
+    print(json.dumps(line))
+    ctx.close()
+    return 0
+
+
 def twod_workload(args):
     """Config 3: 2D amplitude of a 1,000,188-atom fcc crystallite (a = 3.61 A, 63^3 cells, 5 % second
     species, seeded random orientation), X-ray form factors from seeded 4-Gaussian coefficients, on the
@@ -491,8 +572,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cells", type=int, default=CELLS,
                     help="cube edge in unit cells (default 30, the benchmark; smaller only for profiler captures)")
-    ap.add_argument("--workload", default="histogram", choices=["histogram", "debye", "2d"],
-                    help="histogram (default, the headline: config 2); debye (config 1) and 2d (config 3) run on one GPU")
+    ap.add_argument("--workload", default="histogram", choices=["histogram", "debye", "2d", "batch"],
+                    help="histogram (default, the headline: config 2); debye (config 1), 2d (config 3) and batch "
+                         "(config 4) run on one GPU")
+    ap.add_argument("--batch-count", type=int, default=256, help="batch workload: structures in the ensemble")
     ap.add_argument("--cells2d", type=int, default=63, help="2d workload: crystallite edge in fcc cells (63: 1e6 atoms)")
     ap.add_argument("--mesh2d", type=int, default=1024, help="2d workload: q and phi points")
     args = ap.parse_args()
@@ -503,6 +586,8 @@ def main():
         return debye_workload(args)
     if args.workload == "2d" and args.impl == "ours":
         return twod_workload(args)
+    if args.workload == "batch" and args.impl == "ours":
+        return batch_workload(args)
     if args.impl == "reference":
         return reference_arm(args, rank, world)
     if world > 1:

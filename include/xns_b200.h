@@ -159,13 +159,51 @@ int xns_hist_transform_bf16x3(xns_ctx *ctx, const uint64_t *hist, uint32_t ncols
                               const double *q, uint32_t nq, double *G);
 
 /* The same G with exact accumulation on the BF16 tensor cores: the sinc matrix (FP64, with the
- * reference's +1e-8 in the denominator) as four base-256 integer digits, the counts as two or three
+ * reference's +1e-8 in the denominator) as five base-256 integer digits, the counts as two to four
  * base-256 digits, all digit products summed exactly (integers below 2^24 in the FP32 accumulator,
- * flushed to FP64 every 128 bins).  G carries the FP64 sinc's error plus < 2.4e-10 per matrix
+ * flushed to FP64 every 128 bins).  G carries the FP64 sinc's error plus < 1e-12 per matrix
  * element, so I(q) stays within 1e-5 of FP64 even at the deep minima of small particles, where the
- * FP32-accumulated bf16x3 form loses precision.  Counts below 2^24 (XNS_ERR_LIMIT beyond). */
+ * FP32-accumulated bf16x3 form loses precision.  Counts below 2^32 (XNS_ERR_LIMIT beyond). */
 int xns_hist_transform_exact(xns_ctx *ctx, const uint64_t *hist, uint32_t ncols, uint32_t nh, double bin,
                              const double *q, uint32_t nq, double *G);
+
+/* ---- batched ensembles ------------------------------------------------------------------------------ */
+
+/* No reference counterpart as one call: the reference evaluates one structure per run.  Per structure
+ * the result is calcPDFandDebye's Debye_hist intensity (CalcFunctions.cpp:912-968): the histogram of
+ * calcHist (:757-809, bit-exact) and the I(q) of calcInt1DHist (:810-911, exact transform, within 1e-5
+ * of FP64).
+ *
+ * Inputs, for nstruct structures:
+ *   nel[s]      elements of structure s; G = sum nel elements in all;
+ *   n_el[g]     atoms of element g (structure-major, then element order), g < G;
+ *   xyz         all atoms as packed x y z doubles in that order (sum n_el triples);
+ *   nhist, bin  one histogram grid for all structures (nhist >= every structure's need);
+ *   sl[g] / ff[g][iq]  weights per element g (neutron / X-ray), as in the single-structure calls.
+ * Outputs: I (nstruct x nq), hist (optional: classes x nhist u64, classes = sum P(nel[s]), structure s
+ * owning its P(nel[s]) element pairs in the reference's order).
+ *
+ * xns_calc_batch_debye_hist does everything in one call.  xns_batch_create plans the ensemble (spatial
+ * sort and tile pairs of all structures, optionally autotuned), runs it once and captures the launches
+ * of the histogram, transform and epilogue in a CUDA graph; xns_batch_run replays that graph (for the
+ * same coordinates, e.g. after changing nothing but wanting the result again, or for timing).  A batch
+ * owns a private context (stream and working memory) on the caller's device. */
+typedef struct xns_batch xns_batch;
+int xns_calc_batch_debye_hist(xns_ctx *ctx, uint32_t nstruct, const uint32_t *nel, const uint32_t *n_el,
+                              const double *xyz, uint32_t nhist, double bin, const double *q, uint32_t nq, int source,
+                              const double *const *ff, const double *sl, int polar, double lambda, double *I,
+                              uint64_t *hist);
+int xns_batch_create(xns_ctx *ctx, uint32_t nstruct, const uint32_t *nel, const uint32_t *n_el, const double *xyz,
+                     uint32_t nhist, double bin, const double *q, uint32_t nq, int source, const double *const *ff,
+                     const double *sl, int polar, double lambda, int autotune, xns_batch **out);
+int xns_batch_run(xns_batch *b, double *I, uint64_t *hist);
+/* Device time of the last xns_batch_run (ms) and its error message. */
+double xns_batch_last_ms(const xns_batch *b);
+const char *xns_batch_last_error(const xns_batch *b);
+/* The plan the autotuner kept (mean atoms per spatial cell, window bins) and its histogram time in ms
+ * (-1 when the batch was created without autotuning). */
+double xns_batch_tuning(const xns_batch *b, uint32_t *cell_target, uint32_t *window_bins);
+void xns_batch_destroy(xns_batch *b);
 
 /* ---- utilities (no reference counterpart) -------------------------------------------------------- */
 

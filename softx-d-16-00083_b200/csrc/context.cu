@@ -214,6 +214,7 @@ int xns_create(int device, xns_ctx **out) {
 
 void xns_destroy(xns_ctx *ctx) {
   if (!ctx) return;
+  xns_batch_release_cache(ctx);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (int s = 0; s < SLOT_COUNT; s++)
     if (ctx->slot_ptr[s]) cudaFree(ctx->slot_ptr[s]);

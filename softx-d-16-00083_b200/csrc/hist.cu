@@ -37,12 +37,11 @@ using namespace xns_hist;
 
 namespace {
 
-constexpr int CELL_TARGET = 56;      // mean atoms per cell over an element's bounding box
 constexpr int TILE_MAX = 64;         // atoms per tile
 constexpr int MAX_CELLS_AXIS = 256;
 constexpr int HW_WARPS = 16;
 constexpr int HW_THREADS = 32 * HW_WARPS;
-constexpr uint32_t WIN = 39 * 1024;  // window bins
+constexpr uint32_t WIN_MAX = 39 * 1024;  // largest window (bins) that fits with the warp stages
 constexpr uint32_t BUCKET = 1024;    // distance bucket of the tile-pair sort, in bins
 constexpr int SCAN_THREADS = 1024;
 constexpr int RING = 256;            // deferred pairs per warp: 8 per lane (u16 entries i << 6 | j)
@@ -260,6 +259,7 @@ struct KeyParams {
   const Tile *tiles;
   double inv_bin;
   uint32_t nhist, nbuckets, nkeys;  // key = class * nbuckets + bucket; nkeys - 1 = the wide key
+  uint32_t win;                     // window bins of the counting kernel
 };
 
 __device__ __forceinline__ uint32_t pair_key(const KeyParams &p, unsigned long long w, TilePair *tp) {
@@ -270,7 +270,7 @@ __device__ __forceinline__ uint32_t pair_key(const KeyParams &p, unsigned long l
   tp->I = g.a0 + I;
   tp->J = g.b0 + J;
   tile_pair_range(p.tiles[tp->I], p.tiles[tp->J], p.inv_bin, &tp->kmin, &tp->kmax);
-  if (tp->kmax - tp->kmin + BUCKET >= WIN) return p.nkeys - 1;
+  if (tp->kmax - tp->kmin + BUCKET >= p.win) return p.nkeys - 1;
   return g.cls * p.nbuckets + min(tp->kmin, p.nhist) / BUCKET;
 }
 
@@ -304,7 +304,9 @@ struct HistParams {
   double bin, inv_bin, margin;
   uint32_t nhist, nranges;
   uint32_t wide_begin, wide_end;
+  uint32_t win;             // window bins (<= WIN_MAX)
 };
+static_assert(sizeof(HistParams) <= sizeof(((HistLaunch *)0)->params), "HistLaunch holds the kernel parameters");
 
 // One warp counts the pairs of one tile pair: both tiles' FP64 coordinates and the I tile's FP32
 // offsets are staged in the warp's shared memory (stage: WARP_STAGE bytes), the J tile's FP32 offsets
@@ -381,6 +383,7 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
   const float MAGIC = 12582912.0f;                              // 1.5 * 2^23
   const float lim = fminf((float)p.nhist - 1.0f, 4194303.0f);  // the last bin and beyond: exact path
   const int tbase = __float_as_int(MAGIC) + (int)base;          // slot = bits(r + MAGIC) - tbase - (d < 0)
+  const uint32_t W = p.win;
   uint16_t *lq = ring + lane;                                   // this lane's ring: entry s at lq[32 s]
   uint32_t qw = 0, cnt = 0;                                     // next write slot (mod 8), pending entries
   unsigned bad = 0;
@@ -394,7 +397,7 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
       const uint32_t k = ref_bin(d2, p.bin, p.inv_bin, p.margin, p.nhist);
       if (k >= p.nhist) {
         bad++;
-      } else if (WINDOW && k - base < WIN) {
+      } else if (WINDOW && k - base < p.win) {
         atomicAdd(win + (k - base), 1u);
       } else {
         atomicAdd(h + k, 1ull);
@@ -413,10 +416,10 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
     const float d = r - (t - MAGIC);                                                        \
     const float m = fmaf(r, mr, m0);                                                        \
     const uint32_t slot = (uint32_t)(__float_as_int(t) - tbase) - (d < 0.f ? 1u : 0u);      \
-    const bool fast = (VALID) && fabsf(d) >= m && r < lim && (!WINDOW || slot < WIN);      \
+    const bool fast = (VALID) && fabsf(d) >= m && r < lim && (!WINDOW || slot < W);        \
     if (WINDOW) {                                                                           \
       /* branch-free: a lane without a fast pair adds 0 to its own spare slot */            \
-      atomicAdd(win + (fast ? slot : WIN + lane), fast ? 1u : 0u);                          \
+      atomicAdd(win + (fast ? slot : W + lane), fast ? 1u : 0u);                            \
     } else if (fast) {                                                                      \
       atomicAdd(h + slot, 1ull);                                                            \
     }                                                                                       \
@@ -471,32 +474,35 @@ __device__ __forceinline__ void flush_window(uint32_t *win, unsigned long long *
   }
 }
 
-// Moves the window from B to nb > B: bins [B, nb) leave (flushed), bins [nb, B + WIN) move down to
-// slots [0, B + WIN - nb), the vacated top slots are cleared.  Called by all threads between barriers.
-__device__ __forceinline__ void slide_window(uint32_t *win, unsigned long long *h, uint32_t B, uint32_t nb, uint32_t nhist) {
+// Moves the window of W bins from B to nb > B: bins [B, nb) leave (flushed), bins [nb, B + W) move
+// down to slots [0, B + W - nb), the vacated top slots are cleared.  Called by all threads between
+// barriers.
+__device__ __forceinline__ void slide_window(uint32_t *win, uint32_t W, unsigned long long *h, uint32_t B, uint32_t nb,
+                                             uint32_t nhist) {
   const uint32_t delta = nb - B;
-  flush_window(win, h, B, 0, min(delta, WIN), nhist);
-  if (delta >= WIN) return;  // everything left; the flush cleared it
+  flush_window(win, h, B, 0, min(delta, W), nhist);
+  if (delta >= W) return;  // everything left; the flush cleared it
   __syncthreads();
   // shift down by delta in chunks: a chunk's reads lie above every slot written so far
-  for (uint32_t c = 0; c < WIN - delta; c += HW_THREADS) {
+  for (uint32_t c = 0; c < W - delta; c += HW_THREADS) {
     const uint32_t s = c + threadIdx.x;
-    const uint32_t v = s < WIN - delta ? win[s + delta] : 0u;
+    const uint32_t v = s < W - delta ? win[s + delta] : 0u;
     __syncthreads();
-    if (s < WIN - delta) win[s] = v;
+    if (s < W - delta) win[s] = v;
     __syncthreads();
   }
-  for (uint32_t s = WIN - delta + threadIdx.x; s < WIN; s += HW_THREADS) win[s] = 0;
+  for (uint32_t s = W - delta + threadIdx.x; s < W; s += HW_THREADS) win[s] = 0;
 }
 
 // Persistent: each CTA takes runs (one class, a contiguous stretch of the sorted list) from the queue.
 // The window is empty between runs (the final flush clears every slot below nhist, and slots at or
 // above nhist are never written).
 __global__ void __launch_bounds__(HW_THREADS, 1) hist_window_kernel(HistParams p) {
-  extern __shared__ uint32_t win[];  // WIN bins, 32 spare slots, then WARP_STAGE bytes per warp
-  uint8_t *stage = reinterpret_cast<uint8_t *>(win + WIN + 32) + (threadIdx.x >> 5) * WARP_STAGE;
+  extern __shared__ uint32_t win[];  // p.win bins, 32 spare slots, then WARP_STAGE bytes per warp
+  const uint32_t W = p.win;
+  uint8_t *stage = reinterpret_cast<uint8_t *>(win + W + 32) + (threadIdx.x >> 5) * WARP_STAGE;
   __shared__ uint32_t run;
-  for (uint32_t s = threadIdx.x; s < WIN; s += HW_THREADS) win[s] = 0;
+  for (uint32_t s = threadIdx.x; s < W; s += HW_THREADS) win[s] = 0;
   unsigned bad = 0;
   for (;;) {
     __syncthreads();
@@ -508,14 +514,14 @@ __global__ void __launch_bounds__(HW_THREADS, 1) hist_window_kernel(HistParams p
     unsigned long long *h = p.hist + (size_t)rg.type * p.nhist;
     uint32_t B = p.list[rg.begin].kmin / BUCKET * BUCKET;
     for (uint32_t r = rg.begin; r < rg.end; r += HW_WARPS) {
-      // the round's entries must fit the window [B, B + WIN): slide it when the farthest one does not
+      // the round's entries must fit the window [B, B + W): slide it when the farthest one does not
       uint32_t kmax = 0;
       for (uint32_t e = r; e < min(r + HW_WARPS, rg.end); e++) kmax = max(kmax, p.list[e].kmax);
-      if (kmax >= B + WIN) {
+      if (kmax >= B + W) {
         const uint32_t nb = p.list[r].kmin / BUCKET * BUCKET;
         if (nb > B) {
           __syncthreads();
-          slide_window(win, h, B, nb, p.nhist);
+          slide_window(win, W, h, B, nb, p.nhist);
           B = nb;
           __syncthreads();
         }
@@ -526,7 +532,7 @@ __global__ void __launch_bounds__(HW_THREADS, 1) hist_window_kernel(HistParams p
       }
     }
     __syncthreads();
-    flush_window(win, h, B, 0, WIN, p.nhist);
+    flush_window(win, h, B, 0, W, p.nhist);
   }
   if (bad) atomicAdd(p.n_bad, bad);
 }
@@ -548,10 +554,14 @@ __global__ void __launch_bounds__(256) hist_wide_kernel(HistParams p) {
 
 }  // namespace
 
-int xns_hist_set(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, unsigned long long *d_hist) {
+int xns_hist_plan(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, unsigned long long *d_hist,
+                  const HistTuning &tune, HistLaunch *L) {
   const uint32_t nel = (uint32_t)hs.el_n.size();
+  *L = HistLaunch();
   if (nhist == 0 || !(bin > 0)) return xns_fail(ctx, XNS_ERR_ARG, "histogram: nhist == 0 or bin <= 0");
   if (nel == 0) return xns_fail(ctx, XNS_ERR_ARG, "histogram: no elements");
+  if (tune.win < 2 * BUCKET || tune.win > WIN_MAX || tune.cell_target < 8)
+    return xns_fail(ctx, XNS_ERR_ARG, "histogram: tuning outside its range");
   // classes: structure s owns P(nel_s) consecutive classes
   std::vector<ElemCls> ecls(nel);
   uint32_t C = 0;
@@ -560,10 +570,12 @@ int xns_hist_set(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, un
     C += xns_npairs(s.nel);
   }
   int st;
-  XNS_CUDA(ctx, cudaMemsetAsync(d_hist, 0, sizeof(unsigned long long) * (size_t)C * nhist, ctx->stream));
   void *flags;
-  if ((st = xns_scratch(ctx, SLOT_FLAGS, 64, &flags))) return st;
-  XNS_CUDA(ctx, cudaMemsetAsync(flags, 0, 64, ctx->stream));
+  if ((st = xns_scratch(ctx, SLOT_HFLAGS, 64, &flags))) return st;
+  L->hist = d_hist;
+  L->hist_words = (size_t)C * nhist;
+  L->flags = (unsigned int *)flags;
+  L->classes = C;
   uint32_t ntot = 0;
   for (uint32_t e = 0; e < nel; e++) ntot = std::max(ntot, hs.el_off[e] + hs.el_n[e]);
   if (ntot < 2) return XNS_OK;
@@ -609,7 +621,7 @@ int xns_hist_set(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, un
     }
     const double emax = std::max(ext[0], std::max(ext[1], ext[2]));
     for (int k = 0; k < 3; k++) vol *= std::max(ext[k], 1e-3 * emax + 1e-9);
-    const double s = std::max(cbrt(CELL_TARGET * vol / g.natoms), 1e-6);
+    const double s = std::max(cbrt(tune.cell_target * vol / g.natoms), 1e-6);
     for (int k = 0; k < 3; k++) {
       g.n[k] = (uint32_t)std::min<double>(MAX_CELLS_AXIS, std::max(1.0, floor(ext[k] / s) + 1));
       g.inv[k] = ext[k] > 0 ? g.n[k] / (ext[k] * (1 + 1e-12)) : 0.0;
@@ -690,6 +702,7 @@ int xns_hist_set(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, un
   const unsigned long long nkeys = (unsigned long long)C * kp.nbuckets + 1;
   if (nkeys >= (1ull << 31)) return xns_fail(ctx, XNS_ERR_ARG, "histogram: too many classes x distance buckets");
   kp.nkeys = (uint32_t)nkeys;
+  kp.win = tune.win;
   void *vk, *vl;
   if ((st = xns_scratch(ctx, SLOT_HKEY, sizeof(uint32_t) * (3 * (size_t)kp.nkeys + 8), &vk))) return st;
   uint32_t *d_kcnt = (uint32_t *)vk, *d_koff = d_kcnt + kp.nkeys, *d_kcur = d_koff + kp.nkeys, *d_ktot = d_kcur + kp.nkeys;
@@ -711,11 +724,12 @@ int xns_hist_set(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, un
   XNS_CUDA(ctx, cudaMemcpyAsync(koff.data(), d_koff, sizeof(uint32_t) * kp.nkeys, cudaMemcpyDeviceToHost, ctx->stream));
   XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   const uint32_t n_narrow = koff[kp.nkeys - 1];
-  const uint32_t L = std::min<uint32_t>(1u << 19, std::max<uint32_t>(64, (n_narrow + 4 * ctx->num_sms - 1) / (4 * ctx->num_sms)));
+  const uint32_t run_len =
+      std::min<uint32_t>(1u << 19, std::max<uint32_t>(64, (n_narrow + 4 * ctx->num_sms - 1) / (4 * ctx->num_sms)));
   std::vector<CtaRange> ranges;
   for (uint32_t c = 0; c < C; c++) {
     const uint32_t b0 = koff[(size_t)c * kp.nbuckets], b1 = koff[(size_t)(c + 1) * kp.nbuckets];
-    for (uint32_t s = b0; s < b1; s += L) ranges.push_back({s, std::min(b1, s + L), c, 0});
+    for (uint32_t s = b0; s < b1; s += run_len) ranges.push_back({s, std::min(b1, s + run_len), c, 0});
   }
   std::stable_sort(ranges.begin(), ranges.end(),
                    [](const CtaRange &a, const CtaRange &b) { return a.end - a.begin > b.end - b.begin; });
@@ -737,6 +751,7 @@ int xns_hist_set(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, un
   hp.wide_begin = n_narrow;
   hp.wide_end = (uint32_t)ntp;
   hp.ranges = nullptr;
+  hp.win = tune.win;
   if (!ranges.empty()) {
     void *vr, *vrh;
     if ((st = xns_scratch(ctx, SLOT_SEGPAIRS, sizeof(CtaRange) * ranges.size() + sizeof(SegPair) * sched.size(), &vr)))
@@ -748,28 +763,52 @@ int xns_hist_set(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, un
     XNS_CUDA(ctx, cudaMemcpyAsync(vr, vrh, sizeof(CtaRange) * ranges.size(), cudaMemcpyHostToDevice, ctx->stream));
     hp.ranges = (const CtaRange *)vr;
   }
-  if ((st = xns_stage_begin(ctx, STAGE_HIST))) return st;
-  if (!ranges.empty()) {
-    const size_t smem = sizeof(uint32_t) * (WIN + 32) + (size_t)WARP_STAGE * HW_WARPS;
+  memcpy(L->params, &hp, sizeof(hp));
+  L->nranges = (uint32_t)ranges.size();
+  L->window_grid = (uint32_t)std::min<size_t>((size_t)ctx->num_sms, ranges.size());
+  L->window_smem = sizeof(uint32_t) * (tune.win + 32) + (size_t)WARP_STAGE * HW_WARPS;
+  L->wide = hp.wide_end > hp.wide_begin;
+  return XNS_OK;
+}
+
+int xns_hist_enqueue(xns_ctx *ctx, const HistLaunch &L) {
+  XNS_CUDA(ctx, cudaMemsetAsync(L.hist, 0, sizeof(unsigned long long) * L.hist_words, ctx->stream));
+  XNS_CUDA(ctx, cudaMemsetAsync(L.flags, 0, 2 * sizeof(unsigned int), ctx->stream));
+  HistParams hp;
+  memcpy(&hp, L.params, sizeof(hp));
+  if (L.nranges) {
     static bool attr = false;
     if (!attr) {
-      XNS_CUDA(ctx, cudaFuncSetAttribute(hist_window_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      const int max_smem = (int)(sizeof(uint32_t) * (WIN_MAX + 32) + (size_t)WARP_STAGE * HW_WARPS);
+      XNS_CUDA(ctx, cudaFuncSetAttribute(hist_window_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
       attr = true;
     }
-    const unsigned grid = (unsigned)std::min<size_t>((size_t)ctx->num_sms, ranges.size());
-    hist_window_kernel<<<grid, HW_THREADS, smem, ctx->stream>>>(hp);
+    hist_window_kernel<<<L.window_grid, HW_THREADS, L.window_smem, ctx->stream>>>(hp);
     XNS_LAUNCHED(ctx);
   }
-  if (hp.wide_end > hp.wide_begin) {
+  if (L.wide) {
     hist_wide_kernel<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(hp);
     XNS_LAUNCHED(ctx);
   }
-  if ((st = xns_stage_end(ctx, STAGE_HIST))) return st;
+  return XNS_OK;
+}
+
+int xns_hist_check(xns_ctx *ctx, const HistLaunch &L) {
   unsigned int bad = 0;
-  XNS_CUDA(ctx, cudaMemcpyAsync(&bad, flags, sizeof(bad), cudaMemcpyDeviceToHost, ctx->stream));
+  XNS_CUDA(ctx, cudaMemcpyAsync(&bad, L.flags, sizeof(bad), cudaMemcpyDeviceToHost, ctx->stream));
   XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   if (bad) return xns_fail(ctx, XNS_ERR_RANGE, "histogram: " + std::to_string(bad) + " pair distances fall beyond nhist bins");
   return XNS_OK;
+}
+
+int xns_hist_set(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, unsigned long long *d_hist) {
+  HistLaunch L;
+  int st;
+  if ((st = xns_hist_plan(ctx, hs, nhist, bin, d_hist, HistTuning(), &L))) return st;
+  if ((st = xns_stage_begin(ctx, STAGE_HIST))) return st;
+  if ((st = xns_hist_enqueue(ctx, L))) return st;
+  if ((st = xns_stage_end(ctx, STAGE_HIST))) return st;
+  return xns_hist_check(ctx, L);
 }
 
 int xns_hist_device(xns_ctx *ctx, const DevCoords &dc, uint32_t nhist, double bin, unsigned long long *d_hist) {

@@ -15,6 +15,30 @@ struct HistSet {
   std::vector<HistStruct> st;         // structures in class order
 };
 
+// Plan parameters: mean atoms per cell of the spatial sort (sets the tile extent) and the bins of the
+// shared-memory window that slides along the distance axis (its privatisation depth).
+struct HistTuning {
+  uint32_t cell_target = 56;
+  uint32_t win = 39 * 1024;
+};
+
+// Everything the counting kernels need, built by xns_hist_plan; the buffers it points to live in the
+// context's scratch slots until the next plan.
+struct HistLaunch {
+  alignas(16) unsigned char params[256];  // the kernels' parameter block (hist.cu)
+  unsigned long long *hist = nullptr;     // classes x nhist
+  size_t hist_words = 0;
+  unsigned int *flags = nullptr;          // [0] pairs beyond nhist, [1] run queue
+  uint32_t classes = 0, nranges = 0, window_grid = 0, wide = 0;
+  size_t window_smem = 0;
+};
+
 // d_hist receives classes x nhist u64 counts; structure s owns classes [sum_{s'<s} P(nel_s'),
-// + P(nel_s)) in the reference's (a outer, b inner) order.
+// + P(nel_s)) in the reference's (a outer, b inner) order.  Synchronous.
 int xns_hist_set(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, unsigned long long *d_hist);
+// The same in three steps: the plan (spatial sort, tile pairs, runs; synchronises with the host), the
+// counting launches (memsets and kernels only: can be captured in a CUDA graph), the range check.
+int xns_hist_plan(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, unsigned long long *d_hist,
+                  const HistTuning &tune, HistLaunch *L);
+int xns_hist_enqueue(xns_ctx *ctx, const HistLaunch &L);
+int xns_hist_check(xns_ctx *ctx, const HistLaunch &L);

@@ -6,17 +6,17 @@
 // accumulates real products in FP32, and its rounding grows with the running sum; at the low-q minima
 // of a small particle's I(q) that sum is 1e5-1e6 times the result, which puts the error above 1e-4 of
 // I(q).  Here both operands are written as small integers, which BF16 holds exactly (|x| <= 256):
-//   S[q][k] = sum_{i<4}  d_i / (128 * 256^i),  d_i in [-128, 128]  (S in FP64; residual < 2.4e-10)
+//   S[q][k] = sum_{i<5}  d_i / (128 * 256^i),  d_i in [-128, 128]  (S in FP64; residual < 1e-12)
 //   n[k]    = sum_{j<NH} e_j * 256^j,          e_j in [0, 255]     (counts < 2^(8 NH), exact)
 //   G       = sum_{i,j} 256^(j-i) / 128 * (d_i . e_j)
-// A product of digits is an integer below 2^15 and a level v = j - i gains at most 3 of them per k,
-// so over a chunk of CH_K = 128 k every partial sum is an integer below 2^24 and the FP32 tensor-memory
-// accumulator holds it exactly.  All 4*NH digit products are kept; products of one level share one
+// A product of digits is an integer below 2^15 (128 * 255 = 32640) and a level v = j - i gains at most
+// min(4, NH) <= 4 of them per k, so over a chunk of CH_K = 128 k every partial sum is an integer below
+// 128 * 4 * 32640 < 2^24 and the FP32 tensor-memory accumulator holds it exactly.  All 4*NH digit products are kept; products of one level share one
 // accumulator (4 + NH - 1 levels of 64 columns), and every chunk the accumulators are read, combined
 // in FP64 (Horner over the levels, exact: below 2^53) and added to per-thread FP64 sums, which go to
 // the output with FP64 atomics when the CTA's part of an output tile ends.
 //
-// Tile 128 q x 64 columns x 64 k, one CTA per SM, 2 stages of {4 S-digit tiles, NH count-digit
+// Tile 128 q x 64 columns x 64 k, one CTA per SM, 2 stages of {NDS S-digit tiles, NH count-digit
 // tiles}; warp 0 loads (cp.async.bulk), warp 1 issues the MMAs, warps 2-9 drain tensor memory (two
 // warps per 32-lane quarter, 32 columns each).  Waits are bounded as in tc_gemm.cu.
 #include <algorithm>
@@ -29,7 +29,9 @@ using namespace xns_ptx;
 namespace {
 
 constexpr int XM = 128, XN = 64, XK = 64;  // tile: q rows, columns, k (one 128-byte swizzle row of BF16)
-constexpr int NDS = 4;                     // digits of the sinc matrix
+// Digits of the sinc matrix.  Four leave 2.4e-10 per element, which at the deepest minima of a
+// 2e5-atom sphere is 2e-5 of I(q) (the sum over ~3e5 bins of 1e5 counts each); five leave 1e-12.
+constexpr int NDS = 5;
 constexpr int XA = XM * XK * 2;            // 16 KB per S-digit tile
 constexpr int XB = XN * XK * 2;            // 8 KB per count-digit tile
 constexpr int XSTAGES = 2;
@@ -221,7 +223,7 @@ __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) 
         const uint32_t mt = (uint32_t)(r % g.MT), nt = (uint32_t)(r / g.MT);
         const uint32_t m = mt * XM + wq * 32 + lane;
         // level l holds 256^(NH-1-l)/128; Horner gave 256^(NL-1-l): scale 256^(NH-NL)/128
-        const double scale = 1.0 / (128.0 * 16777216.0);  // NL - NH = NDS - 1 = 3 -> 256^-3
+        const double scale = ldexp(1.0, -8 * (NDS - 1)) / 128.0;  // NL - NH = NDS - 1 -> 256^-(NDS-1)
         if (m < g.m_valid) {
 #pragma unroll
           for (int j = 0; j < 32; j++) {
@@ -254,7 +256,7 @@ __device__ __forceinline__ uint4 pack8(const float *v) {
 
 // One CTA of 128 threads per (mt, kt) tile; a thread makes the 64 k of one row.  sin(x_k) comes from
 // one FP64 sincos at the row's first bin and the rotation by delta = q * bin (4 FMAs per bin; the
-// drift over 64 bins is ~1e-14, far below the 2.4e-10 digit residual).
+// drift over 64 bins is ~1e-14, below the 1e-12 digit residual).
 __global__ void pack_sinc_digits_kernel(const double *__restrict__ q, uint32_t nq, double bin, uint32_t nh, uint32_t KT,
                                         uint8_t *__restrict__ A, size_t a_plane) {
   const uint32_t tile = blockIdx.x, mt = tile / KT, kt = tile % KT;
@@ -326,36 +328,30 @@ __global__ void max_count_kernel(const unsigned long long *__restrict__ hist, ui
 }
 
 template <int NH>
-int run_exact(xns_ctx *ctx, const unsigned long long *d_hist, uint32_t ncols, uint32_t nh, size_t ldh, uint32_t MT,
-              uint32_t KT, const uint8_t *A, size_t a_plane, double *d_G, uint32_t nq, int *flags) {
+int enqueue_exact(xns_ctx *ctx, const ExactLaunch &X) {
   using E = Exact<NH>;
   static bool attr_set = false;
   if (!attr_set) {
     XNS_CUDA(ctx, cudaFuncSetAttribute(sinc_exact_kernel<NH>, cudaFuncAttributeMaxDynamicSharedMemorySize, E::SMEM));
     attr_set = true;
   }
-  int st;
-  const uint32_t NT = (ncols + XN - 1) / XN;
-  const size_t b_plane = (size_t)NT * KT * XB;
-  void *B;
-  if ((st = xns_scratch(ctx, SLOT_TC_B, NH * b_plane, &B))) return st;
-  pack_count_digits_kernel<NH><<<NT * KT, 256, 0, ctx->stream>>>(d_hist, ncols, nh, ldh, KT, (uint8_t *)B, b_plane,
-                                                                  flags + 1);
+  pack_count_digits_kernel<NH><<<X.NT * X.KT, 256, 0, ctx->stream>>>(X.hist, X.ncols, X.nh, X.ldh, X.KT, X.B, X.b_plane,
+                                                                      X.flags + 1);
   XNS_LAUNCHED(ctx);
   XArgs g{};
-  g.A = A;
-  g.B = (const uint8_t *)B;
-  g.a_plane = a_plane;
-  g.b_plane = b_plane;
-  g.MT = MT;
-  g.NT = NT;
-  g.KT = KT;
-  g.out = d_G;
-  g.ldo = nq;
-  g.m_valid = nq;
-  g.n_valid = ncols;
-  g.err = flags;
-  const unsigned long long units = (unsigned long long)NT * MT * KT;
+  g.A = X.A;
+  g.B = X.B;
+  g.a_plane = X.a_plane;
+  g.b_plane = X.b_plane;
+  g.MT = X.MT;
+  g.NT = X.NT;
+  g.KT = X.KT;
+  g.out = X.G;
+  g.ldo = X.nq;
+  g.m_valid = X.nq;
+  g.n_valid = X.ncols;
+  g.err = X.flags;
+  const unsigned long long units = (unsigned long long)X.NT * X.MT * X.KT;
   const unsigned grid = (unsigned)std::min<unsigned long long>((unsigned long long)ctx->num_sms, units);
   sinc_exact_kernel<NH><<<grid, XTHREADS, E::SMEM, ctx->stream>>>(g);
   XNS_LAUNCHED(ctx);
@@ -364,48 +360,95 @@ int run_exact(xns_ctx *ctx, const unsigned long long *d_hist, uint32_t ncols, ui
 
 }  // namespace
 
-int xns_tc_hist_transform_exact(xns_ctx *ctx, const unsigned long long *d_hist, uint32_t ncols, uint32_t nh, size_t ldh,
-                                double bin, const double *q, uint32_t nq, double *d_G) {
+int xns_tc_exact_plan(xns_ctx *ctx, const unsigned long long *d_hist, uint32_t ncols, uint32_t nh, size_t ldh, double bin,
+                      const double *q, uint32_t nq, unsigned long long max_count, double *d_G, ExactLaunch *X) {
+  *X = ExactLaunch();
   if (!ncols || !nq) return XNS_OK;
-  const uint32_t MT = (nq + XM - 1) / XM, KT = (nh + XK - 1) / XK;
+  if (max_count >> 32) return xns_fail(ctx, XNS_ERR_LIMIT, "exact transform: a bin count reaches 2^32");
+  X->digits = (max_count >> 24) ? 4 : (max_count >> 16) ? 3 : 2;
+  X->hist = d_hist;
+  X->ncols = ncols;
+  X->nh = nh;
+  X->ldh = ldh;
+  X->nq = nq;
+  X->G = d_G;
+  X->MT = (nq + XM - 1) / XM;
+  X->KT = (nh + XK - 1) / XK;
+  X->NT = (ncols + XN - 1) / XN;
   int st;
   void *flags;
   if ((st = xns_scratch(ctx, SLOT_FLAGS, 64, &flags))) return st;
-  XNS_CUDA(ctx, cudaMemsetAsync(flags, 0, 16, ctx->stream));
-  // the largest count picks the number of count digits (one small read-back)
-  unsigned long long *d_max = (unsigned long long *)((char *)flags + 8);
-  max_count_kernel<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(d_hist, ncols, nh, ldh, d_max);
-  XNS_LAUNCHED(ctx);
-  unsigned long long maxc = 0;
-  XNS_CUDA(ctx, cudaMemcpyAsync(&maxc, d_max, 8, cudaMemcpyDeviceToHost, ctx->stream));
-  XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  if (maxc >> 24) return xns_fail(ctx, XNS_ERR_LIMIT, "exact transform: a bin count reaches 2^24");
+  X->flags = (int *)flags;
   // sinc digits: rebuilt only when the q mesh, the bin width or the K extent change
-  const size_t a_plane = (size_t)MT * KT * XA;
+  X->a_plane = (size_t)X->MT * X->KT * XA;
   void *A;
-  const bool same = ctx->x_bin == bin && ctx->x_kt == KT && ctx->x_q.size() == nq &&
-                    std::equal(q, q + nq, ctx->x_q.begin()) && ctx->slot_size[SLOT_X_A] >= NDS * a_plane;
-  if ((st = xns_scratch(ctx, SLOT_X_A, NDS * a_plane, &A))) return st;
+  const bool same = ctx->x_bin == bin && ctx->x_kt == X->KT && ctx->x_q.size() == nq &&
+                    std::equal(q, q + nq, ctx->x_q.begin()) && ctx->slot_size[SLOT_X_A] >= NDS * X->a_plane;
+  if ((st = xns_scratch(ctx, SLOT_X_A, NDS * X->a_plane, &A))) return st;
   if (!same) {
     void *dq;
     if ((st = xns_scratch(ctx, SLOT_QMESH, sizeof(double) * nq, &dq))) return st;
     XNS_CUDA(ctx, cudaMemcpyAsync(dq, q, sizeof(double) * nq, cudaMemcpyHostToDevice, ctx->stream));
-    pack_sinc_digits_kernel<<<MT * KT, XM, 0, ctx->stream>>>((const double *)dq, nq, bin, nh, KT, (uint8_t *)A, a_plane);
+    pack_sinc_digits_kernel<<<X->MT * X->KT, XM, 0, ctx->stream>>>((const double *)dq, nq, bin, nh, X->KT, (uint8_t *)A,
+                                                                    X->a_plane);
     XNS_LAUNCHED(ctx);
     ctx->x_q.assign(q, q + nq);
     ctx->x_bin = bin;
-    ctx->x_kt = KT;
+    ctx->x_kt = X->KT;
   }
-  XNS_CUDA(ctx, cudaMemsetAsync(d_G, 0, sizeof(double) * ncols * nq, ctx->stream));
-  st = (maxc >> 16) ? run_exact<3>(ctx, d_hist, ncols, nh, ldh, MT, KT, (const uint8_t *)A, a_plane, d_G, nq, (int *)flags)
-                    : run_exact<2>(ctx, d_hist, ncols, nh, ldh, MT, KT, (const uint8_t *)A, a_plane, d_G, nq, (int *)flags);
-  if (st) return st;
+  X->A = (const uint8_t *)A;
+  X->b_plane = (size_t)X->NT * X->KT * XB;
+  void *B;
+  if ((st = xns_scratch(ctx, SLOT_TC_B, X->digits * X->b_plane, &B))) return st;
+  X->B = (uint8_t *)B;
+  return XNS_OK;
+}
+
+int xns_tc_exact_enqueue(xns_ctx *ctx, const ExactLaunch &X) {
+  if (!X.ncols) return XNS_OK;
+  XNS_CUDA(ctx, cudaMemsetAsync(X.flags, 0, 2 * sizeof(int), ctx->stream));
+  XNS_CUDA(ctx, cudaMemsetAsync(X.G, 0, sizeof(double) * X.ncols * X.nq, ctx->stream));
+  switch (X.digits) {
+    case 2: return enqueue_exact<2>(ctx, X);
+    case 3: return enqueue_exact<3>(ctx, X);
+    default: return enqueue_exact<4>(ctx, X);
+  }
+}
+
+int xns_tc_exact_check(xns_ctx *ctx, const ExactLaunch &X) {
+  if (!X.ncols) return XNS_OK;
   int err[2] = {0, 0};
-  XNS_CUDA(ctx, cudaMemcpyAsync(err, flags, sizeof(err), cudaMemcpyDeviceToHost, ctx->stream));
+  XNS_CUDA(ctx, cudaMemcpyAsync(err, X.flags, sizeof(err), cudaMemcpyDeviceToHost, ctx->stream));
   XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   if (err[0]) return xns_fail(ctx, XNS_ERR_CUDA, "exact transform: a pipeline wait ran out of time");
-  if (err[1]) return xns_fail(ctx, XNS_ERR_LIMIT, "exact transform: a bin count exceeds the digit range");
+  if (err[1]) return xns_fail(ctx, XNS_ERR_LIMIT, "exact transform: a bin count exceeds the planned digits");
   return XNS_OK;
+}
+
+int xns_tc_max_count(xns_ctx *ctx, const unsigned long long *d_hist, uint32_t ncols, uint32_t nh, size_t ldh,
+                     unsigned long long *max_count) {
+  int st;
+  void *flags;
+  if ((st = xns_scratch(ctx, SLOT_FLAGS, 64, &flags))) return st;
+  unsigned long long *d_max = (unsigned long long *)((char *)flags + 8);
+  XNS_CUDA(ctx, cudaMemsetAsync(d_max, 0, 8, ctx->stream));
+  max_count_kernel<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(d_hist, ncols, nh, ldh, d_max);
+  XNS_LAUNCHED(ctx);
+  XNS_CUDA(ctx, cudaMemcpyAsync(max_count, d_max, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return XNS_OK;
+}
+
+int xns_tc_hist_transform_exact(xns_ctx *ctx, const unsigned long long *d_hist, uint32_t ncols, uint32_t nh, size_t ldh,
+                                double bin, const double *q, uint32_t nq, double *d_G) {
+  if (!ncols || !nq) return XNS_OK;
+  int st;
+  unsigned long long maxc = 0;  // the largest count picks the number of count digits
+  if ((st = xns_tc_max_count(ctx, d_hist, ncols, nh, ldh, &maxc))) return st;
+  ExactLaunch X;
+  if ((st = xns_tc_exact_plan(ctx, d_hist, ncols, nh, ldh, bin, q, nq, maxc, d_G, &X))) return st;
+  if ((st = xns_tc_exact_enqueue(ctx, X))) return st;
+  return xns_tc_exact_check(ctx, X);
 }
 
 // Host-buffer entry: as xns_hist_transform_bf16x3, with exact digit accumulation.

@@ -61,6 +61,26 @@ int xns_tc_sinc_gemm(xns_ctx *ctx, const xns_tc::GemmArgs &g, int grid);
 // context for the last q mesh / bin / extent) and multiplies.  d_G receives ncols x nq FP64.
 int xns_tc_hist_transform(xns_ctx *ctx, const unsigned long long *d_hist, uint32_t ncols, uint32_t nh, size_t ldh,
                           double bin, const double *q, uint32_t nq, double *d_G);
-// The same contraction with integer digits and exact accumulation (tc_exact.cu).
+// The exact transform in steps: the plan (sinc digit planes, count digits chosen from max_count;
+// may synchronise), the launches (memsets and kernels only: can be captured in a CUDA graph), and the
+// check of its flags.  d_G: ncols x nq FP64.
+struct ExactLaunch {
+  const unsigned long long *hist = nullptr;
+  uint32_t ncols = 0, nh = 0, nq = 0, MT = 0, NT = 0, KT = 0;
+  size_t ldh = 0, a_plane = 0, b_plane = 0;
+  int digits = 0;  // count digits: 2, 3 or 4 (counts below 2^16, 2^24, 2^32)
+  const uint8_t *A = nullptr;
+  uint8_t *B = nullptr;
+  double *G = nullptr;
+  int *flags = nullptr;
+};
+int xns_tc_exact_plan(xns_ctx *ctx, const unsigned long long *d_hist, uint32_t ncols, uint32_t nh, size_t ldh, double bin,
+                      const double *q, uint32_t nq, unsigned long long max_count, double *d_G, ExactLaunch *X);
+int xns_tc_exact_enqueue(xns_ctx *ctx, const ExactLaunch &X);
+int xns_tc_exact_check(xns_ctx *ctx, const ExactLaunch &X);
+// Largest count of ncols histogram columns (synchronises).
+int xns_tc_max_count(xns_ctx *ctx, const unsigned long long *d_hist, uint32_t ncols, uint32_t nh, size_t ldh,
+                     unsigned long long *max_count);
+// The whole contraction with integer digits and exact accumulation (tc_exact.cu).
 int xns_tc_hist_transform_exact(xns_ctx *ctx, const unsigned long long *d_hist, uint32_t ncols, uint32_t nh, size_t ldh,
                              double bin, const double *q, uint32_t nq, double *d_G);

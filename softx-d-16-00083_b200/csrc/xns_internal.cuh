@@ -32,6 +32,7 @@ enum ScratchSlot {
   SLOT_TC_B,            // split-BF16 histogram columns (hi and lo planes)
   SLOT_TC_OUT,          // FP64 sinc-transform output (columns x q)
   SLOT_X_A,             // integer-digit planes of the sinc matrix (exact transform)
+  SLOT_HFLAGS,          // histogram: out-of-range count and run queue
   SLOT_BATCH,           // batched ensemble: coordinates, schedules and per-structure tables
   SLOT_BATCH_HIST,      // batched ensemble: histograms
   SLOT_COUNT
@@ -63,7 +64,10 @@ struct xns_ctx {
   std::vector<double> x_q;
   double x_bin = 0;
   uint32_t x_kt = 0;
+  // private batch reused by the one-shot batched entry point (batch.cu)
+  struct xns_batch *batch_cache = nullptr;
 };
+void xns_batch_release_cache(xns_ctx *ctx);
 
 // One entry of the tile-pair schedule: atoms [a0, a0+na) against [b0, b0+nb) of the SoA arrays.
 // same != 0: the two ranges are the same segment and only pairs i < j count (CalcFunctions.cpp:576).

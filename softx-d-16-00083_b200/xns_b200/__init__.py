@@ -61,6 +61,18 @@ lib.xns_calc_int_partial_debye.argtypes = [_p, _PP, _p, _u32, _u32, _p, _p, _u32
 lib.xns_calc_int_2d.argtypes = [_p, _PP, _p, _u32, _p, _u32, _u32, _p, _p, _p, _u32, _dbl, _int, _PP, _p, _int, _p, _p]
 lib.xns_hist_transform_bf16x3.argtypes = [_p, _p, _u32, _u32, _dbl, _p, _u32, _p]
 lib.xns_hist_transform_exact.argtypes = [_p, _p, _u32, _u32, _dbl, _p, _u32, _p]
+_BATCH_IN = [_u32, _p, _p, _p, _u32, _dbl, _p, _u32, _int, _PP, _p, _int, _dbl]
+lib.xns_calc_batch_debye_hist.argtypes = [_p] + _BATCH_IN + [_p, _p]
+lib.xns_batch_create.argtypes = [_p] + _BATCH_IN + [_int, C.POINTER(_p)]
+lib.xns_batch_run.argtypes = [_p, _p, _p]
+lib.xns_batch_last_ms.argtypes = [_p]
+lib.xns_batch_last_ms.restype = _dbl
+lib.xns_batch_last_error.argtypes = [_p]
+lib.xns_batch_last_error.restype = C.c_char_p
+lib.xns_batch_tuning.argtypes = [_p, C.POINTER(_u32), C.POINTER(_u32)]
+lib.xns_batch_tuning.restype = _dbl
+lib.xns_batch_destroy.argtypes = [_p]
+lib.xns_batch_destroy.restype = None
 
 
 def _ptr(a):
@@ -88,6 +100,67 @@ def _rows(rows, nq):
 
 def _f64(a):
     return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+class _Ensemble:
+    """Flattens structures (each a list of per-element (n, 3) arrays) and their per-element weights into
+    the batch ABI's arrays."""
+
+    def __init__(self, structures, q, sl=None, ff=None):
+        self.nel = np.array([len(s) for s in structures], dtype=np.uint32)
+        arrs = [np.ascontiguousarray(e, dtype=np.float64).reshape(-1, 3) for s in structures for e in s]
+        self.n_el = np.array([len(a) for a in arrs], dtype=np.uint32)
+        self.xyz = np.ascontiguousarray(np.concatenate(arrs, axis=0) if arrs else np.zeros((0, 3)))
+        self.P = [int(n) * (int(n) + 1) // 2 for n in self.nel]
+        self.classes = sum(self.P)
+        self.q = _f64(q)
+        self.sl = None if sl is None else np.ascontiguousarray(np.concatenate([np.atleast_1d(w) for w in sl]), np.float64)
+        self.ffa, self.fft = (None, None) if ff is None else _rows([row for s in ff for row in s], len(self.q))
+
+    def args(self, nhist, bin, source, polar, lam):
+        return (len(self.nel), _ptr(self.nel), _ptr(self.n_el), _ptr(self.xyz), nhist, bin, _ptr(self.q), len(self.q),
+                source, self.fft, _ptr(self.sl), int(polar), lam)
+
+
+class Batch:
+    """A planned ensemble with its launches captured in a CUDA graph (xns_batch_create)."""
+
+    def __init__(self, ctx, structures, nhist, bin, q, source, sl=None, ff=None, polar=False, lam=0.0, autotune=False):
+        self._ens = _Ensemble(structures, q, sl, ff)
+        self.nhist = nhist
+        self._h = _p()
+        st = lib.xns_batch_create(ctx.handle, *self._ens.args(nhist, bin, source, polar, lam), int(autotune),
+                                  C.byref(self._h))
+        if st:
+            raise XnsError(st, lib.xns_last_error(ctx.handle).decode())
+
+    def run(self, want_hist=False):
+        I = np.zeros((len(self._ens.nel), len(self._ens.q)))
+        h = np.zeros(self._ens.classes * self.nhist, dtype=np.uint64) if want_hist else None
+        st = lib.xns_batch_run(self._h, _ptr(I), _ptr(h))
+        if st:
+            raise XnsError(st, lib.xns_batch_last_error(self._h).decode())
+        return (I, h) if want_hist else I
+
+    @property
+    def last_ms(self):
+        return lib.xns_batch_last_ms(self._h)
+
+    def tuning(self):
+        ct, wb = _u32(), _u32()
+        ms = lib.xns_batch_tuning(self._h, C.byref(ct), C.byref(wb))
+        return int(ct.value), int(wb.value), ms
+
+    def close(self):
+        if self._h:
+            lib.xns_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Context:
@@ -159,6 +232,18 @@ class Context:
         self._check(lib.xns_calc_pdf(self._h, _ptr(hist), _ptr(n_el), len(n_el), nhist, bin, pdftype, p0, _ptr(sl),
                                      _ptr(out)))
         return out
+
+    def calc_batch_debye_hist(self, structures, nhist, bin, q, source, sl=None, ff=None, polar=False, lam=0.0,
+                              want_hist=False):
+        """I(q) (nstruct x nq) of an ensemble in one pass; sl / ff are per structure, per element."""
+        ens = _Ensemble(structures, q, sl, ff)
+        I = np.zeros((len(ens.nel), len(ens.q)))
+        h = np.zeros(ens.classes * nhist, dtype=np.uint64) if want_hist else None
+        self._check(lib.xns_calc_batch_debye_hist(self._h, *ens.args(nhist, bin, source, polar, lam), _ptr(I), _ptr(h)))
+        return (I, h) if want_hist else I
+
+    def batch(self, structures, nhist, bin, q, source, sl=None, ff=None, polar=False, lam=0.0, autotune=False):
+        return Batch(self, structures, nhist, bin, q, source, sl, ff, polar, lam, autotune)
 
     def hist_transform(self, hist, bin, q, scheme="exact"):
         """G[c, i] = sum_k hist[c, k] sin(q_i r_k)/(q_i r_k) on the tensor cores: scheme "bf16x3" (split

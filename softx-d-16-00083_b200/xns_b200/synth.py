@@ -34,6 +34,23 @@ def fcc_sphere(n=5000, a=4.078, sigma=0.05, seed=0):
     return [xyz]
 
 
+def sphere_ensemble(count=256, nmin=1000, nmax=200000, a=4.078, smin=0.02, smax=0.1, seed=0):
+    """count fcc spheres (one element each) with atom counts log-uniform in [nmin, nmax] and their own
+    Gaussian displacement sigma uniform in [smin, smax]: the n sites nearest the lattice centre, as
+    fcc_sphere, sorted once for all.  Returns (structures, atom counts, sigmas)."""
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(np.log(nmin), np.log(nmax), count)).astype(np.int64)
+    sig = rng.uniform(smin, smax, count)
+    m = int(np.ceil((ns.max() / 4 * 6 / np.pi) ** (1 / 3))) + 3
+    sites = _fcc_cells(m) * a
+    c = sites.mean(axis=0)
+    d2 = ((sites - c) ** 2).sum(axis=1)
+    order = np.lexsort((np.arange(len(sites)), np.round(d2, 9)))[:ns.max()]
+    base = sites[order] - c
+    structs = [[base[:n] + rng.normal(0.0, s, size=(n, 3))] for n, s in zip(ns, sig)]
+    return structs, ns, sig
+
+
 def rocksalt_cube(cells=30, a=5.64, vacancy=0.1, sigma=0.07, seed=0):
     """Rock-salt cube of cells^3 unit cells; species 0 (Na) on the fcc sites, species 1 (Cl) on the
     half-shifted ones.  Returns [na, cl]."""

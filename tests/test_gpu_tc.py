@@ -41,15 +41,17 @@ def test_transform_vs_fp64(gpu_ctx, scheme, tol, ncols, nh, nq):
     assert col_err(G, G64) < tol
 
 
-def test_exact_large_counts(gpu_ctx):
-    """Counts beyond 2^16 switch the exact transform to three count digits; 2^24 is refused."""
+@pytest.mark.parametrize("top", [1 << 24, 1 << 31])
+def test_exact_large_counts(gpu_ctx, top):
+    """Counts beyond 2^16 / 2^24 switch the exact transform to three / four count digits; 2^32 is
+    refused."""
     import xns_b200
     rng = np.random.default_rng(8)
-    H = rng.integers(0, 1 << 24, size=(2, 900)).astype(np.uint64)
+    H = rng.integers(0, top, size=(2, 900)).astype(np.uint64)
     q = synth.q_mesh(0.1, 10.0, 200)
     G64 = H.astype(np.float64) @ sinc_matrix(q, 900, 0.01).T
     assert col_err(gpu_ctx.hist_transform(H, 0.01, q, "exact"), G64) < 1e-8
-    H[1, 5] = 1 << 24
+    H[1, 5] = 1 << 32
     with pytest.raises(xns_b200.XnsError) as e:
         gpu_ctx.hist_transform(H, 0.01, q, "exact")
     assert e.value.status == 6
