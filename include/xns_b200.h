@@ -205,6 +205,38 @@ const char *xns_batch_last_error(const xns_batch *b);
 double xns_batch_tuning(const xns_batch *b, uint32_t *cell_target, uint32_t *window_bins);
 void xns_batch_destroy(xns_batch *b);
 
+/* ---- learned binning correction: a small MLP trained on the GPU ------------------------------------ */
+
+/* No reference counterpart.  A 3-layer perceptron y = W3 gelu(W2 gelu(W1 x + b1) + b2) + b3 with FP32
+ * master weights used in BF16 by hand-written forward and backward kernels (FP32 accumulation), trained
+ * with Adam on a mean weighted squared error.  dims = {in, hidden, hidden, out}.  Parameters are laid
+ * out W1 (hidden x in, row-major), b1, W2, b2, W3, b3.  x, t, y, grad are host buffers; w (per output
+ * column loss weights) may be NULL.  The network owns a private context on the caller's device. */
+typedef struct xns_mlp xns_mlp;
+int xns_mlp_create(xns_ctx *ctx, const int *dims, uint64_t seed, xns_mlp **out);
+void xns_mlp_destroy(xns_mlp *m);
+const char *xns_mlp_last_error(const xns_mlp *m);
+long xns_mlp_param_count(const xns_mlp *m);
+int xns_mlp_get_params(xns_mlp *m, float *params);
+int xns_mlp_set_params(xns_mlp *m, const float *params);
+int xns_mlp_forward(xns_mlp *m, const float *x, int batch, float *y);
+int xns_mlp_gradients(xns_mlp *m, const float *x, const float *t, const float *w, int batch, float *grad,
+                      double *loss);
+int xns_mlp_train(xns_mlp *m, const float *x, const float *t, const float *w, int n, int batch, int epochs, float lr,
+                  double *loss);
+
+/* Kernels of the learned correction.  h: a structure's weighted coarse histogram normalised by N s0
+ * (so that I = s0 [1 + sum_k h_k sin(q r_k)/(q r_k)]), nh bins of width bin.
+ * xns_binning_features: per bin the perceptron's XNS_BINNING_FEATURES inputs (log(1 + h) of the bin and
+ * its 4 neighbours on each side, the neighbours' ratios to the bin, the bin position), X: nh x 18.
+ * xns_binning_correction: dI(q) = s0 sum_k h_k [mu1_k D S'(q r_k) + m2_k D^2/2 S''(q r_k)], the second
+ * order Taylor correction for within-bin offsets with moments mu = (mu1, m2) per bin (nh x 2, in units
+ * of the bin width D); S = sin(q r)/(q r). */
+#define XNS_BINNING_FEATURES 18
+int xns_binning_features(xns_ctx *ctx, const double *h, uint32_t nh, float *X);
+int xns_binning_correction(xns_ctx *ctx, const double *h, const float *mu, uint32_t nh, double bin, const double *q,
+                           uint32_t nq, double s0, double *dI);
+
 /* ---- utilities (no reference counterpart) -------------------------------------------------------- */
 
 /* Measured FMA-pipe throughput of this device in TFLOP/s (an FMA counts 2 flops): FP64 when fp64 != 0,

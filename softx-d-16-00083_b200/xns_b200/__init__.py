@@ -73,6 +73,20 @@ lib.xns_batch_tuning.argtypes = [_p, C.POINTER(_u32), C.POINTER(_u32)]
 lib.xns_batch_tuning.restype = _dbl
 lib.xns_batch_destroy.argtypes = [_p]
 lib.xns_batch_destroy.restype = None
+lib.xns_mlp_create.argtypes = [_p, _p, C.c_uint64, C.POINTER(_p)]
+lib.xns_mlp_destroy.argtypes = [_p]
+lib.xns_mlp_destroy.restype = None
+lib.xns_mlp_last_error.argtypes = [_p]
+lib.xns_mlp_last_error.restype = C.c_char_p
+lib.xns_mlp_param_count.argtypes = [_p]
+lib.xns_mlp_param_count.restype = C.c_long
+lib.xns_mlp_get_params.argtypes = [_p, _p]
+lib.xns_mlp_set_params.argtypes = [_p, _p]
+lib.xns_mlp_forward.argtypes = [_p, _p, _int, _p]
+lib.xns_mlp_gradients.argtypes = [_p, _p, _p, _p, _int, _p, C.POINTER(_dbl)]
+lib.xns_mlp_train.argtypes = [_p, _p, _p, _p, _int, _int, _int, C.c_float, C.POINTER(_dbl)]
+lib.xns_binning_features.argtypes = [_p, _p, _u32, _p]
+lib.xns_binning_correction.argtypes = [_p, _p, _p, _u32, _dbl, _p, _u32, _dbl, _p]
 
 
 def _ptr(a):
@@ -154,6 +168,69 @@ class Batch:
     def close(self):
         if self._h:
             lib.xns_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class MLP:
+    """The learned correction's perceptron on the GPU (xns_mlp_*): dims = (in, hidden, hidden, out)."""
+
+    def __init__(self, ctx, dims, seed=0):
+        self.dims = tuple(int(d) for d in dims)
+        d = np.array(self.dims, dtype=np.int32)
+        self._h = _p()
+        st = lib.xns_mlp_create(ctx.handle, _ptr(d), seed, C.byref(self._h))
+        if st:
+            raise XnsError(st, lib.xns_last_error(ctx.handle).decode())
+
+    def _check(self, st):
+        if st:
+            raise XnsError(st, lib.xns_mlp_last_error(self._h).decode())
+
+    @property
+    def nparams(self):
+        return int(lib.xns_mlp_param_count(self._h))
+
+    def get_params(self):
+        p = np.zeros(self.nparams, dtype=np.float32)
+        self._check(lib.xns_mlp_get_params(self._h, _ptr(p)))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        self._check(lib.xns_mlp_set_params(self._h, _ptr(p)))
+
+    def forward(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.zeros((x.shape[0], self.dims[3]), dtype=np.float32)
+        self._check(lib.xns_mlp_forward(self._h, _ptr(x), x.shape[0], _ptr(y)))
+        return y
+
+    def gradients(self, x, t, w=None):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        w = None if w is None else np.ascontiguousarray(w, dtype=np.float32)
+        g = np.zeros(self.nparams, dtype=np.float32)
+        loss = C.c_double()
+        self._check(lib.xns_mlp_gradients(self._h, _ptr(x), _ptr(t), _ptr(w), x.shape[0], _ptr(g), C.byref(loss)))
+        return loss.value, g
+
+    def train(self, x, t, w=None, batch=128, epochs=1, lr=1e-3):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        w = None if w is None else np.ascontiguousarray(w, dtype=np.float32)
+        loss = C.c_double()
+        self._check(lib.xns_mlp_train(self._h, _ptr(x), _ptr(t), _ptr(w), x.shape[0], batch, epochs, lr, C.byref(loss)))
+        return loss.value
+
+    def close(self):
+        if self._h:
+            lib.xns_mlp_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -93,3 +93,36 @@ def test_oracle_vs_reference_seeded():
         assert np.array_equal(O.hist(els, nh, bin), R.hist(els, nh, bin))
     q = synth.q_mesh(0.3, 15, 96)
     assert rel_err(O.int_debye(els, q, 0, sl=[1.0, -2.0]), R.int_debye(els, q, 0, sl=[1.0, -2.0])) < 1e-11
+
+
+def test_mlp_oracle_gradients_by_finite_differences():
+    """The perceptron oracle's analytic gradient against central differences (FP64, BF16 weights held
+    fixed by perturbing only the biases and a few BF16-exact weight steps)."""
+    import mlp_oracle
+    dims = (5, 7, 6, 3)
+    rng = np.random.default_rng(0)
+    n = 7 * 5 + 7 + 6 * 7 + 6 + 3 * 6 + 3
+    p = rng.normal(size=n).astype(np.float32)
+    x, t = rng.normal(size=(4, 5)), rng.normal(size=(4, 3))
+    w = np.array([1.0, 2.0, 0.5])
+    loss, g = mlp_oracle.gradients(p, dims, x, t, w)
+    # biases are used in FP64 as given: perturb them directly
+    bias_idx = list(range(35, 42)) + list(range(84, 90)) + list(range(108, 111))
+    for i in bias_idx:
+        e = np.zeros(n)
+        e[i] = 1e-4
+        lp, _ = mlp_oracle.gradients(p.astype(np.float64) + e, dims, x, t, w)
+        lm, _ = mlp_oracle.gradients(p.astype(np.float64) - e, dims, x, t, w)
+        assert abs((lp - lm) / 2e-4 - g[i]) < 1e-6 * max(1.0, abs(g[i]))
+    # weights go through BF16 rounding: step by exactly one BF16 ulp of 1.0 on weights equal to 1.0
+    q = p.copy()
+    for i in (0, 50, 95):
+        q[i] = 1.0
+    _, gq = mlp_oracle.gradients(q, dims, x, t, w)
+    for i in (0, 50, 95):
+        h = 2.0 ** -7
+        qp, qm = q.copy(), q.copy()
+        qp[i], qm[i] = 1.0 + h, 1.0 - h
+        lp, _ = mlp_oracle.gradients(qp, dims, x, t, w)
+        lm, _ = mlp_oracle.gradients(qm, dims, x, t, w)
+        assert abs((lp - lm) / (2 * h) - gq[i]) < 2e-2 * max(1.0, abs(gq[i]))
