@@ -167,6 +167,20 @@ int xns_hist_transform_bf16x3(xns_ctx *ctx, const uint64_t *hist, uint32_t ncols
 int xns_hist_transform_exact(xns_ctx *ctx, const uint64_t *hist, uint32_t ncols, uint32_t nh, double bin,
                              const double *q, uint32_t nq, double *G);
 
+/* ---- 2D intensity on a flat Cartesian q plane ------------------------------------------------------ */
+
+/* The calcInt2D amplitude (CalcFunctions.cpp:1026-1046) for the detector plane normal to the beam in the
+ * limit of a flat Ewald surface: I[iy * nqx + ix] = |sum_e f_e(|q|) sum_{j in e} exp(i (qx x_j + qy y_j))|^2
+ * / N with qx = qx0 + ix dqx, qy = qy0 + iy dqy; coordinates as given (pre-rotate them for another
+ * orientation).  Since exp(i (qx x + qy y)) factorises, the sum is a complex matrix product over atoms,
+ * run on the tensor cores with three integer digits per cos / sin value and exact accumulation (error
+ * ~1e-7 of |A|^2).  X-ray: coef holds 9 numbers per element, f(q) = sum_k a_k exp(-b_k (q/4pi)^2) + c
+ * as (a1..a4, b1..b4, c); neutron: sl.  No counterpart entry in the reference (its 2D mesh is polar on
+ * the Ewald sphere: xns_calc_int_2d). */
+int xns_calc_amp_plane(xns_ctx *ctx, const double *const *xyz_el, const uint32_t *n_el, uint32_t nel, double qx0,
+                       double dqx, uint32_t nqx, double qy0, double dqy, uint32_t nqy, int source, const double *coef,
+                       const double *sl, double *I);
+
 /* ---- batched ensembles ------------------------------------------------------------------------------ */
 
 /* No reference counterpart as one call: the reference evaluates one structure per run.  Per structure

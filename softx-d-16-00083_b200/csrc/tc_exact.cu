@@ -39,27 +39,38 @@ constexpr int CH_TILES = 2;                // k tiles per exact chunk (CH_K = 12
 constexpr int XTHREADS = 320;
 constexpr uint32_t XTMEM_COLS = 512;
 
-template <int NH>
-struct Exact {
-  static constexpr int NL = NDS + NH - 1;  // levels NH-1 .. -(NDS-1)
-  static constexpr int STAGE = NDS * XA + NH * XB;
+// A digit scheme: NA digit planes of the A operand, NB of the B operand, NL accumulator levels, and the
+// level of the product of A digit i with B digit j (-1: dropped; 0 is the most significant level).
+//   KIND 0 (sinc transform): A = sinc digits, B = count digits, every product kept, level
+//          (NB-1) - (j - i);
+//   KIND 1 (plane amplitude): A and B = cos / sin digits, products of level i + j < NL kept.
+template <int NA_, int NB_, int NL_, int KIND>
+struct Scheme {
+  static constexpr int NA = NA_, NB = NB_, NL = NL_;
+  static constexpr int STAGE = NA * XA + NB * XB;
   static constexpr int SMEM = XSTAGES * STAGE + 1024;
   static_assert(NL * XN <= (int)XTMEM_COLS, "levels must fit in tensor memory");
+  static_assert(SMEM <= 232448, "stages must fit in shared memory");
+  __host__ __device__ static constexpr int level(int i, int j) {
+    return KIND == 0 ? (NB - 1) - (j - i) : (i + j < NL ? i + j : -1);
+  }
 };
+template <int NH>
+using SincScheme = Scheme<NDS, NH, NDS + NH - 1, 0>;
 
 struct XArgs {
-  const uint8_t *A;  // NDS digit planes of MT*KT tiles, plane stride a_plane bytes
-  const uint8_t *B;  // NH digit planes of NT*KT tiles, plane stride b_plane bytes
+  const uint8_t *A;  // NA digit planes of MT*KT tiles, plane stride a_plane bytes
+  const uint8_t *B;  // NB digit planes of NT*KT tiles, plane stride b_plane bytes
   size_t a_plane, b_plane;
   uint32_t MT, NT, KT;
   double *out;
   uint32_t ldo, m_valid, n_valid;
+  double scale;  // value of one unit of the Horner sum over the levels
   int *err;
 };
 
-template <int NH>
+template <class E>
 __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) {
-  using E = Exact<NH>;
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) unsigned long long bars[2 * XSTAGES + 3];
   __shared__ uint32_t tmem_sh;
@@ -115,9 +126,9 @@ __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) 
         const size_t ao = ((size_t)mt * g.KT + kt) * XA, bo = ((size_t)nt * g.KT + kt) * XB;
         mbar_expect_tx(bar, (uint32_t)E::STAGE);
 #pragma unroll
-        for (int d = 0; d < NDS; d++) bulk_g2s(dst + d * XA, g.A + d * g.a_plane + ao, XA, bar);
+        for (int d = 0; d < E::NA; d++) bulk_g2s(dst + d * XA, g.A + d * g.a_plane + ao, XA, bar);
 #pragma unroll
-        for (int e = 0; e < NH; e++) bulk_g2s(dst + NDS * XA + e * XB, g.B + e * g.b_plane + bo, XB, bar);
+        for (int e = 0; e < E::NB; e++) bulk_g2s(dst + E::NA * XA + e * XB, g.B + e * g.b_plane + bo, XB, bar);
         fills[s] = k + 1;
       }
       if (*abort)
@@ -151,16 +162,17 @@ __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) 
           break;
         }
         tc_fence_after();
-        const uint32_t a0 = base + s * E::STAGE, b0 = a0 + NDS * XA;
+        const uint32_t a0 = base + s * E::STAGE, b0 = a0 + E::NA * XA;
 #pragma unroll
         for (int ks = 0; ks < XK / 16; ks++) {
           const uint32_t off = ks * 32;
           uint32_t written = 0;
 #pragma unroll
-          for (int di = 0; di < NDS; di++) {
+          for (int di = 0; di < E::NA; di++) {
 #pragma unroll
-            for (int ej = 0; ej < NH; ej++) {
-              const int lev = (NH - 1) - (ej - di);  // 0 = top level
+            for (int ej = 0; ej < E::NB; ej++) {
+              const int lev = E::level(di, ej);  // 0 = top level
+              if (lev < 0) continue;
               const uint32_t acc = (first && ks == 0 && !(written & (1u << lev))) ? 0u : 1u;
               written |= 1u << lev;
               tc_mma(tmem + lev * XN, sw128_desc(a0 + di * XA + off), sw128_desc(b0 + ej * XB + off), idesc, acc);
@@ -222,8 +234,7 @@ __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) 
         const unsigned long long r = u / KT;
         const uint32_t mt = (uint32_t)(r % g.MT), nt = (uint32_t)(r / g.MT);
         const uint32_t m = mt * XM + wq * 32 + lane;
-        // level l holds 256^(NH-1-l)/128; Horner gave 256^(NL-1-l): scale 256^(NH-NL)/128
-        const double scale = ldexp(1.0, -8 * (NDS - 1)) / 128.0;  // NL - NH = NDS - 1 -> 256^-(NDS-1)
+        const double scale = g.scale;
         if (m < g.m_valid) {
 #pragma unroll
           for (int j = 0; j < 32; j++) {
@@ -327,14 +338,24 @@ __global__ void max_count_kernel(const unsigned long long *__restrict__ hist, ui
   if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
 }
 
-template <int NH>
-int enqueue_exact(xns_ctx *ctx, const ExactLaunch &X) {
-  using E = Exact<NH>;
+// Launches the digit GEMM of scheme E; grid 0: one CTA per SM (stream-K over all units), otherwise the
+// given number of CTAs.
+template <class E>
+int launch_digit_gemm(xns_ctx *ctx, const XArgs &g, unsigned grid) {
   static bool attr_set = false;
   if (!attr_set) {
-    XNS_CUDA(ctx, cudaFuncSetAttribute(sinc_exact_kernel<NH>, cudaFuncAttributeMaxDynamicSharedMemorySize, E::SMEM));
+    XNS_CUDA(ctx, cudaFuncSetAttribute(sinc_exact_kernel<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, E::SMEM));
     attr_set = true;
   }
+  const unsigned long long units = (unsigned long long)g.NT * g.MT * g.KT;
+  if (!grid) grid = (unsigned)std::min<unsigned long long>((unsigned long long)ctx->num_sms, units);
+  sinc_exact_kernel<E><<<grid, XTHREADS, E::SMEM, ctx->stream>>>(g);
+  XNS_LAUNCHED(ctx);
+  return XNS_OK;
+}
+
+template <int NH>
+int enqueue_exact(xns_ctx *ctx, const ExactLaunch &X) {
   pack_count_digits_kernel<NH><<<X.NT * X.KT, 256, 0, ctx->stream>>>(X.hist, X.ncols, X.nh, X.ldh, X.KT, X.B, X.b_plane,
                                                                       X.flags + 1);
   XNS_LAUNCHED(ctx);
@@ -351,11 +372,97 @@ int enqueue_exact(xns_ctx *ctx, const ExactLaunch &X) {
   g.m_valid = X.nq;
   g.n_valid = X.ncols;
   g.err = X.flags;
-  const unsigned long long units = (unsigned long long)X.NT * X.MT * X.KT;
-  const unsigned grid = (unsigned)std::min<unsigned long long>((unsigned long long)ctx->num_sms, units);
-  sinc_exact_kernel<NH><<<grid, XTHREADS, E::SMEM, ctx->stream>>>(g);
-  XNS_LAUNCHED(ctx);
-  return XNS_OK;
+  // level l holds 256^(NH-1-l)/128; the Horner sum weights it 256^(NL-1-l): one unit is 256^-(NDS-1)/128
+  g.scale = ldexp(1.0, -8 * (NDS - 1)) / 128.0;
+  return launch_digit_gemm<SincScheme<NH>>(ctx, g, 0);
+}
+
+// ---- 2D amplitude on a Cartesian q plane ---------------------------------------------------------
+//
+// A_e(qx, qy) = sum_{j in e} exp(i (qx x_j + qy y_j)) factorises into cos / sin of qx x_j and qy y_j,
+// so Re A_e and Im A_e are one real GEMM over k = 2 n_e: A rows are qx with columns
+// [cos(qx x_j) | sin(qx x_j)], B rows are first qy for Re with [cos(qy y_j) | -sin(qy y_j)], then qy for
+// Im with [sin(qy y_j) | cos(qy y_j)].  Values in [-1, 1] (FP64 sines) become PD base-256 digits
+// (d/128 + d'/128/256 + ...) and the digit products of level i + j < PD are summed exactly
+// (PlaneScheme).  Three digits (residual 2^-24) leave 1e-5..3e-5 of I at the dim points of a crystal's
+// pattern, where the rounding of the lattice's repeated phases adds coherently; four leave 2^-32.
+constexpr int PD = 4;
+using PlaneScheme = Scheme<PD, PD, PD, 1>;
+
+__device__ __forceinline__ void put_digits(uint8_t *plane0, size_t plane, size_t off, double v) {
+  double r = v * 128.0;
+#pragma unroll
+  for (int d = 0; d < PD; d++) {
+    const double di = rint(r);
+    *reinterpret_cast<__nv_bfloat16 *>(plane0 + d * plane + off) = __float2bfloat16_rn((float)di);
+    r = (r - di) * 256.0;
+  }
+}
+
+// One CTA of 64 threads per (mt, kt) tile of the qx operand; thread = column k; the 128 rows come from
+// one FP64 sincos and the rotation by dq x (FP64, drift ~1e-14 over 128 rows).
+__global__ void plane_pack_a_kernel(const double *__restrict__ x, uint32_t n, double q0, double dq, uint32_t nq,
+                                    uint32_t KT, uint8_t *__restrict__ A, size_t a_plane) {
+  const uint32_t tile = blockIdx.x, mt = tile / KT, kt = tile % KT, kk = threadIdx.x, k = kt * XK + kk;
+  const bool use = k < 2 * n, is_sin = k >= n;
+  const double xj = use ? x[is_sin ? k - n : k] : 0.0;
+  double s, c, sd, cd;
+  sincos((q0 + (double)(mt * XM) * dq) * xj, &s, &c);
+  sincos(dq * xj, &sd, &cd);
+  uint8_t *t0 = A + (size_t)tile * XA;
+  for (uint32_t row = 0; row < XM; row++) {
+    const bool valid = use && mt * XM + row < nq;
+    put_digits(t0, a_plane, xns_tc::sw128_offset(row, kk), valid ? (is_sin ? s : c) : 0.0);
+    const double s1 = fma(s, cd, c * sd), c1 = fma(c, cd, -(s * sd));
+    s = s1;
+    c = c1;
+  }
+}
+
+// One CTA of 64 threads per (nt, kt) tile of the qy operand (rows: qy for Re, then qy for Im).
+__global__ void plane_pack_b_kernel(const double *__restrict__ y, uint32_t n, double q0, double dq, uint32_t nq,
+                                    uint32_t KT, uint8_t *__restrict__ B, size_t b_plane) {
+  const uint32_t tile = blockIdx.x, nt = tile / KT, kt = tile % KT, kk = threadIdx.x, k = kt * XK + kk;
+  const bool use = k < 2 * n, second = k >= n;
+  const double yj = use ? y[second ? k - n : k] : 0.0;
+  double s = 0, c = 1, sd, cd;
+  sincos(dq * yj, &sd, &cd);
+  uint8_t *t0 = B + (size_t)tile * XB;
+  for (uint32_t row = 0; row < XN; row++) {
+    const uint32_t np = nt * XN + row, part = np >= nq ? 1u : 0u, iy = np - part * nq;
+    if (row == 0 || iy == 0) sincos((q0 + (double)iy * dq) * yj, &s, &c);  // new run of qy
+    double v = 0.0;
+    if (use && np < 2 * nq) v = part == 0 ? (second ? -s : c) : (second ? c : s);
+    put_digits(t0, b_plane, xns_tc::sw128_offset(row, kk), v);
+    const double s1 = fma(s, cd, c * sd), c1 = fma(c, cd, -(s * sd));
+    s = s1;
+    c = c1;
+  }
+}
+
+// Ar/Ai (nqy x nqx) += f_e(|q|) * (Re, Im) of one element; f from 4-Gaussian coefficients (X-ray) or a
+// scattering length.
+__global__ void plane_accum_kernel(const double *__restrict__ C, uint32_t nqx, uint32_t nqy, double qx0, double dqx,
+                                   double qy0, double dqy, const double *__restrict__ coef, double sl,
+                                   double *__restrict__ Ar, double *__restrict__ Ai) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)nqx * nqy) return;
+  const uint32_t iy = (uint32_t)(i / nqx), ix = (uint32_t)(i % nqx);
+  double f = sl;
+  if (coef) {
+    const double qx = qx0 + ix * dqx, qy = qy0 + iy * dqy, qm = sqrt(qx * qx + qy * qy);
+    const double s2 = (qm / (4.0 * XNS_PI)) * (qm / (4.0 * XNS_PI));
+    f = coef[0] * exp(-coef[4] * s2) + coef[1] * exp(-coef[5] * s2) + coef[2] * exp(-coef[6] * s2) +
+        coef[3] * exp(-coef[7] * s2) + coef[8];
+  }
+  Ar[i] += f * C[(size_t)iy * nqx + ix];
+  Ai[i] += f * C[(size_t)(nqy + iy) * nqx + ix];
+}
+
+__global__ void plane_intensity_kernel(const double *__restrict__ Ar, const double *__restrict__ Ai, size_t n, double inv_n,
+                                       double *__restrict__ I) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) I[i] = (Ar[i] * Ar[i] + Ai[i] * Ai[i]) * inv_n;
 }
 
 }  // namespace
@@ -469,5 +576,83 @@ extern "C" int xns_hist_transform_exact(xns_ctx *ctx, const uint64_t *hist, uint
   if ((st = xns_timer_stop(ctx))) return st;
   XNS_CUDA(ctx, cudaMemcpyAsync(G, dG, sizeof(double) * ncols * nq, cudaMemcpyDeviceToHost, ctx->stream));
   XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return XNS_OK;
+}
+
+// I[iy * nqx + ix] = |sum_e f_e(|q|) sum_{j in e} exp(i (qx x_j + qy y_j))|^2 / N on the plane
+// qx = qx0 + ix dqx, qy = qy0 + iy dqy (coordinates as given: rotate them first for another
+// orientation).  coef: 9 coefficients per element (X-ray) or null with sl (neutron).
+extern "C" int xns_calc_amp_plane(xns_ctx *ctx, const double *const *xyz_el, const uint32_t *n_el, uint32_t nel,
+                                  double qx0, double dqx, uint32_t nqx, double qy0, double dqy, uint32_t nqy, int source,
+                                  const double *coef, const double *sl, double *I) {
+  if (!ctx) return XNS_ERR_ARG;
+  if (!I || nqx == 0 || nqy == 0) return xns_fail(ctx, XNS_ERR_ARG, "plane: null output or empty mesh");
+  if (source == XNS_XRAY ? !coef : !sl) return xns_fail(ctx, XNS_ERR_ARG, "plane: missing form factors / lengths");
+  int st;
+  DevCoords dc;
+  if ((st = xns_upload_coords(ctx, xyz_el, n_el, nel, &dc))) return st;
+  if (dc.ntot == 0) return xns_fail(ctx, XNS_ERR_ARG, "plane: no atoms");
+  const size_t npix = (size_t)nqx * nqy;
+  void *vacc, *vC, *vI, *vcoef = nullptr, *flags;
+  if ((st = xns_scratch(ctx, SLOT_OUT, sizeof(double) * 2 * npix, &vacc))) return st;
+  if ((st = xns_scratch(ctx, SLOT_TC_OUT, sizeof(double) * 2 * npix, &vC))) return st;
+  if ((st = xns_scratch(ctx, SLOT_OUT2, sizeof(double) * npix, &vI))) return st;
+  if ((st = xns_scratch(ctx, SLOT_FLAGS, 64, &flags))) return st;
+  if (source == XNS_XRAY) {
+    if ((st = xns_scratch(ctx, SLOT_WEIGHTS, sizeof(double) * 9 * nel, &vcoef))) return st;
+    XNS_CUDA(ctx, cudaMemcpyAsync(vcoef, coef, sizeof(double) * 9 * nel, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  double *Ar = (double *)vacc, *Ai = Ar + npix;
+  if ((st = xns_timer_start(ctx))) return st;
+  if ((st = xns_stage_begin(ctx, STAGE_2D))) return st;
+  XNS_CUDA(ctx, cudaMemsetAsync(vacc, 0, sizeof(double) * 2 * npix, ctx->stream));
+  XNS_CUDA(ctx, cudaMemsetAsync(flags, 0, sizeof(int), ctx->stream));
+  const uint32_t MT = (nqx + XM - 1) / XM, NT = (2 * nqy + XN - 1) / XN;
+  for (uint32_t e = 0; e < nel; e++) {
+    const uint32_t n = dc.n_el[e];
+    if (!n) continue;
+    const uint32_t KT = (2 * n + XK - 1) / XK;
+    const size_t a_plane = (size_t)MT * KT * XA, b_plane = (size_t)NT * KT * XB;
+    void *A, *B;
+    if ((st = xns_scratch(ctx, SLOT_X_A, PD * a_plane, &A))) return st;
+    if ((st = xns_scratch(ctx, SLOT_TC_B, PD * b_plane, &B))) return st;
+    ctx->x_q.clear();  // the sinc-digit cache of the histogram transform shares SLOT_X_A
+    const double *xe = dc.x + dc.off_el[e], *ye = dc.y + dc.off_el[e];
+    plane_pack_a_kernel<<<MT * KT, XK, 0, ctx->stream>>>(xe, n, qx0, dqx, nqx, KT, (uint8_t *)A, a_plane);
+    XNS_LAUNCHED(ctx);
+    plane_pack_b_kernel<<<NT * KT, XK, 0, ctx->stream>>>(ye, n, qy0, dqy, nqy, KT, (uint8_t *)B, b_plane);
+    XNS_LAUNCHED(ctx);
+    XNS_CUDA(ctx, cudaMemsetAsync(vC, 0, sizeof(double) * 2 * npix, ctx->stream));
+    XArgs g{};
+    g.A = (const uint8_t *)A;
+    g.B = (const uint8_t *)B;
+    g.a_plane = a_plane;
+    g.b_plane = b_plane;
+    g.MT = MT;
+    g.NT = NT;
+    g.KT = KT;
+    g.out = (double *)vC;
+    g.ldo = nqx;
+    g.m_valid = nqx;
+    g.n_valid = 2 * nqy;
+    g.scale = ldexp(1.0, -14 - 8 * (PD - 1));  // (1/128)^2 per unit of level 0, Horner over PD levels
+    g.err = (int *)flags;
+    // one CTA per output tile: CTAs that run together read the same k tiles, which stay in L2
+    if ((st = launch_digit_gemm<PlaneScheme>(ctx, g, MT * NT))) return st;
+    plane_accum_kernel<<<(unsigned)((npix + 255) / 256), 256, 0, ctx->stream>>>(
+        (const double *)vC, nqx, nqy, qx0, dqx, qy0, dqy, vcoef ? (const double *)vcoef + 9 * e : nullptr,
+        vcoef ? 0.0 : sl[e], Ar, Ai);
+    XNS_LAUNCHED(ctx);
+  }
+  plane_intensity_kernel<<<(unsigned)((npix + 255) / 256), 256, 0, ctx->stream>>>(Ar, Ai, npix, 1.0 / dc.ntot,
+                                                                                  (double *)vI);
+  XNS_LAUNCHED(ctx);
+  if ((st = xns_stage_end(ctx, STAGE_2D))) return st;
+  if ((st = xns_timer_stop(ctx))) return st;
+  int err = 0;
+  XNS_CUDA(ctx, cudaMemcpyAsync(&err, flags, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  XNS_CUDA(ctx, cudaMemcpyAsync(I, vI, sizeof(double) * npix, cudaMemcpyDeviceToHost, ctx->stream));
+  XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (err) return xns_fail(ctx, XNS_ERR_CUDA, "plane: a pipeline wait ran out of time");
   return XNS_OK;
 }

@@ -85,6 +85,7 @@ lib.xns_mlp_set_params.argtypes = [_p, _p]
 lib.xns_mlp_forward.argtypes = [_p, _p, _int, _p]
 lib.xns_mlp_gradients.argtypes = [_p, _p, _p, _p, _int, _p, C.POINTER(_dbl)]
 lib.xns_mlp_train.argtypes = [_p, _p, _p, _p, _int, _int, _int, C.c_float, C.POINTER(_dbl)]
+lib.xns_calc_amp_plane.argtypes = [_p, _PP, _p, _u32, _dbl, _dbl, _u32, _dbl, _dbl, _u32, _int, _p, _p, _p]
 lib.xns_binning_features.argtypes = [_p, _p, _u32, _p]
 lib.xns_binning_correction.argtypes = [_p, _p, _p, _u32, _dbl, _p, _u32, _dbl, _p]
 
@@ -318,6 +319,16 @@ class Context:
         h = np.zeros(ens.classes * nhist, dtype=np.uint64) if want_hist else None
         self._check(lib.xns_calc_batch_debye_hist(self._h, *ens.args(nhist, bin, source, polar, lam), _ptr(I), _ptr(h)))
         return (I, h) if want_hist else I
+
+    def calc_amp_plane(self, elements, qx0, dqx, nqx, qy0, dqy, nqy, source, coef=None, sl=None):
+        """|A(qx, qy)|^2 / N on a Cartesian plane (nqy x nqx), tensor cores with exact digit sums."""
+        el = _Elements(elements)
+        coef = None if coef is None else np.ascontiguousarray(coef, dtype=np.float64).reshape(-1, 9)
+        sl = _f64(sl)
+        out = np.zeros((nqy, nqx))
+        self._check(lib.xns_calc_amp_plane(self._h, el.table, _ptr(el.n_el), el.nel, qx0, dqx, nqx, qy0, dqy, nqy, source,
+                                           _ptr(coef), _ptr(sl), _ptr(out)))
+        return out
 
     def batch(self, structures, nhist, bin, q, source, sl=None, ff=None, polar=False, lam=0.0, autotune=False):
         return Batch(self, structures, nhist, bin, q, source, sl, ff, polar, lam, autotune)

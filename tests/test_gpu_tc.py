@@ -8,7 +8,7 @@ path's 1e-5 everywhere."""
 import numpy as np
 import pytest
 
-from conftest import rel_err
+from conftest import rel_err, rel_err_floor
 
 from xns_b200 import synth
 
@@ -121,3 +121,26 @@ def test_iq_full_size_vs_reference(gpu_ctx, oracle):
     assert rel_err(gpu_ctx.calc_int_1d_hist(h, n_el, nh, 0.001, q, 0, sl=[3.63, 9.58]), Io) < TOL_I
     G = gpu_ctx.hist_transform(h.reshape(3, nh), 0.001, q, "exact")
     assert rel_err(iq_from_g(G, n_el, [3.63, 9.58]), Io) < TOL_I
+
+
+@pytest.mark.parametrize("source", [0, 1])
+def test_amp_plane_vs_oracle(gpu_ctx, oracle, source):
+    """Cartesian q plane (tensor-core complex product with exact digit sums) against the FP64 oracle:
+    fcc crystallite with a 5 % second species, rotated, 80 x 96 points over [-8, 8) A^-1."""
+    els = synth.fcc_crystallite(cells=6, a=3.61, subst=0.05, seed=4)
+    nqx, nqy = 96, 80
+    dqx, dqy = 16.0 / nqx, 16.0 / nqy
+    coef = synth.ff_coefficients(2, seed=3) if source == 1 else None
+    sl = [7.0, 3.0] if source == 0 else None
+    I = gpu_ctx.calc_amp_plane(els, -8.0, dqx, nqx, -8.0, dqy, nqy, source, coef=coef, sl=sl)
+    Io = oracle.amp_plane(els, -8.0, dqx, nqx, -8.0, dqy, nqy, source, coef=coef, sl=sl).reshape(nqy, nqx)
+    assert rel_err_floor(I, Io, 1e-2) < 1e-5
+
+
+def test_amp_plane_ragged_sizes(gpu_ctx, oracle):
+    """Atom counts and mesh sizes that are not multiples of the tiles, one element empty."""
+    rng = np.random.default_rng(2)
+    els = [rng.normal(0, 6, (333, 3)), np.zeros((0, 3)), rng.normal(0, 6, (70, 3))]
+    I = gpu_ctx.calc_amp_plane(els, -5.0, 0.1, 131, -3.0, 0.07, 67, 0, sl=[1.0, 2.0, 3.0])
+    Io = oracle.amp_plane(els, -5.0, 0.1, 131, -3.0, 0.07, 67, 0, sl=[1.0, 2.0, 3.0]).reshape(67, 131)
+    assert rel_err_floor(I, Io, 1e-2) < 1e-5
