@@ -257,6 +257,10 @@ int xns_binning_correction(xns_ctx *ctx, const double *h, const float *mu, uint3
  * FP32 otherwise.  The roofline denominator for the FP64 distance and FP32 sinc kernels. */
 int xns_measure_fma_peak(xns_ctx *ctx, int fp64, double *tflops);
 
+/* Measured rate of conflict-free shared-memory atomic increments on this device, in 1e9 per second:
+ * the roofline of a shared-memory histogram, which makes one such increment per counted pair. */
+int xns_measure_smem_atomic_peak(xns_ctx *ctx, double *gops);
+
 #ifdef __cplusplus
 }
 #endif

@@ -293,6 +293,42 @@ __global__ void fma_probe_kernel(T *out, int iters, T a, T b) {
   out[blockIdx.x * blockDim.x + threadIdx.x] = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
 }
 
+// Conflict-free shared-memory atomic increments: each warp hits 32 consecutive words, 8 per thread per
+// iteration, 1024 threads per CTA.
+__global__ void __launch_bounds__(1024) smem_atomic_probe_kernel(unsigned *out, int iters) {
+  __shared__ unsigned h[4096];
+  for (int i = threadIdx.x; i < 4096; i += blockDim.x) h[i] = 0;
+  __syncthreads();
+  const unsigned base = ((threadIdx.x >> 5) * 32u) & 4095u, lane = threadIdx.x & 31u;
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) atomicAdd(&h[(base + lane + 512u * k) & 4095u], 1u);
+  }
+  __syncthreads();
+  out[blockIdx.x * blockDim.x + threadIdx.x] = h[threadIdx.x & 4095u];
+}
+
+extern "C" int xns_measure_smem_atomic_peak(xns_ctx *ctx, double *gops) {
+  if (!ctx || !gops) return XNS_ERR_ARG;
+  const int threads = 1024, blocks = ctx->num_sms * 2, iters = 2048;
+  void *out;
+  int st;
+  if ((st = xns_scratch(ctx, SLOT_AUX, sizeof(unsigned) * threads * blocks, &out))) return st;
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; rep++) {
+    XNS_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    smem_atomic_probe_kernel<<<blocks, threads, 0, ctx->stream>>>((unsigned *)out, iters);
+    XNS_LAUNCHED(ctx);
+    XNS_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    XNS_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
+    float ms;
+    XNS_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    if (rep && ms < best) best = ms;
+  }
+  *gops = 8.0 * iters * (double)threads * blocks / (best * 1e-3) / 1e9;
+  return XNS_OK;
+}
+
 extern "C" int xns_measure_fma_peak(xns_ctx *ctx, int fp64, double *tflops) {
   if (!ctx || !tflops) return XNS_ERR_ARG;
   const int threads = 256, blocks = ctx->num_sms * 8, iters = fp64 ? 1024 : 4096;
