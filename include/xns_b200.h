@@ -114,6 +114,11 @@ int xns_calc_int_2d(xns_ctx *ctx, const double *const *xyz_el, const uint32_t *n
                     uint32_t convention, double lambda, int source, const double *const *ff, const double *sl, int polar,
                     double *I2D, double *I);
 
+/* The rotation matrix of calcRotMatrix (CalcFunctions.cpp:46-115) for Euler angles euler[0..2] (radians)
+ * in convention 0..11 (typedefs.h:59-70), row-major, as xns_calc_int_2d applies it per orientation.
+ * Host-only; needs no device.  Use it to orient coordinates for xns_calc_amp_plane. */
+void xns_rot_matrix(const double euler[3], uint32_t convention, double m[9]);
+
 /* ---- device-buffer entry points ----------------------------------------------------------------- */
 
 /* calcPDFandDebye (CalcFunctions.cpp:912-968) on device-resident data: xyz_dev is a device array of
@@ -173,8 +178,8 @@ int xns_hist_transform_exact(xns_ctx *ctx, const uint64_t *hist, uint32_t ncols,
  * limit of a flat Ewald surface: I[iy * nqx + ix] = |sum_e f_e(|q|) sum_{j in e} exp(i (qx x_j + qy y_j))|^2
  * / N with qx = qx0 + ix dqx, qy = qy0 + iy dqy; coordinates as given (pre-rotate them for another
  * orientation).  Since exp(i (qx x + qy y)) factorises, the sum is a complex matrix product over atoms,
- * run on the tensor cores with three integer digits per cos / sin value and exact accumulation (error
- * ~1e-7 of |A|^2).  X-ray: coef holds 9 numbers per element, f(q) = sum_k a_k exp(-b_k (q/4pi)^2) + c
+ * run on the tensor cores with four base-256 integer digits per cos / sin value and exact accumulation
+ * (measured error 2e-7 of the pattern's maximum).  X-ray: coef holds 9 numbers per element, f(q) = sum_k a_k exp(-b_k (q/4pi)^2) + c
  * as (a1..a4, b1..b4, c); neutron: sl.  No counterpart entry in the reference (its 2D mesh is polar on
  * the Ewald sphere: xns_calc_int_2d). */
 int xns_calc_amp_plane(xns_ctx *ctx, const double *const *xyz_el, const uint32_t *n_el, uint32_t nel, double qx0,

@@ -40,3 +40,20 @@ def test_no_device_is_an_error_not_a_fallback():
     with pytest.raises(xns_b200.XnsError) as e:
         xns_b200.Context(0)
     assert e.value.status == 3  # XNS_ERR_NODEV
+
+
+def test_rotation_matrix_matches_reference():
+    """xns_rot_matrix (host code, no device) against calcRotMatrix's matrices for all 12 conventions."""
+    import numpy as np
+
+    import xns_b200
+    from conftest import load_golden
+    g = load_golden("rot__all")
+    f = xns_b200.lib.xns_rot_matrix
+    f.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.c_uint32, ctypes.POINTER(ctypes.c_double)]
+    f.restype = None
+    eul = (ctypes.c_double * 3)(*[float(v) for v in g["euler"]])
+    for c in range(12):
+        m = (ctypes.c_double * 9)()
+        f(eul, c, m)
+        assert np.allclose(np.array(m[:]).reshape(3, 3), np.asarray(g["m"][c]).reshape(3, 3), rtol=0, atol=1e-15), c
