@@ -20,8 +20,8 @@
 //
 // Bin decision, per pair: an FP32 estimate of r/bin from tile-local offsets, with a proven error bound
 // (count_tile_pair_t); pairs whose estimate lies within that bound of a bin edge (about 9 % at 0.001 A
-// bins and 1e5-bin distances), or near the last bin, are queued in per-lane rings and binned exactly
-// with FP64 in the reference's operation order (hist_bin.cuh).  Atom order inside a cell and list order
+// bins and 1e5-bin distances), or near the last bin, are queued per warp and binned exactly, 32 at a
+// time, with FP64 in the reference's operation order (hist_bin.cuh).  Atom order inside a cell and list order
 // inside a bucket come from atomics, but counts do not depend on either.
 #include <math.h>
 #include <string.h>
@@ -44,9 +44,9 @@ constexpr int HW_THREADS = 32 * HW_WARPS;
 constexpr uint32_t WIN_MAX = 39 * 1024;  // largest window (bins) that fits with the warp stages
 constexpr uint32_t BUCKET = 1024;    // distance bucket of the tile-pair sort, in bins
 constexpr int SCAN_THREADS = 1024;
-constexpr int RING = 256;            // deferred pairs per warp: 8 per lane (u16 entries i << 6 | j)
-// per warp: FP64 I and J tiles, FP32 I-tile offsets, the rings (bytes)
-constexpr int WARP_STAGE = 2 * 3 * TILE_MAX * 8 + 3 * TILE_MAX * 4 + RING * 2;
+constexpr int QUEUE = 256;           // near pairs queued per warp for exact binning (u16 i << 6 | j)
+// per warp: FP64 I and J tiles, FP32 I-tile offsets, the queue (bytes)
+constexpr int WARP_STAGE = 2 * 3 * TILE_MAX * 8 + 3 * TILE_MAX * 4 + QUEUE * 2;
 
 struct Tile {
   uint32_t start, count, elem, pad;
@@ -322,14 +322,14 @@ static_assert(sizeof(HistParams) <= sizeof(((HistLaunch *)0)->params), "HistLaun
 // integer is >= m has floor(r) equal to the reference's bin (whose own FP64 rounding is below 1e-10
 // bins).  r + 1.5*2^23 rounds r to an integer in the low mantissa bits (r < 2^22), which gives
 // round(r) and d without a conversion.  Pairs with d < m, near or beyond the last bin, or outside the
-// CTA's window go to the lane's ring and are binned exactly with FP64 from the staged coordinates
-// (hist_bin.cuh) once some lane holds four.
+// CTA's window are appended to the warp's queue (ballot + popc: consecutive entries) and binned exactly
+// with FP64 from the staged coordinates (hist_bin.cuh), one entry per lane, whenever 32 are waiting.
 template <bool SAME, bool WINDOW>
 __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const TilePair tp, uint8_t *stage,
                                                       uint32_t *win, uint32_t base, unsigned long long *h) {
   double *wI = reinterpret_cast<double *>(stage), *wJ = wI + 3 * TILE_MAX;
   float *wIf = reinterpret_cast<float *>(wJ + 3 * TILE_MAX);
-  uint16_t *ring = reinterpret_cast<uint16_t *>(wIf + 3 * TILE_MAX);
+  uint16_t *queue = reinterpret_cast<uint16_t *>(wIf + 3 * TILE_MAX);
   const uint32_t lane = threadIdx.x & 31;
   const Tile TI = p.tiles[tp.I], TJ = p.tiles[tp.J];
   const uint32_t ni = TI.count, nj = TJ.count;
@@ -384,27 +384,31 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
   const float lim = fminf((float)p.nhist - 1.0f, 4194303.0f);  // the last bin and beyond: exact path
   const int tbase = __float_as_int(MAGIC) + (int)base;          // slot = bits(r + MAGIC) - tbase - (d < 0)
   const uint32_t W = p.win;
-  uint16_t *lq = ring + lane;                                   // this lane's ring: entry s at lq[32 s]
-  uint32_t qw = 0, cnt = 0;                                     // next write slot (mod 8), pending entries
+  const uint32_t below = (1u << lane) - 1u;                     // lanes below this one
+  const double nhm1 = (double)p.nhist - 1.0;
+  uint32_t qn = 0, qd = 0;                                      // entries queued / binned (warp-uniform)
   unsigned bad = 0;
-  auto drain_one = [&]() {  // lanes with a pending entry bin their oldest exactly
-    if (cnt) {
-      const uint32_t e = lq[((qw - cnt) & 7u) << 5];
-      cnt--;
+  // Lane l bins queued entry qd + l exactly (l < n), then n entries are done.  The warp drains full
+  // batches of 32 while it counts, so every lane has an entry.
+  auto drain = [&](uint32_t n) {
+    if (lane < n) {
+      const uint32_t e = queue[(qd + lane) & (QUEUE - 1)];
       const uint32_t a = e >> 6, b = e & 63u;
       const double d2 = ref_dist2(wI[a], wI[TILE_MAX + a], wI[2 * TILE_MAX + a], wJ[b], wJ[TILE_MAX + b],
                                   wJ[2 * TILE_MAX + b]);
-      const uint32_t k = ref_bin(d2, p.bin, p.inv_bin, p.margin, p.nhist);
+      uint32_t k;
+      if (!ref_bin_fast(d2, p.inv_bin, p.margin, nhm1, &k)) k = ref_bin_slow(d2, p.bin, p.inv_bin, p.margin, p.nhist);
       if (k >= p.nhist) {
         bad++;
-      } else if (WINDOW && k - base < p.win) {
+      } else if (WINDOW && k - base < W) {
         atomicAdd(win + (k - base), 1u);
       } else {
         atomicAdd(h + k, 1ull);
       }
     }
+    qd += n;
   };
-#define XNS_PAIR(XA, YA, ZA, XJ, YJ, ZJ, VALID, II, JJ)                                   \
+#define XNS_PAIR(XA, YA, ZA, XJ, YJ, ZJ, VALID, EE)                                       \
   {                                                                                         \
     const float dx = dh[0] + (XA - XJ), dy = dh[1] + (YA - YJ), dz = dh[2] + (ZA - ZJ);    \
     const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));                                   \
@@ -423,11 +427,11 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
     } else if (fast) {                                                                      \
       atomicAdd(h + slot, 1ull);                                                            \
     }                                                                                       \
-    /* branch-free push: the write to the next free slot is harmless when nothing is pushed */ \
-    const uint32_t push = ((VALID) && !fast) ? 1u : 0u;                                     \
-    lq[qw << 5] = (uint16_t)(((II) << 6) | (JJ));                                           \
-    qw = (qw + push) & 7u;                                                                  \
-    cnt += push;                                                                            \
+    /* queue the pair for exact binning: the warp's near pairs take consecutive entries */  \
+    const bool near = (VALID) && !fast;                                                     \
+    const unsigned nb = __ballot_sync(0xffffffffu, near);                                   \
+    if (near) queue[(qn + __popc(nb & below)) & (QUEUE - 1)] = (uint16_t)(EE);              \
+    qn += __popc(nb);                                                                       \
   }
   for (uint32_t i = 0; i < ni; i += 2) {
     const uint32_t i1 = min(i + 1, ni - 1);
@@ -441,15 +445,17 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
       v2 = v2 && i + 1 < j0;
       v3 = v3 && i + 1 < j1;
     }
-    XNS_PAIR(xa, ya, za, xj0, yj0, zj0, v0, i, j0)
-    XNS_PAIR(xa, ya, za, xj1, yj1, zj1, v1, i, j1)
-    XNS_PAIR(xb, yb, zb, xj0, yj0, zj0, v2, i + 1, j0)
-    XNS_PAIR(xb, yb, zb, xj1, yj1, zj1, v3, i + 1, j1)
-    // a ring holds 8: after this every lane holds at most 3, and the next step adds at most 4
-    while (__any_sync(0xffffffffu, cnt >= 4)) drain_one();
+    const uint32_t e0 = (i << 6) | j0, e1 = (i << 6) | j1;  // queue entries: row << 6 | column
+    XNS_PAIR(xa, ya, za, xj0, yj0, zj0, v0, e0)
+    XNS_PAIR(xa, ya, za, xj1, yj1, zj1, v1, e1)
+    XNS_PAIR(xb, yb, zb, xj0, yj0, zj0, v2, e0 + 64u)
+    XNS_PAIR(xb, yb, zb, xj1, yj1, zj1, v3, e1 + 64u)
+    // fewer than 32 entries wait here and a step adds at most 128: the queue never holds more than
+    // 159 of its QUEUE entries
+    while (qn - qd >= 32) drain(32);
   }
 #undef XNS_PAIR
-  while (__any_sync(0xffffffffu, cnt > 0)) drain_one();
+  if (qn != qd) drain(qn - qd);
   return bad;
 }
 
