@@ -41,12 +41,12 @@ constexpr int TILE_MAX = 64;         // atoms per tile
 constexpr int MAX_CELLS_AXIS = 256;
 constexpr int HW_WARPS = 16;
 constexpr int HW_THREADS = 32 * HW_WARPS;
-constexpr uint32_t WIN_MAX = 39 * 1024;  // largest window (bins) that fits with the warp stages
+constexpr uint32_t WIN_MAX = 44 * 1024;  // largest window (bins) that fits with the warp stages
 constexpr uint32_t BUCKET = 1024;    // distance bucket of the tile-pair sort, in bins
 constexpr int SCAN_THREADS = 1024;
 constexpr int QUEUE = 256;           // near pairs queued per warp for exact binning (u16 i << 6 | j)
-// per warp: FP64 I and J tiles, FP32 I-tile offsets, the queue (bytes)
-constexpr int WARP_STAGE = 2 * 3 * TILE_MAX * 8 + 3 * TILE_MAX * 4 + QUEUE * 2;
+// per warp: FP64 I tile, FP32 I-tile offsets (+ P_i), the queue (bytes)
+constexpr int WARP_STAGE = 3 * TILE_MAX * 8 + 4 * TILE_MAX * 4 + QUEUE * 2;
 
 struct Tile {
   uint32_t start, count, elem, pad;
@@ -308,94 +308,197 @@ struct HistParams {
 };
 static_assert(sizeof(HistParams) <= sizeof(((HistLaunch *)0)->params), "HistLaunch holds the kernel parameters");
 
-// One warp counts the pairs of one tile pair: both tiles' FP64 coordinates and the I tile's FP32
-// offsets are staged in the warp's shared memory (stage: WARP_STAGE bytes), the J tile's FP32 offsets
-// sit in registers (atoms lane and lane + 32), the warp walks i two rows at a time (four independent
-// chains).  SAME (a tile against itself) keeps only i < j.
+// Geometry of a tile pair in bins: centres' offset D = (c_I - c_J)/bin, R0 = |D|, per-axis half
+// extents E (+1 bin against rounding) and the radii rho = |E| of the boxes around the centres.
+struct PairGeom {
+  double D[3], R0, EI, EJ, rhoI, rhoJ;
+};
+__device__ __forceinline__ PairGeom pair_geom(const Tile &TI, const Tile &TJ, double ib) {
+  PairGeom g;
+  double r2 = 0, eI2 = 0, eJ2 = 0;
+  g.EI = 0;
+  g.EJ = 0;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    g.D[k] = (0.5 * (TI.lo[k] + TI.hi[k]) - 0.5 * (TJ.lo[k] + TJ.hi[k])) * ib;
+    const double eI = 0.5 * (TI.hi[k] - TI.lo[k]) * ib + 1.0, eJ = 0.5 * (TJ.hi[k] - TJ.lo[k]) * ib + 1.0;
+    g.EI = fmax(g.EI, eI);
+    g.EJ = fmax(g.EJ, eJ);
+    r2 += g.D[k] * g.D[k];
+    eI2 += eI * eI;
+    eJ2 += eJ * eJ;
+  }
+  g.R0 = sqrt(r2);
+  g.rhoI = sqrt(eI2);
+  g.rhoJ = sqrt(eJ2);
+  return g;
+}
+
+// Far tile pairs (R0 >= 2 (rho_I + rho_J), so every pair has r >= R0 / 2) take the centred estimate.
+__device__ __forceinline__ bool far_pair(const PairGeom &g) { return g.R0 >= 2.0 * (g.rhoI + g.rhoJ); }
+
+// One warp counts the pairs of one tile pair: the I tile's FP64 coordinates and FP32 offsets are
+// staged in the warp's shared memory (stage: WARP_STAGE bytes), the J tile's sit in registers (atoms
+// lane and lane + 32), the warp walks i two rows at a time (four independent chains).  SAME (a tile
+// against itself) keeps only i < j.  Each pair gets an FP32 estimate of r/bin with a proven error
+// bound; pairs whose estimate lies within the bound of a bin edge, near or beyond the last bin, or
+// outside the CTA's window are appended to the warp's queue (ballot + popc: consecutive entries) and
+// binned exactly with FP64 from the coordinates (hist_bin.cuh), one entry per lane, whenever 32 wait.
 //
-// FP32 estimate of r/bin: dh is the tile-centre offset (c_I - c_J)/bin rounded to float, dl its low
-// part; the I offsets are (x_i - c_I)/bin and the J offsets (x_j - c_J)/bin - dl, rounded to float.
-// Error bound (bins; u = 2^-24, E_I / E_J the tiles' largest half extent in bins): each axis
-// |dx - dx_true| <= u|dx| + C, C = u(2 E_I + 3 E_J + 2) + 2^-40 |D|; d2 by FMAs adds 3u relative;
+// Direct estimate (SAME and close tile pairs; u = 2^-24): dh is D rounded to float, dl its low part;
+// the I offsets are (x_i - c_I)/bin and the J offsets (x_j - c_J)/bin - dl, rounded to float.  Each
+// axis |dx - dx_true| <= u|dx| + C, C = u(2 E_I + 3 E_J + 2) + 2^-40 |D|; d2 by FMAs adds 3u relative;
 // rsqrt.approx (2 ulp) followed by one Newton step leaves u + O(u^2) relative to sqrt(d2); so
 // |r - r_true| <= 4.3 u r + 1.74 C.  With m = 6 u r + 2 C, any r whose distance d to the nearest
 // integer is >= m has floor(r) equal to the reference's bin (whose own FP64 rounding is below 1e-10
 // bins).  r + 1.5*2^23 rounds r to an integer in the low mantissa bits (r < 2^22), which gives
-// round(r) and d without a conversion.  Pairs with d < m, near or beyond the last bin, or outside the
-// CTA's window are appended to the warp's queue (ballot + popc: consecutive entries) and binned exactly
-// with FP64 from the staged coordinates (hist_bin.cuh), one entry per lane, whenever 32 are waiting.
-template <bool SAME, bool WINDOW>
-__device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const TilePair tp, uint8_t *stage,
-                                                      uint32_t *win, uint32_t base, unsigned long long *h) {
-  double *wI = reinterpret_cast<double *>(stage), *wJ = wI + 3 * TILE_MAX;
-  float *wIf = reinterpret_cast<float *>(wJ + 3 * TILE_MAX);
-  uint16_t *queue = reinterpret_cast<uint16_t *>(wIf + 3 * TILE_MAX);
+// round(r) and d without a conversion.
+//
+// Centred estimate (far tile pairs): with a = (x_i - c_I)/bin, b = (x_j - c_J)/bin,
+//   r^2 = R0^2 + num,  num = P_i - Q_j - 2 a.b,  P_i = 2 D.a + |a|^2,  Q_j = 2 D.b - |b|^2,
+// and r = R0 + delta with delta = num / (R0 + r) exactly.  P_i and Q_j are formed in FP64 per tile pair
+// and rounded to float; per pair num = (P_i - Q_j) + a.(-2 b) in FP32, r' = d2 rsqrt(d2) with
+// d2 = num + R0^2 only for the denominator, and t = num rcp(r' + R0) + (R0 - floor(R0) - 0.5) in one
+// FMA, so that floor(r) = floor(R0) + round(t).  Its error (centred_margin) is K0 + K1 |delta| with K0
+// of order u rho and K1 of order 20 u: it grows with the tile size, not with r, and at 1e5-bin
+// distances leaves about a quarter of the direct estimate's near-edge pairs.
+struct CentredConsts {
+  float R0sq, R0f, R0fr, K1, mc;  // fast iff |d| <= mc - K1 |t|
+  int R0i;
+};
+// The bound, for r >= R0/2 (far_pair); each line is one source of error (first order in u):
+//   num:   |num~ - num| <= u(|P| + |Q|) + 2u|num| + 14u rho_I rho_J, |P| <= 2 R0 rho_I + rho_I^2 (Q alike);
+//          divided by r + R0 >= 1.5 R0 this is A + 2u|delta|;
+//   d2:    relative error eps_d <= 5u + 4 dnum_max / R0^2 (R0^2 rounded, num's error, one add);
+//   r':    rsqrt.approx 4u + product u + eps_d / 2;  den = r' + R0: eps_den <= eps_r + 2u;
+//   t:     rcp.approx 2u, the FMA's rounding u|t| <= u|delta| + u/2;
+// so |t - (r - floor(R0) - 0.5)| <= K0 + (5u + eps_den) |delta| and |delta| <= |t| + 1.
+__device__ __forceinline__ CentredConsts centred_consts(const PairGeom &g) {
+  const double u = 5.9604644775390625e-08;  // 2^-24
+  const double rs = g.rhoI + g.rhoJ, rr = g.rhoI * g.rhoI + g.rhoJ * g.rhoJ + 14.0 * g.rhoI * g.rhoJ;
+  const double A = u * (4.0 / 3.0 * rs + rr / (1.5 * g.R0));
+  const double num_max = 2.0 * g.R0 * rs + rs * rs;
+  const double dnum_max = u * (2.0 * g.R0 * rs + rr) + 2.0 * u * num_max;
+  const double eps_d = 5.0 * u + 4.0 * dnum_max / (g.R0 * g.R0);
+  const double eps_den = eps_d / 2.0 + 7.0 * u;
+  const double K1 = (5.0 * u + eps_den) * 1.01;
+  // u/2 + rounding of R0fr; 1e-9 for FP64 errors of D, a, P, Q and the reference's own rounding
+  const double K0 = A * 1.01 + u + 1e-9 + ldexp(g.R0, -40);
+  CentredConsts c;
+  const double fl = floor(g.R0);
+  c.R0sq = (float)(g.R0 * g.R0);
+  c.R0f = (float)g.R0;
+  c.R0fr = (float)(g.R0 - fl - 0.5);
+  c.R0i = (int)fl;
+  c.K1 = (float)(K1 * 1.0001);
+  c.mc = (float)(0.5 - K0 - K1) - 1e-6f;
+  return c;
+}
+
+template <bool SAME, bool WINDOW, bool CENTRED>
+__device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const TilePair tp, const PairGeom &g,
+                                                      uint8_t *stage, uint32_t *win, uint32_t base,
+                                                      unsigned long long *h) {
+  double *wI = reinterpret_cast<double *>(stage);
+  float4 *wI4 = reinterpret_cast<float4 *>(wI + 3 * TILE_MAX);  // per I atom: offsets (+ P_i, centred)
+  uint16_t *queue = reinterpret_cast<uint16_t *>(wI4 + TILE_MAX);
   const uint32_t lane = threadIdx.x & 31;
   const Tile TI = p.tiles[tp.I], TJ = p.tiles[tp.J];
   const uint32_t ni = TI.count, nj = TJ.count;
   const double ib = p.inv_bin;
-  double cI[3], cJ[3], EI = 0, EJ = 0, Dm = 0;
+  double cI[3], cJ[3];
   float dh[3], dl[3];
 #pragma unroll
   for (int k = 0; k < 3; k++) {
     cI[k] = 0.5 * (TI.lo[k] + TI.hi[k]);
     cJ[k] = 0.5 * (TJ.lo[k] + TJ.hi[k]);
-    EI = fmax(EI, 0.5 * (TI.hi[k] - TI.lo[k]) * ib + 1.0);
-    EJ = fmax(EJ, 0.5 * (TJ.hi[k] - TJ.lo[k]) * ib + 1.0);
-    const double D = (cI[k] - cJ[k]) * ib;
-    dh[k] = (float)D;
-    dl[k] = (float)(D - (double)dh[k]);
-    Dm = fmax(Dm, fabs(D));
+    dh[k] = (float)g.D[k];
+    dl[k] = (float)(g.D[k] - (double)dh[k]);
   }
-  const float m0 = (float)(2.0 * (ldexp(2.0 * EI + 3.0 * EJ + 2.0, -24) + ldexp(Dm, -40))) + 1e-6f;
-  const float mr = 6.0f * 5.9604645e-8f;
+  const float MAGIC = 12582912.0f;  // 1.5 * 2^23
+  const uint32_t W = p.win;
+  // Slots below Wl are window slots of bins below the last one and below 2^22 (the last bin and beyond,
+  // and distances the magic-number rounding does not cover, take the exact path).  A slot computed
+  // from r >= 2^22 is at least 2^22 - base: never below Wl.
+  const uint32_t lim = min(p.nhist - 1u, 1u << 22);
+  const uint32_t Wl = lim > base ? min(WINDOW ? W : 0xffffffffu, lim - base) : 0u;
+  float m0 = 0.f, mr = 0.f;
+  int tbase;
+  CentredConsts cc;
+  if (CENTRED) {
+    cc = centred_consts(g);
+    tbase = __float_as_int(MAGIC) + (int)base - cc.R0i;  // slot = bits(t + MAGIC) - tbase
+  } else {
+    const double Dm = fmax(fabs(g.D[0]), fmax(fabs(g.D[1]), fabs(g.D[2])));
+    m0 = (float)(2.0 * (ldexp(2.0 * g.EI + 3.0 * g.EJ + 2.0, -24) + ldexp(Dm, -40))) + 1e-6f;
+    mr = 6.0f * 5.9604645e-8f;
+    tbase = __float_as_int(MAGIC) + (int)base;  // slot = bits(r + MAGIC) - tbase - (d < 0)
+  }
   for (uint32_t i = lane; i < ni; i += 32) {
     const double x = p.X[TI.start + i], y = p.Y[TI.start + i], z = p.Z[TI.start + i];
     wI[i] = x;
     wI[TILE_MAX + i] = y;
     wI[2 * TILE_MAX + i] = z;
-    wIf[i] = (float)((x - cI[0]) * ib);
-    wIf[TILE_MAX + i] = (float)((y - cI[1]) * ib);
-    wIf[2 * TILE_MAX + i] = (float)((z - cI[2]) * ib);
+    const double ax = (x - cI[0]) * ib, ay = (y - cI[1]) * ib, az = (z - cI[2]) * ib;
+    float P = 0.f;
+    if (CENTRED) P = (float)(2.0 * (g.D[0] * ax + g.D[1] * ay + g.D[2] * az) + (ax * ax + ay * ay + az * az));
+    wI4[i] = make_float4((float)ax, (float)ay, (float)az, P);
   }
   const uint32_t j0 = lane, j1 = lane + 32;
   const bool c0 = j0 < nj, c1 = j1 < nj;
-  float xj0 = 0.f, yj0 = 0.f, zj0 = 0.f, xj1 = 0.f, yj1 = 0.f, zj1 = 0.f;
+  // the J tile stays in registers: FP64 for the exact path (other lanes fetch it by shuffle), FP32
+  // for the estimate
+  double Xj0 = 0.0, Yj0 = 0.0, Zj0 = 0.0, Xj1 = 0.0, Yj1 = 0.0, Zj1 = 0.0;
   if (c0) {
-    const double x = p.X[TJ.start + j0], y = p.Y[TJ.start + j0], z = p.Z[TJ.start + j0];
-    wJ[j0] = x;
-    wJ[TILE_MAX + j0] = y;
-    wJ[2 * TILE_MAX + j0] = z;
-    xj0 = (float)((x - cJ[0]) * ib) - dl[0];
-    yj0 = (float)((y - cJ[1]) * ib) - dl[1];
-    zj0 = (float)((z - cJ[2]) * ib) - dl[2];
+    Xj0 = p.X[TJ.start + j0];
+    Yj0 = p.Y[TJ.start + j0];
+    Zj0 = p.Z[TJ.start + j0];
   }
   if (c1) {
-    const double x = p.X[TJ.start + j1], y = p.Y[TJ.start + j1], z = p.Z[TJ.start + j1];
-    wJ[j1] = x;
-    wJ[TILE_MAX + j1] = y;
-    wJ[2 * TILE_MAX + j1] = z;
-    xj1 = (float)((x - cJ[0]) * ib) - dl[0];
-    yj1 = (float)((y - cJ[1]) * ib) - dl[1];
-    zj1 = (float)((z - cJ[2]) * ib) - dl[2];
+    Xj1 = p.X[TJ.start + j1];
+    Yj1 = p.Y[TJ.start + j1];
+    Zj1 = p.Z[TJ.start + j1];
+  }
+  float xj0, yj0, zj0, xj1, yj1, zj1, qj0 = 0.f, qj1 = 0.f;
+  {
+    const double bx0 = (Xj0 - cJ[0]) * ib, by0 = (Yj0 - cJ[1]) * ib, bz0 = (Zj0 - cJ[2]) * ib;
+    const double bx1 = (Xj1 - cJ[0]) * ib, by1 = (Yj1 - cJ[1]) * ib, bz1 = (Zj1 - cJ[2]) * ib;
+    if (CENTRED) {  // -2 b rounded (the factor is exact) and Q_j
+      xj0 = -2.0f * (float)bx0;
+      yj0 = -2.0f * (float)by0;
+      zj0 = -2.0f * (float)bz0;
+      xj1 = -2.0f * (float)bx1;
+      yj1 = -2.0f * (float)by1;
+      zj1 = -2.0f * (float)bz1;
+      qj0 = (float)(2.0 * (g.D[0] * bx0 + g.D[1] * by0 + g.D[2] * bz0) - (bx0 * bx0 + by0 * by0 + bz0 * bz0));
+      qj1 = (float)(2.0 * (g.D[0] * bx1 + g.D[1] * by1 + g.D[2] * bz1) - (bx1 * bx1 + by1 * by1 + bz1 * bz1));
+    } else {
+      xj0 = (float)bx0 - dl[0];
+      yj0 = (float)by0 - dl[1];
+      zj0 = (float)bz0 - dl[2];
+      xj1 = (float)bx1 - dl[0];
+      yj1 = (float)by1 - dl[1];
+      zj1 = (float)bz1 - dl[2];
+    }
   }
   __syncwarp();
-  const float MAGIC = 12582912.0f;                              // 1.5 * 2^23
-  const float lim = fminf((float)p.nhist - 1.0f, 4194303.0f);  // the last bin and beyond: exact path
-  const int tbase = __float_as_int(MAGIC) + (int)base;          // slot = bits(r + MAGIC) - tbase - (d < 0)
-  const uint32_t W = p.win;
-  const uint32_t below = (1u << lane) - 1u;                     // lanes below this one
+  const uint32_t below = (1u << lane) - 1u;  // lanes below this one
   const double nhm1 = (double)p.nhist - 1.0;
-  uint32_t qn = 0, qd = 0;                                      // entries queued / binned (warp-uniform)
+  uint32_t qn = 0, qd = 0;  // entries queued / binned (warp-uniform)
   unsigned bad = 0;
   // Lane l bins queued entry qd + l exactly (l < n), then n entries are done.  The warp drains full
   // batches of 32 while it counts, so every lane has an entry.
   auto drain = [&](uint32_t n) {
+    const uint32_t e = lane < n ? queue[(qd + lane) & (QUEUE - 1)] : 0u;
+    const uint32_t a = e >> 6, b = e & 63u, src = b & 31u;
+    // J atom b sits in lane b & 31 (as its atom j0 when b < 32, else j1)
+    const double xb0 = __shfl_sync(0xffffffffu, Xj0, src), xb1 = __shfl_sync(0xffffffffu, Xj1, src);
+    const double yb0 = __shfl_sync(0xffffffffu, Yj0, src), yb1 = __shfl_sync(0xffffffffu, Yj1, src);
+    const double zb0 = __shfl_sync(0xffffffffu, Zj0, src), zb1 = __shfl_sync(0xffffffffu, Zj1, src);
     if (lane < n) {
-      const uint32_t e = queue[(qd + lane) & (QUEUE - 1)];
-      const uint32_t a = e >> 6, b = e & 63u;
-      const double d2 = ref_dist2(wI[a], wI[TILE_MAX + a], wI[2 * TILE_MAX + a], wJ[b], wJ[TILE_MAX + b],
-                                  wJ[2 * TILE_MAX + b]);
+      const bool hi = b >= 32u;
+      const double d2 = ref_dist2(wI[a], wI[TILE_MAX + a], wI[2 * TILE_MAX + a], hi ? xb1 : xb0, hi ? yb1 : yb0,
+                                  hi ? zb1 : zb0);
       uint32_t k;
       if (!ref_bin_fast(d2, p.inv_bin, p.margin, nhm1, &k)) k = ref_bin_slow(d2, p.bin, p.inv_bin, p.margin, p.nhist);
       if (k >= p.nhist) {
@@ -408,9 +511,24 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
     }
     qd += n;
   };
-#define XNS_PAIR(XA, YA, ZA, XJ, YJ, ZJ, VALID, EE)                                       \
+  // FAST: the estimate's bin is certain and its slot is below Wl; a lane without a fast pair adds 0 to
+  // its own spare slot (branch-free), near pairs join the warp's queue.
+#define XNS_COUNT(FAST, SLOT, VALID, EE)                                                    \
   {                                                                                         \
-    const float dx = dh[0] + (XA - XJ), dy = dh[1] + (YA - YJ), dz = dh[2] + (ZA - ZJ);    \
+    const bool fast = (VALID) && (FAST) && (SLOT) < Wl;                                     \
+    if (WINDOW) {                                                                           \
+      atomicAdd(win + (fast ? (SLOT) : W + lane), fast ? 1u : 0u);                          \
+    } else if (fast) {                                                                      \
+      atomicAdd(h + (SLOT), 1ull);                                                          \
+    }                                                                                       \
+    const bool near = (VALID) && !fast;                                                     \
+    const unsigned nb = __ballot_sync(0xffffffffu, near);                                   \
+    if (near) queue[(qn + __popc(nb & below)) & (QUEUE - 1)] = (uint16_t)(EE);              \
+    qn += __popc(nb);                                                                       \
+  }
+#define XNS_DIRECT(RA, XJ, YJ, ZJ, VALID, EE)                                               \
+  {                                                                                         \
+    const float dx = dh[0] + (RA.x - XJ), dy = dh[1] + (RA.y - YJ), dz = dh[2] + (RA.z - ZJ); \
     const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));                                   \
     float y;                                                                                \
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(d2));                                \
@@ -418,25 +536,25 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
     const float r = fmaf(fmaf(-r0, r0, d2), 0.5f * y, r0); /* one Newton step */            \
     const float t = r + MAGIC;                                                              \
     const float d = r - (t - MAGIC);                                                        \
-    const float m = fmaf(r, mr, m0);                                                        \
     const uint32_t slot = (uint32_t)(__float_as_int(t) - tbase) - (d < 0.f ? 1u : 0u);      \
-    const bool fast = (VALID) && fabsf(d) >= m && r < lim && (!WINDOW || slot < W);        \
-    if (WINDOW) {                                                                           \
-      /* branch-free: a lane without a fast pair adds 0 to its own spare slot */            \
-      atomicAdd(win + (fast ? slot : W + lane), fast ? 1u : 0u);                            \
-    } else if (fast) {                                                                      \
-      atomicAdd(h + slot, 1ull);                                                            \
-    }                                                                                       \
-    /* queue the pair for exact binning: the warp's near pairs take consecutive entries */  \
-    const bool near = (VALID) && !fast;                                                     \
-    const unsigned nb = __ballot_sync(0xffffffffu, near);                                   \
-    if (near) queue[(qn + __popc(nb & below)) & (QUEUE - 1)] = (uint16_t)(EE);              \
-    qn += __popc(nb);                                                                       \
+    XNS_COUNT(fabsf(d) >= fmaf(r, mr, m0), slot, VALID, EE)                                 \
+  }
+#define XNS_CENTRED(RA, XJ, YJ, ZJ, QJ, VALID, EE)                                          \
+  {                                                                                         \
+    const float num = (RA.w - QJ) + fmaf(RA.x, XJ, fmaf(RA.y, YJ, RA.z * ZJ));              \
+    const float d2 = num + cc.R0sq;                                                         \
+    float y, rc;                                                                            \
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(d2));                                \
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rc) : "f"(fmaf(d2, y, cc.R0f)));                \
+    const float t = fmaf(num, rc, cc.R0fr); /* r - floor(R0) - 0.5 */                       \
+    const float tm = t + MAGIC;                                                             \
+    const float d = t - (tm - MAGIC);                                                       \
+    const uint32_t slot = (uint32_t)(__float_as_int(tm) - tbase);                           \
+    XNS_COUNT(fabsf(d) <= fmaf(fabsf(t), -cc.K1, cc.mc), slot, VALID, EE)                   \
   }
   for (uint32_t i = 0; i < ni; i += 2) {
     const uint32_t i1 = min(i + 1, ni - 1);
-    const float xa = wIf[i], ya = wIf[TILE_MAX + i], za = wIf[2 * TILE_MAX + i];
-    const float xb = wIf[i1], yb = wIf[TILE_MAX + i1], zb = wIf[2 * TILE_MAX + i1];
+    const float4 ra = wI4[i], rb = wI4[i1];
     const bool r1 = i + 1 < ni;
     bool v0 = c0, v1 = c1, v2 = c0 && r1, v3 = c1 && r1;
     if (SAME) {
@@ -446,15 +564,24 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
       v3 = v3 && i + 1 < j1;
     }
     const uint32_t e0 = (i << 6) | j0, e1 = (i << 6) | j1;  // queue entries: row << 6 | column
-    XNS_PAIR(xa, ya, za, xj0, yj0, zj0, v0, e0)
-    XNS_PAIR(xa, ya, za, xj1, yj1, zj1, v1, e1)
-    XNS_PAIR(xb, yb, zb, xj0, yj0, zj0, v2, e0 + 64u)
-    XNS_PAIR(xb, yb, zb, xj1, yj1, zj1, v3, e1 + 64u)
+    if (CENTRED) {
+      XNS_CENTRED(ra, xj0, yj0, zj0, qj0, v0, e0)
+      XNS_CENTRED(ra, xj1, yj1, zj1, qj1, v1, e1)
+      XNS_CENTRED(rb, xj0, yj0, zj0, qj0, v2, e0 + 64u)
+      XNS_CENTRED(rb, xj1, yj1, zj1, qj1, v3, e1 + 64u)
+    } else {
+      XNS_DIRECT(ra, xj0, yj0, zj0, v0, e0)
+      XNS_DIRECT(ra, xj1, yj1, zj1, v1, e1)
+      XNS_DIRECT(rb, xj0, yj0, zj0, v2, e0 + 64u)
+      XNS_DIRECT(rb, xj1, yj1, zj1, v3, e1 + 64u)
+    }
     // fewer than 32 entries wait here and a step adds at most 128: the queue never holds more than
     // 159 of its QUEUE entries
     while (qn - qd >= 32) drain(32);
   }
-#undef XNS_PAIR
+#undef XNS_CENTRED
+#undef XNS_DIRECT
+#undef XNS_COUNT
   if (qn != qd) drain(qn - qd);
   return bad;
 }
@@ -462,8 +589,10 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
 template <bool WINDOW>
 __device__ __forceinline__ unsigned count_tile_pair(const HistParams &p, const TilePair tp, uint8_t *stage, uint32_t *win,
                                                     uint32_t base, unsigned long long *h) {
-  return tp.I == tp.J ? count_tile_pair_t<true, WINDOW>(p, tp, stage, win, base, h)
-                      : count_tile_pair_t<false, WINDOW>(p, tp, stage, win, base, h);
+  const PairGeom g = pair_geom(p.tiles[tp.I], p.tiles[tp.J], p.inv_bin);
+  if (tp.I == tp.J) return count_tile_pair_t<true, WINDOW, false>(p, tp, g, stage, win, base, h);
+  if (far_pair(g)) return count_tile_pair_t<false, WINDOW, true>(p, tp, g, stage, win, base, h);
+  return count_tile_pair_t<false, WINDOW, false>(p, tp, g, stage, win, base, h);
 }
 
 // Slot s of the window holds bin B + s.  flush_window adds slots [lo, hi) (bins B + lo ...) to the
@@ -543,7 +672,7 @@ __global__ void __launch_bounds__(HW_THREADS, 1) hist_window_kernel(HistParams p
   if (bad) atomicAdd(p.n_bad, bad);
 }
 
-__global__ void __launch_bounds__(256) hist_wide_kernel(HistParams p) {
+__global__ void __launch_bounds__(256, 2) hist_wide_kernel(HistParams p) {
   __shared__ __align__(16) uint8_t stage_all[8 * WARP_STAGE];
   uint8_t *stage = stage_all + (threadIdx.x >> 5) * WARP_STAGE;
   unsigned bad = 0;
@@ -566,7 +695,7 @@ int xns_hist_plan(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, u
   *L = HistLaunch();
   if (nhist == 0 || !(bin > 0)) return xns_fail(ctx, XNS_ERR_ARG, "histogram: nhist == 0 or bin <= 0");
   if (nel == 0) return xns_fail(ctx, XNS_ERR_ARG, "histogram: no elements");
-  if (tune.win < 2 * BUCKET || tune.win > WIN_MAX || tune.cell_target < 8)
+  if (tune.win < 2 * BUCKET || tune.win > WIN_MAX || tune.win % 4 || tune.cell_target < 8)
     return xns_fail(ctx, XNS_ERR_ARG, "histogram: tuning outside its range");
   // classes: structure s owns P(nel_s) consecutive classes
   std::vector<ElemCls> ecls(nel);

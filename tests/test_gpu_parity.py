@@ -23,7 +23,10 @@ def test_hist_golden(gpu_ctx, name):
     assert np.array_equal(h, g["hist"])
 
 
-@pytest.mark.parametrize("cells,bin,seed", [(6, 0.001, 1), (8, 0.001, 2), (5, 0.0007, 3), (7, 0.01, 4)])
+# the 16-cell cube (90 A) at 0.001 A and the 12-cell one at 0.002 A have many tile pairs beyond the
+# centred estimate's threshold (twice the sum of the tile radii, about 48 A and 24 A)
+@pytest.mark.parametrize("cells,bin,seed", [(6, 0.001, 1), (8, 0.001, 2), (5, 0.0007, 3), (7, 0.01, 4), (16, 0.001, 5),
+                                            (12, 0.002, 6)])
 def test_hist_vs_oracle(gpu_ctx, oracle, cells, bin, seed):
     els = synth.rocksalt_cube(cells=cells, seed=seed)
     nh = synth.hist_size(els, bin)
