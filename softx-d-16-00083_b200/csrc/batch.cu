@@ -164,7 +164,7 @@ int batch_build(xns_batch *b, uint32_t nstruct, const uint32_t *nel, const uint3
   for (uint32_t s = 0; s < nstruct; s++) hs.st.push_back({si[s].e0, si[s].nel});
 
   if (autotune) {  // time the histogram launch for each candidate plan; keep the fastest
-    static const HistTuning cand[] = {{56, 44 * 1024}, {32, 44 * 1024}, {96, 44 * 1024}, {56, 16 * 1024}};
+    static const HistTuning cand[] = {{56, 45 * 1024 + 512}, {32, 45 * 1024 + 512}, {96, 45 * 1024 + 512}, {56, 16 * 1024}};
     double best = 1e300;
     for (const HistTuning &t : cand) {
       HistLaunch L;

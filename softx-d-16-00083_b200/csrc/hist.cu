@@ -41,10 +41,10 @@ constexpr int TILE_MAX = 64;         // atoms per tile
 constexpr int MAX_CELLS_AXIS = 256;
 constexpr int HW_WARPS = 16;
 constexpr int HW_THREADS = 32 * HW_WARPS;
-constexpr uint32_t WIN_MAX = 44 * 1024;  // largest window (bins) that fits with the warp stages
+constexpr uint32_t WIN_MAX = 45 * 1024 + 512;  // largest window (bins) that fits with the warp stages
 constexpr uint32_t BUCKET = 1024;    // distance bucket of the tile-pair sort, in bins
 constexpr int SCAN_THREADS = 1024;
-constexpr int QUEUE = 256;           // near pairs queued per warp for exact binning (u16 i << 6 | j)
+constexpr int QUEUE = 64;            // queue entries per warp: u16 (i/2) << 9 | lane << 4 | 4-bit pair mask
 // per warp: FP64 I tile, FP32 I-tile offsets (+ P_i), the queue (bytes)
 constexpr int WARP_STAGE = 3 * TILE_MAX * 8 + 4 * TILE_MAX * 4 + QUEUE * 2;
 
@@ -486,17 +486,23 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
   const double nhm1 = (double)p.nhist - 1.0;
   uint32_t qn = 0, qd = 0;  // entries queued / binned (warp-uniform)
   unsigned bad = 0;
-  // Lane l bins queued entry qd + l exactly (l < n), then n entries are done.  The warp drains full
+  // Lane l bins the pairs of queued entry qd + l exactly (l < n), then n entries are done.  An entry is
+  // one lane's near pairs of one step: rows i, i + 1 against that lane's J atoms (lane, lane + 32),
+  // bit k of the mask standing for row i + k / 2 and J atom lane + 32 (k & 1).  The warp drains full
   // batches of 32 while it counts, so every lane has an entry.
   auto drain = [&](uint32_t n) {
     const uint32_t e = lane < n ? queue[(qd + lane) & (QUEUE - 1)] : 0u;
-    const uint32_t a = e >> 6, b = e & 63u, src = b & 31u;
-    // J atom b sits in lane b & 31 (as its atom j0 when b < 32, else j1)
+    const uint32_t src = (e >> 4) & 31u, row = (e >> 9) << 1;
+    uint32_t pm = e & 15u;
+    // the J atoms sit in lane src
     const double xb0 = __shfl_sync(0xffffffffu, Xj0, src), xb1 = __shfl_sync(0xffffffffu, Xj1, src);
     const double yb0 = __shfl_sync(0xffffffffu, Yj0, src), yb1 = __shfl_sync(0xffffffffu, Yj1, src);
     const double zb0 = __shfl_sync(0xffffffffu, Zj0, src), zb1 = __shfl_sync(0xffffffffu, Zj1, src);
-    if (lane < n) {
-      const bool hi = b >= 32u;
+    while (pm) {
+      const uint32_t bit = __ffs(pm) - 1;
+      pm &= pm - 1;
+      const uint32_t a = row + (bit >> 1);
+      const bool hi = (bit & 1u) != 0;
       const double d2 = ref_dist2(wI[a], wI[TILE_MAX + a], wI[2 * TILE_MAX + a], hi ? xb1 : xb0, hi ? yb1 : yb0,
                                   hi ? zb1 : zb0);
       uint32_t k;
@@ -512,8 +518,8 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
     qd += n;
   };
   // FAST: the estimate's bin is certain and its slot is below Wl; a lane without a fast pair adds 0 to
-  // its own spare slot (branch-free), near pairs join the warp's queue.
-#define XNS_COUNT(FAST, SLOT, VALID, EE)                                                    \
+  // its own spare slot (branch-free), near pairs set their bit K of the step's mask.
+#define XNS_COUNT(FAST, SLOT, VALID, K)                                                     \
   {                                                                                         \
     const bool fast = (VALID) && (FAST) && (SLOT) < Wl;                                     \
     if (WINDOW) {                                                                           \
@@ -521,12 +527,9 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
     } else if (fast) {                                                                      \
       atomicAdd(h + (SLOT), 1ull);                                                          \
     }                                                                                       \
-    const bool near = (VALID) && !fast;                                                     \
-    const unsigned nb = __ballot_sync(0xffffffffu, near);                                   \
-    if (near) queue[(qn + __popc(nb & below)) & (QUEUE - 1)] = (uint16_t)(EE);              \
-    qn += __popc(nb);                                                                       \
+    nm |= ((VALID) && !fast) ? (1u << (K)) : 0u;                                            \
   }
-#define XNS_DIRECT(RA, XJ, YJ, ZJ, VALID, EE)                                               \
+#define XNS_DIRECT(RA, XJ, YJ, ZJ, VALID, K)                                                \
   {                                                                                         \
     const float dx = dh[0] + (RA.x - XJ), dy = dh[1] + (RA.y - YJ), dz = dh[2] + (RA.z - ZJ); \
     const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));                                   \
@@ -537,9 +540,9 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
     const float t = r + MAGIC;                                                              \
     const float d = r - (t - MAGIC);                                                        \
     const uint32_t slot = (uint32_t)(__float_as_int(t) - tbase) - (d < 0.f ? 1u : 0u);      \
-    XNS_COUNT(fabsf(d) >= fmaf(r, mr, m0), slot, VALID, EE)                                 \
+    XNS_COUNT(fabsf(d) >= fmaf(r, mr, m0), slot, VALID, K)                                  \
   }
-#define XNS_CENTRED(RA, XJ, YJ, ZJ, QJ, VALID, EE)                                          \
+#define XNS_CENTRED(RA, XJ, YJ, ZJ, QJ, VALID, K)                                           \
   {                                                                                         \
     const float num = (RA.w - QJ) + fmaf(RA.x, XJ, fmaf(RA.y, YJ, RA.z * ZJ));              \
     const float d2 = num + cc.R0sq;                                                         \
@@ -550,7 +553,7 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
     const float tm = t + MAGIC;                                                             \
     const float d = t - (tm - MAGIC);                                                       \
     const uint32_t slot = (uint32_t)(__float_as_int(tm) - tbase);                           \
-    XNS_COUNT(fabsf(d) <= fmaf(fabsf(t), -cc.K1, cc.mc), slot, VALID, EE)                   \
+    XNS_COUNT(fabsf(d) <= fmaf(fabsf(t), -cc.K1, cc.mc), slot, VALID, K)                    \
   }
   for (uint32_t i = 0; i < ni; i += 2) {
     const uint32_t i1 = min(i + 1, ni - 1);
@@ -563,20 +566,23 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
       v2 = v2 && i + 1 < j0;
       v3 = v3 && i + 1 < j1;
     }
-    const uint32_t e0 = (i << 6) | j0, e1 = (i << 6) | j1;  // queue entries: row << 6 | column
+    uint32_t nm = 0;  // this step's near pairs (bit k: row i + k / 2, J atom lane + 32 (k & 1))
     if (CENTRED) {
-      XNS_CENTRED(ra, xj0, yj0, zj0, qj0, v0, e0)
-      XNS_CENTRED(ra, xj1, yj1, zj1, qj1, v1, e1)
-      XNS_CENTRED(rb, xj0, yj0, zj0, qj0, v2, e0 + 64u)
-      XNS_CENTRED(rb, xj1, yj1, zj1, qj1, v3, e1 + 64u)
+      XNS_CENTRED(ra, xj0, yj0, zj0, qj0, v0, 0)
+      XNS_CENTRED(ra, xj1, yj1, zj1, qj1, v1, 1)
+      XNS_CENTRED(rb, xj0, yj0, zj0, qj0, v2, 2)
+      XNS_CENTRED(rb, xj1, yj1, zj1, qj1, v3, 3)
     } else {
-      XNS_DIRECT(ra, xj0, yj0, zj0, v0, e0)
-      XNS_DIRECT(ra, xj1, yj1, zj1, v1, e1)
-      XNS_DIRECT(rb, xj0, yj0, zj0, v2, e0 + 64u)
-      XNS_DIRECT(rb, xj1, yj1, zj1, v3, e1 + 64u)
+      XNS_DIRECT(ra, xj0, yj0, zj0, v0, 0)
+      XNS_DIRECT(ra, xj1, yj1, zj1, v1, 1)
+      XNS_DIRECT(rb, xj0, yj0, zj0, v2, 2)
+      XNS_DIRECT(rb, xj1, yj1, zj1, v3, 3)
     }
-    // fewer than 32 entries wait here and a step adds at most 128: the queue never holds more than
-    // 159 of its QUEUE entries
+    // lanes with near pairs append one entry each, in lane order
+    const unsigned nb = __ballot_sync(0xffffffffu, nm != 0);
+    if (nm) queue[(qn + __popc(nb & below)) & (QUEUE - 1)] = (uint16_t)(((i >> 1) << 9) | (lane << 4) | nm);
+    qn += __popc(nb);
+    // fewer than 32 entries wait here and a step adds at most 32: the queue never holds more than 63
     while (qn - qd >= 32) drain(32);
   }
 #undef XNS_CENTRED

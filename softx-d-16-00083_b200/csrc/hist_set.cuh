@@ -19,7 +19,7 @@ struct HistSet {
 // shared-memory window that slides along the distance axis (its privatisation depth).
 struct HistTuning {
   uint32_t cell_target = 56;
-  uint32_t win = 44 * 1024;
+  uint32_t win = 45 * 1024 + 512;
 };
 
 // Everything the counting kernels need, built by xns_hist_plan; the buffers it points to live in the
