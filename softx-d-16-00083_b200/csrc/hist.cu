@@ -185,6 +185,26 @@ __global__ void gather_u32_kernel(const uint32_t *__restrict__ src, const uint32
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[idx[i]];
 }
 
+// Candidate cell grids (NCAND per element, cg[e * NCAND + c], cells counted from cg[].base): atoms per
+// cell, then the warp lanes that the grid's tiles would occupy, 64 per tile (the counting kernel walks
+// a J tile with 64 lanes whatever its size).
+constexpr int NCAND = 6;
+__global__ void cand_count_kernel(const double *__restrict__ X, const double *__restrict__ Y, const double *__restrict__ Z,
+                                  const ElemGrid *__restrict__ cg, uint32_t *__restrict__ cnt) {
+  const ElemGrid g = cg[blockIdx.y * NCAND + blockIdx.z];
+  for (uint32_t i = g.atom0 + blockIdx.x * blockDim.x + threadIdx.x; i < g.atom0 + g.natoms; i += gridDim.x * blockDim.x)
+    atomicAdd(cnt + cell_of(g, X[i], Y[i], Z[i]), 1u);
+}
+__global__ void cand_slots_kernel(const uint32_t *__restrict__ cnt, const ElemGrid *__restrict__ cg,
+                                  unsigned long long *__restrict__ slots) {
+  const ElemGrid g = cg[blockIdx.x];
+  const uint32_t nc = g.n[0] * g.n[1] * g.n[2];
+  unsigned long long t = 0;
+  for (uint32_t c = threadIdx.x; c < nc; c += blockDim.x) t += (cnt[g.base + c] + TILE_MAX - 1) / TILE_MAX;
+  for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  if ((threadIdx.x & 31) == 0 && t) atomicAdd(slots + blockIdx.x, t * TILE_MAX);
+}
+
 // Cells -> tiles: a cell of n atoms becomes ceil(n/64) tiles of near-equal size.
 __global__ void tile_build_kernel(const uint32_t *__restrict__ cnt, const uint32_t *__restrict__ cell_off,
                                   const uint32_t *__restrict__ tile_off, uint32_t ncells, const ElemGrid *__restrict__ eg,
@@ -748,11 +768,16 @@ int xns_hist_plan(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, u
   std::vector<unsigned long long> bb(6 * (size_t)nel);
   XNS_CUDA(ctx, cudaMemcpyAsync(bb.data(), d_bmin, 6 * sizeof(unsigned long long) * nel, cudaMemcpyDeviceToHost, ctx->stream));
   XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  uint32_t ncells = 0;
+  uint32_t ncells = 0, ccells = 0;
   std::vector<uint32_t> ebase(nel);
+  std::vector<ElemGrid> cand((size_t)nel * NCAND);
   for (uint32_t e = 0; e < nel; e++) {
     ElemGrid &g = eg[e];
-    g.base = ncells;
+    g.base = 0;
+    for (int c = 0; c < NCAND; c++) {
+      cand[(size_t)e * NCAND + c] = g;
+      cand[(size_t)e * NCAND + c].n[0] = cand[(size_t)e * NCAND + c].n[1] = cand[(size_t)e * NCAND + c].n[2] = 0;
+    }
     if (!g.natoms) continue;
     double ext[3], vol = 1;
     for (int k = 0; k < 3; k++) {
@@ -763,11 +788,62 @@ int xns_hist_plan(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, u
     const double emax = std::max(ext[0], std::max(ext[1], ext[2]));
     for (int k = 0; k < 3; k++) vol *= std::max(ext[k], 1e-3 * emax + 1e-9);
     const double s = std::max(cbrt(tune.cell_target * vol / g.natoms), 1e-6);
-    for (int k = 0; k < 3; k++) {
-      g.n[k] = (uint32_t)std::min<double>(MAX_CELLS_AXIS, std::max(1.0, floor(ext[k] / s) + 1));
-      g.inv[k] = ext[k] > 0 ? g.n[k] / (ext[k] * (1 + 1e-12)) : 0.0;
+    // candidates: the grid of cell edge s, and grids whose cells divide the extent evenly for edges
+    // near s (a grid that leaves a thin layer of part-empty cells wastes lanes on small tiles)
+    static const double scale[NCAND - 1] = {0.88, 0.94, 1.0, 1.06, 1.12};
+    for (int c = 0; c < NCAND; c++) {
+      ElemGrid &q = cand[(size_t)e * NCAND + c];
+      q = g;
+      q.base = ccells;
+      for (int k = 0; k < 3; k++) {
+        const double n = c == 0 ? floor(ext[k] / s) + 1 : round(ext[k] / (s * scale[c - 1]));
+        q.n[k] = (uint32_t)std::min<double>(MAX_CELLS_AXIS, std::max(1.0, n));
+        q.inv[k] = ext[k] > 0 ? q.n[k] / (ext[k] * (1 + 1e-12)) : 0.0;
+      }
+      ccells += q.n[0] * q.n[1] * q.n[2];
     }
-    ncells += g.n[0] * g.n[1] * g.n[2];
+  }
+  // -- per element, the candidate grid whose tiles occupy the fewest lanes (cells no larger than the
+  // largest candidate's), counted on the device
+  {
+    void *vcand, *vslots;
+    if ((st = xns_scratch(ctx, SLOT_HCELL, sizeof(uint32_t) * (size_t)ccells + 64, &vcand))) return st;
+    if ((st = xns_scratch(ctx, SLOT_HKEY, (sizeof(ElemGrid) + sizeof(unsigned long long)) * cand.size() + 64, &vslots)))
+      return st;
+    ElemGrid *d_cg = (ElemGrid *)vslots;
+    unsigned long long *d_slots = (unsigned long long *)(d_cg + cand.size());
+    void *vh2;
+    if ((st = xns_pinned(ctx, std::max(aux_bytes, (sizeof(ElemGrid) + sizeof(unsigned long long)) * cand.size()), &vh2)))
+      return st;
+    memcpy(vh2, cand.data(), sizeof(ElemGrid) * cand.size());
+    XNS_CUDA(ctx, cudaMemcpyAsync(d_cg, vh2, sizeof(ElemGrid) * cand.size(), cudaMemcpyHostToDevice, ctx->stream));
+    XNS_CUDA(ctx, cudaMemsetAsync(vcand, 0, sizeof(uint32_t) * (size_t)ccells, ctx->stream));
+    XNS_CUDA(ctx, cudaMemsetAsync(d_slots, 0, sizeof(unsigned long long) * cand.size(), ctx->stream));
+    cand_count_kernel<<<dim3(std::max(1, ctx->num_sms / (int)nel), nel, NCAND), 256, 0, ctx->stream>>>(
+        hs.x, hs.y, hs.z, d_cg, (uint32_t *)vcand);
+    XNS_LAUNCHED(ctx);
+    cand_slots_kernel<<<(unsigned)cand.size(), 256, 0, ctx->stream>>>((const uint32_t *)vcand, d_cg, d_slots);
+    XNS_LAUNCHED(ctx);
+    std::vector<unsigned long long> slots(cand.size());
+    XNS_CUDA(ctx, cudaMemcpyAsync(slots.data(), d_slots, sizeof(unsigned long long) * cand.size(),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    for (uint32_t e = 0; e < nel; e++) {
+      if (!eg[e].natoms) continue;
+      int best = 0;
+      for (int c = 1; c < NCAND; c++)
+        if (slots[(size_t)e * NCAND + c] < slots[(size_t)e * NCAND + best]) best = c;
+      const ElemGrid &q = cand[(size_t)e * NCAND + best];
+      for (int k = 0; k < 3; k++) {
+        eg[e].n[k] = q.n[k];
+        eg[e].inv[k] = q.inv[k];
+      }
+    }
+    for (uint32_t e = 0; e < nel; e++) {
+      eg[e].base = ncells;
+      if (eg[e].natoms) ncells += eg[e].n[0] * eg[e].n[1] * eg[e].n[2];
+    }
+    vh = vh2;  // the pinned staging buffer may have moved
   }
 
   // -- counting sort of atoms by cell
