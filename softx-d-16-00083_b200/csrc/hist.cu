@@ -331,26 +331,30 @@ static_assert(sizeof(HistParams) <= sizeof(((HistLaunch *)0)->params), "HistLaun
 // Geometry of a tile pair in bins: centres' offset D = (c_I - c_J)/bin, R0 = |D|, per-axis half
 // extents E (+1 bin against rounding) and the radii rho = |E| of the boxes around the centres.
 struct PairGeom {
-  double D[3], R0, EI, EJ, rhoI, rhoJ;
+  double D[3], R0;
+  float EI, EJ, rhoI, rhoJ;
 };
 __device__ __forceinline__ PairGeom pair_geom(const Tile &TI, const Tile &TJ, double ib) {
   PairGeom g;
-  double r2 = 0, eI2 = 0, eJ2 = 0;
-  g.EI = 0;
-  g.EJ = 0;
+  double r2 = 0;
+  float eI2 = 0.f, eJ2 = 0.f;
+  g.EI = 0.f;
+  g.EJ = 0.f;
 #pragma unroll
   for (int k = 0; k < 3; k++) {
     g.D[k] = (0.5 * (TI.lo[k] + TI.hi[k]) - 0.5 * (TJ.lo[k] + TJ.hi[k])) * ib;
-    const double eI = 0.5 * (TI.hi[k] - TI.lo[k]) * ib + 1.0, eJ = 0.5 * (TJ.hi[k] - TJ.lo[k]) * ib + 1.0;
-    g.EI = fmax(g.EI, eI);
-    g.EJ = fmax(g.EJ, eJ);
+    // half extents rounded up by a part in 1e6 (bounds, not values)
+    const float eI = (float)(0.5 * (TI.hi[k] - TI.lo[k]) * ib + 1.0) * 1.000001f;
+    const float eJ = (float)(0.5 * (TJ.hi[k] - TJ.lo[k]) * ib + 1.0) * 1.000001f;
+    g.EI = fmaxf(g.EI, eI);
+    g.EJ = fmaxf(g.EJ, eJ);
     r2 += g.D[k] * g.D[k];
-    eI2 += eI * eI;
-    eJ2 += eJ * eJ;
+    eI2 = fmaf(eI, eI, eI2);
+    eJ2 = fmaf(eJ, eJ, eJ2);
   }
   g.R0 = sqrt(r2);
-  g.rhoI = sqrt(eI2);
-  g.rhoJ = sqrt(eJ2);
+  g.rhoI = sqrtf(eI2) * 1.000001f;
+  g.rhoJ = sqrtf(eJ2) * 1.000001f;
   return g;
 }
 
@@ -393,25 +397,27 @@ struct CentredConsts {
 //   r':    rsqrt.approx 4u + product u + eps_d / 2;  den = r' + R0: eps_den <= eps_r + 2u;
 //   t:     rcp.approx 2u, the FMA's rounding u|t| <= u|delta| + u/2;
 // so |t - (r - floor(R0) - 0.5)| <= K0 + (5u + eps_den) |delta| and |delta| <= |t| + 1.
+// The constants are bounds: evaluated in FP32 and enlarged by 2 % (more than FP32 rounding can take away).
 __device__ __forceinline__ CentredConsts centred_consts(const PairGeom &g) {
-  const double u = 5.9604644775390625e-08;  // 2^-24
-  const double rs = g.rhoI + g.rhoJ, rr = g.rhoI * g.rhoI + g.rhoJ * g.rhoJ + 14.0 * g.rhoI * g.rhoJ;
-  const double A = u * (4.0 / 3.0 * rs + rr / (1.5 * g.R0));
-  const double num_max = 2.0 * g.R0 * rs + rs * rs;
-  const double dnum_max = u * (2.0 * g.R0 * rs + rr) + 2.0 * u * num_max;
-  const double eps_d = 5.0 * u + 4.0 * dnum_max / (g.R0 * g.R0);
-  const double eps_den = eps_d / 2.0 + 7.0 * u;
-  const double K1 = (5.0 * u + eps_den) * 1.01;
+  const float u = 5.9604645e-08f;  // 2^-24
+  const float R0 = (float)g.R0, iR0 = 1.0f / R0;
+  const float rs = g.rhoI + g.rhoJ, rr = g.rhoI * g.rhoI + g.rhoJ * g.rhoJ + 14.0f * g.rhoI * g.rhoJ;
+  const float A = u * (4.0f / 3.0f * rs + rr * iR0 * (1.0f / 1.5f));
+  const float num_max = 2.0f * R0 * rs + rs * rs;
+  const float dnum_max = u * (2.0f * R0 * rs + rr) + 2.0f * u * num_max;
+  const float eps_d = 5.0f * u + 4.0f * dnum_max * iR0 * iR0;
+  const float eps_den = 0.5f * eps_d + 7.0f * u;
+  const float K1 = (5.0f * u + eps_den) * 1.02f;
   // u/2 + rounding of R0fr; 1e-9 for FP64 errors of D, a, P, Q and the reference's own rounding
-  const double K0 = A * 1.01 + u + 1e-9 + ldexp(g.R0, -40);
+  const float K0 = A * 1.02f + u + 1e-9f + R0 * 9.094947e-13f;  // 2^-40 R0
   CentredConsts c;
   const double fl = floor(g.R0);
   c.R0sq = (float)(g.R0 * g.R0);
-  c.R0f = (float)g.R0;
+  c.R0f = R0;
   c.R0fr = (float)(g.R0 - fl - 0.5);
   c.R0i = (int)fl;
-  c.K1 = (float)(K1 * 1.0001);
-  c.mc = (float)(0.5 - K0 - K1) - 1e-6f;
+  c.K1 = K1;
+  c.mc = 0.5f - K0 - K1 - 1e-6f;
   return c;
 }
 
@@ -449,8 +455,8 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
     cc = centred_consts(g);
     tbase = __float_as_int(MAGIC) + (int)base - cc.R0i;  // slot = bits(t + MAGIC) - tbase
   } else {
-    const double Dm = fmax(fabs(g.D[0]), fmax(fabs(g.D[1]), fabs(g.D[2])));
-    m0 = (float)(2.0 * (ldexp(2.0 * g.EI + 3.0 * g.EJ + 2.0, -24) + ldexp(Dm, -40))) + 1e-6f;
+    const float Dm = (float)fmax(fabs(g.D[0]), fmax(fabs(g.D[1]), fabs(g.D[2])));
+    m0 = 2.02f * (5.9604645e-8f * (2.0f * g.EI + 3.0f * g.EJ + 2.0f) + 9.094947e-13f * Dm) + 1e-6f;
     mr = 6.0f * 5.9604645e-8f;
     tbase = __float_as_int(MAGIC) + (int)base;  // slot = bits(r + MAGIC) - tbase - (d < 0)
   }

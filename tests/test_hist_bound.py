@@ -20,26 +20,35 @@ def fma32(a, b, c):
 
 
 def centred_consts(R0, rhoI, rhoJ):
-    """Mirror of centred_consts in hist.cu."""
-    rs, rr = rhoI + rhoJ, rhoI * rhoI + rhoJ * rhoJ + 14.0 * rhoI * rhoJ
-    A = U * (4.0 / 3.0 * rs + rr / (1.5 * R0))
-    num_max = 2.0 * R0 * rs + rs * rs
-    dnum_max = U * (2.0 * R0 * rs + rr) + 2.0 * U * num_max
-    eps_d = 5.0 * U + 4.0 * dnum_max / (R0 * R0)
-    eps_den = eps_d / 2.0 + 7.0 * U
-    K1 = (5.0 * U + eps_den) * 1.01
-    K0 = A * 1.01 + U + 1e-9 + np.ldexp(R0, -40)
+    """Mirror of centred_consts in hist.cu (float32 arithmetic, 2 % enlargement)."""
+    u = f32(U)
+    R0f = f32(R0)
+    iR0 = f32(1.0) / R0f
+    rhoI, rhoJ = f32(rhoI), f32(rhoJ)
+    rs = rhoI + rhoJ
+    rr = rhoI * rhoI + rhoJ * rhoJ + f32(14.0) * rhoI * rhoJ
+    A = u * (f32(4.0 / 3.0) * rs + rr * iR0 * f32(1.0 / 1.5))
+    num_max = f32(2.0) * R0f * rs + rs * rs
+    dnum_max = u * (f32(2.0) * R0f * rs + rr) + f32(2.0) * u * num_max
+    eps_d = f32(5.0) * u + f32(4.0) * dnum_max * iR0 * iR0
+    eps_den = f32(0.5) * eps_d + f32(7.0) * u
+    K1 = (f32(5.0) * u + eps_den) * f32(1.02)
+    K0 = A * f32(1.02) + u + f32(1e-9) + R0f * f32(9.094947e-13)
     fl = np.floor(R0)
-    return dict(R0sq=f32(R0 * R0), R0f=f32(R0), R0fr=f32(R0 - fl - 0.5), R0i=int(fl), K1=f32(K1 * 1.0001),
-                mc=f32(0.5 - K0 - K1) - f32(1e-6), K0=K0, K1d=K1)
+    return dict(R0sq=f32(R0 * R0), R0f=R0f, R0fr=f32(R0 - fl - 0.5), R0i=int(fl), K1=K1,
+                mc=f32(0.5) - K0 - K1 - f32(1e-6), K0=float(K0), K1d=float(K1))
+
+
+def tile_radius(h, ib):
+    """Mirror of pair_geom's radius: per-axis half extents (+1 bin) enlarged by 1e-6, in float32."""
+    e = (h * ib + 1.0).astype(np.float32) * f32(1.000001)
+    return float(np.sqrt((e.astype(np.float32) ** 2).sum(dtype=np.float32)) * f32(1.000001))
 
 
 def emulate_tile_pair(rng, bin_, hI, hJ, cI, cJ, n=4000, corners=True):
     ib = 1.0 / bin_
     D = (cI - cJ) * ib
-    EI = hI * ib + 1.0
-    EJ = hJ * ib + 1.0
-    rhoI, rhoJ = np.sqrt((EI ** 2).sum()), np.sqrt((EJ ** 2).sum())
+    rhoI, rhoJ = tile_radius(hI, ib), tile_radius(hJ, ib)
     R0 = np.sqrt((D ** 2).sum())
     assert R0 >= 2.0 * (rhoI + rhoJ)  # far_pair
     c = centred_consts(R0, rhoI, rhoJ)
@@ -86,7 +95,7 @@ def test_centred_bound_holds_and_fast_bins_are_exact():
     for trial in range(300):
         hI = rng.uniform(1.0, 8.0, 3)
         hJ = rng.uniform(1.0, 8.0, 3)
-        rho = np.sqrt(((hI / bin_ + 1) ** 2).sum()) + np.sqrt(((hJ / bin_ + 1) ** 2).sum())
+        rho = tile_radius(hI, 1.0 / bin_) + tile_radius(hJ, 1.0 / bin_)
         # from the far threshold up to 3e5 bins, half of them right at the threshold
         R0 = 2.0 * rho * (1.0 + 1e-9) if trial % 2 == 0 else rng.uniform(2.0 * rho, max(3e5, 2.5 * rho))
         v = rng.normal(size=3)
