@@ -532,7 +532,7 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
       const double d2 = ref_dist2(wI[a], wI[TILE_MAX + a], wI[2 * TILE_MAX + a], hi ? xb1 : xb0, hi ? yb1 : yb0,
                                   hi ? zb1 : zb0);
       uint32_t k;
-      if (!ref_bin_fast(d2, p.inv_bin, p.margin, nhm1, &k)) k = ref_bin_slow(d2, p.bin, p.inv_bin, p.margin, p.nhist);
+      if (!ref_bin_fast(d2, p.inv_bin, p.margin, nhm1, &k)) k = ref_bin(d2, p.bin, p.inv_bin, p.margin, p.nhist);
       if (k >= p.nhist) {
         bad++;
       } else if (WINDOW && k - base < W) {

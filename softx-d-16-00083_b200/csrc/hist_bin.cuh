@@ -52,12 +52,6 @@ __device__ __forceinline__ uint32_t ref_bin(double d2, double bin, double inv_bi
   return (uint32_t)q;
 }
 
-// ref_bin out of line, for callers whose fast estimate failed (a few pairs in a million): keeps the
-// correctly rounded sqrt and divide out of their loop.
-__device__ __noinline__ uint32_t ref_bin_slow(double d2, double bin, double inv_bin, double margin, uint32_t nhist) {
-  return ref_bin(d2, bin, inv_bin, margin, nhist);
-}
-
 // The estimate of ref_bin without branches: k is valid when the return value is true.  Callers run
 // several of these side by side (independent FP64 chains) and send the rare false ones to ref_bin.
 __device__ __forceinline__ bool ref_bin_fast(double d2, double inv_bin, double margin, double nhist_m1, uint32_t *k) {
