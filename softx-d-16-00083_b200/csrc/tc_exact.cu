@@ -16,9 +16,12 @@
 // in FP64 (Horner over the levels, exact: below 2^53) and added to per-thread FP64 sums, which go to
 // the output with FP64 atomics when the CTA's part of an output tile ends.
 //
-// Tile 128 q x 64 columns x 64 k, one CTA per SM, 2 stages of {NDS S-digit tiles, NH count-digit
-// tiles}; warp 0 loads (cp.async.bulk), warp 1 issues the MMAs, warps 2-9 drain tensor memory (two
-// warps per 32-lane quarter, 32 columns each).  Waits are bounded as in tc_gemm.cu.
+// Tile 128 q x N columns x 64 k (N = 16 or 32 for the transform, 64 for the plane), one CTA per SM,
+// 2 stages of {NA A-digit tiles, NB B-digit tiles}; warp 0 loads (cp.async.bulk), warp 1 issues the
+// MMAs, warps 2-9 drain tensor memory.  The accumulators are double-buffered in tensor memory
+// (2 x levels x N <= 512 columns), so the MMAs of one chunk run while the previous chunk is drained;
+// with N <= 32 the two groups of four drain warps take alternate chunks (one buffer each), with N = 64
+// each group drains 32 columns of every chunk.  Waits are bounded as in tc_gemm.cu.
 #include <algorithm>
 
 #include "tc_gemm.cuh"
@@ -28,12 +31,11 @@ using namespace xns_ptx;
 
 namespace {
 
-constexpr int XM = 128, XN = 64, XK = 64;  // tile: q rows, columns, k (one 128-byte swizzle row of BF16)
+constexpr int XM = 128, XK = 64;  // tile: q rows, k (one 128-byte swizzle row of BF16); N per scheme
 // Digits of the sinc matrix.  Four leave 2.4e-10 per element, which at the deepest minima of a
 // 2e5-atom sphere is 2e-5 of I(q) (the sum over ~3e5 bins of 1e5 counts each); five leave 1e-12.
 constexpr int NDS = 5;
 constexpr int XA = XM * XK * 2;            // 16 KB per S-digit tile
-constexpr int XB = XN * XK * 2;            // 8 KB per count-digit tile
 constexpr int XSTAGES = 2;
 constexpr int CH_TILES = 2;                // k tiles per exact chunk (CH_K = 128)
 constexpr int XTHREADS = 320;
@@ -44,19 +46,22 @@ constexpr uint32_t XTMEM_COLS = 512;
 //   KIND 0 (sinc transform): A = sinc digits, B = count digits, every product kept, level
 //          (NB-1) - (j - i);
 //   KIND 1 (plane amplitude): A and B = cos / sin digits, products of level i + j < NL kept.
-template <int NA_, int NB_, int NL_, int KIND>
+template <int NA_, int NB_, int NL_, int KIND, int N_>
 struct Scheme {
-  static constexpr int NA = NA_, NB = NB_, NL = NL_;
+  static constexpr int NA = NA_, NB = NB_, NL = NL_, N = N_;
+  static constexpr int XB = N * XK * 2;  // bytes per B-digit tile
+  static constexpr bool ALT = N <= 32;   // drain groups take alternate chunks (else split the columns)
   static constexpr int STAGE = NA * XA + NB * XB;
   static constexpr int SMEM = XSTAGES * STAGE + 1024;
-  static_assert(NL * XN <= (int)XTMEM_COLS, "levels must fit in tensor memory");
+  static_assert(N % 16 == 0 && N >= 16 && N <= 64, "N tile: 16, 32 or 64 columns");
+  static_assert(2 * NL * N <= (int)XTMEM_COLS, "two buffers of levels must fit in tensor memory");
   static_assert(SMEM <= 232448, "stages must fit in shared memory");
   __host__ __device__ static constexpr int level(int i, int j) {
     return KIND == 0 ? (NB - 1) - (j - i) : (i + j < NL ? i + j : -1);
   }
 };
-template <int NH>
-using SincScheme = Scheme<NDS, NH, NDS + NH - 1, 0>;
+template <int NH, int N>
+using SincScheme = Scheme<NDS, NH, NDS + NH - 1, 0, N>;
 
 struct XArgs {
   const uint8_t *A;  // NA digit planes of MT*KT tiles, plane stride a_plane bytes
@@ -72,13 +77,15 @@ struct XArgs {
 template <class E>
 __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) {
   extern __shared__ uint8_t smem_raw[];
-  __shared__ __align__(8) unsigned long long bars[2 * XSTAGES + 3];
+  __shared__ __align__(8) unsigned long long bars[2 * XSTAGES + 5];
   __shared__ uint32_t tmem_sh;
   __shared__ int abort_sh;
   const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
   const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[XSTAGES]);
-  const uint32_t tfull = smem_u32(&bars[2 * XSTAGES]), tempty = smem_u32(&bars[2 * XSTAGES + 1]);
-  const uint32_t drain = smem_u32(&bars[2 * XSTAGES + 2]);
+  // per accumulator buffer b: tfull0 + 8 b (MMAs done), tempty0 + 8 b (drained)
+  const uint32_t tfull0 = smem_u32(&bars[2 * XSTAGES]), tempty0 = smem_u32(&bars[2 * XSTAGES + 2]);
+  const uint32_t drain = smem_u32(&bars[2 * XSTAGES + 4]);
+  constexpr uint32_t BUFCOLS = E::NL * E::N;  // tensor-memory columns of one accumulator buffer
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   volatile int *abort = &abort_sh;
 
@@ -87,8 +94,10 @@ __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) 
       mbar_init(full0 + 8 * s, 1);
       mbar_init(empty0 + 8 * s, 1);
     }
-    mbar_init(tfull, 1);
-    mbar_init(tempty, XTHREADS - 64);
+    for (int b = 0; b < 2; b++) {
+      mbar_init(tfull0 + 8 * b, 1);
+      mbar_init(tempty0 + 8 * b, E::ALT ? 128 : XTHREADS - 64);
+    }
     mbar_init(drain, 1);
     abort_sh = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -123,12 +132,12 @@ __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) 
         const unsigned long long r = u / KT;
         const uint32_t mt = (uint32_t)(r % g.MT), nt = (uint32_t)(r / g.MT);
         const uint32_t dst = base + s * E::STAGE, bar = full0 + 8 * s;
-        const size_t ao = ((size_t)mt * g.KT + kt) * XA, bo = ((size_t)nt * g.KT + kt) * XB;
+        const size_t ao = ((size_t)mt * g.KT + kt) * XA, bo = ((size_t)nt * g.KT + kt) * E::XB;
         mbar_expect_tx(bar, (uint32_t)E::STAGE);
 #pragma unroll
         for (int d = 0; d < E::NA; d++) bulk_g2s(dst + d * XA, g.A + d * g.a_plane + ao, XA, bar);
 #pragma unroll
-        for (int e = 0; e < E::NB; e++) bulk_g2s(dst + E::NA * XA + e * XB, g.B + e * g.b_plane + bo, XB, bar);
+        for (int e = 0; e < E::NB; e++) bulk_g2s(dst + E::NA * XA + e * E::XB, g.B + e * g.b_plane + bo, E::XB, bar);
         fills[s] = k + 1;
       }
       if (*abort)
@@ -137,8 +146,8 @@ __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) 
     }
   } else if (warp == 1) {
     if (lane == 0) {  // MMA issuer
-      // kind::f16: F32 accumulator (1), BF16 A and B (1, 1), K-major, N = 64, M = 128
-      const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(XN >> 3) << 17) | ((uint32_t)(XM >> 4) << 24);
+      // kind::f16: F32 accumulator (1), BF16 A and B (1, 1), K-major, N = E::N, M = 128
+      const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(E::N >> 3) << 17) | ((uint32_t)(XM >> 4) << 24);
       uint32_t chunk = 0;  // chunks handed to the drain warps so far
       bool issued = false;
       unsigned long long i = 0;
@@ -148,8 +157,8 @@ __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) 
         const bool seg_first = (u == u0) || (u % KT == 0);
         const bool seg_last = (u + 1 == u1) || ((u + 1) % KT == 0);
         const bool first = seg_first || in_chunk == 0;
-        if (first && chunk > 0) {  // the drain warps have read the previous chunk
-          if (!mbar_wait(tempty, (chunk - 1) & 1u, abort, WAIT_LIMIT_NS)) {
+        if (first && chunk >= 2) {  // the drain warps have read this buffer's previous chunk
+          if (!mbar_wait(tempty0 + 8 * (chunk & 1u), ((chunk >> 1) - 1) & 1u, abort, WAIT_LIMIT_NS)) {
             abort_sh = 1;
             atomicOr(g.err, 1);
             break;
@@ -162,7 +171,7 @@ __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) 
           break;
         }
         tc_fence_after();
-        const uint32_t a0 = base + s * E::STAGE, b0 = a0 + E::NA * XA;
+        const uint32_t a0 = base + s * E::STAGE, b0 = a0 + E::NA * XA, tacc = tmem + (chunk & 1u) * BUFCOLS;
 #pragma unroll
         for (int ks = 0; ks < XK / 16; ks++) {
           const uint32_t off = ks * 32;
@@ -175,7 +184,7 @@ __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) 
               if (lev < 0) continue;
               const uint32_t acc = (first && ks == 0 && !(written & (1u << lev))) ? 0u : 1u;
               written |= 1u << lev;
-              tc_mma(tmem + lev * XN, sw128_desc(a0 + di * XA + off), sw128_desc(b0 + ej * XB + off), idesc, acc);
+              tc_mma(tacc + lev * E::N, sw128_desc(a0 + di * XA + off), sw128_desc(b0 + ej * E::XB + off), idesc, acc);
             }
           }
         }
@@ -183,7 +192,7 @@ __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) 
         tc_commit(empty0 + 8 * s);
         in_chunk++;
         if (seg_last || in_chunk == CH_TILES) {
-          tc_commit(tfull);
+          tc_commit(tfull0 + 8 * (chunk & 1u));
           chunk++;
           in_chunk = 0;
         }
@@ -193,42 +202,49 @@ __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) 
         mbar_wait(drain, 0, nullptr, DRAIN_LIMIT_NS);
       }
     }
-  } else {  // drain: warp w reads TMEM lanes 32*(w%4) .. +31, columns 32*h .. +31
+  } else {
+    // drain: warp w reads TMEM lanes 32*(w%4) .. +31 (its quarter of the 128 rows).  Group h = 0, 1:
+    // with ALT, chunks c with c % 2 == h (buffer h), all N columns; otherwise every chunk, columns
+    // 32 h .. 32 h + 31.
+    constexpr int COLS = E::ALT ? E::N : 32;
     const uint32_t wq = warp & 3, h = (uint32_t)(warp - 2) >> 2;
-    const uint32_t lane_addr = tmem + ((wq * 32u) << 16) + h * 32u;
-    double sum[32];
+    const uint32_t lane_addr = tmem + ((wq * 32u) << 16) + (E::ALT ? 0u : h * 32u);
+    double sum[COLS];
 #pragma unroll
-    for (int j = 0; j < 32; j++) sum[j] = 0.0;
+    for (int j = 0; j < COLS; j++) sum[j] = 0.0;
     uint32_t chunk = 0, in_chunk = 0;
     for (unsigned long long u = u0; u < u1; ++u) {
       const bool seg_last = (u + 1 == u1) || ((u + 1) % KT == 0);
       in_chunk++;
       if (!(seg_last || in_chunk == CH_TILES)) continue;
       in_chunk = 0;
-      const bool ok = mbar_wait(tfull, chunk & 1u, abort, WAIT_LIMIT_NS);
-      if (__any_sync(0xffffffffu, !ok)) {
-        abort_sh = 1;
-        if (lane == 0) atomicOr(g.err, 1);
-        break;
-      }
-      tc_fence_after();
-#pragma unroll
-      for (int c = 0; c < 32; c += 16) {
-        double t[16];
-#pragma unroll
-        for (int j = 0; j < 16; j++) t[j] = 0.0;
-#pragma unroll
-        for (int lev = 0; lev < E::NL; lev++) {  // Horner over the levels, top first
-          uint32_t rr[16];
-          tc_ld16_raw(lane_addr + lev * XN + c, rr);
-#pragma unroll
-          for (int j = 0; j < 16; j++) t[j] = t[j] * 256.0 + (double)__uint_as_float(rr[j]);
+      const uint32_t b = chunk & 1u;
+      if (!E::ALT || b == h) {
+        const bool ok = mbar_wait(tfull0 + 8 * b, (chunk >> 1) & 1u, abort, WAIT_LIMIT_NS);
+        if (__any_sync(0xffffffffu, !ok)) {
+          abort_sh = 1;
+          if (lane == 0) atomicOr(g.err, 1);
+          break;
         }
+        tc_fence_after();
 #pragma unroll
-        for (int j = 0; j < 16; j++) sum[c + j] += t[j];
+        for (int c = 0; c < COLS; c += 16) {
+          double t[16];
+#pragma unroll
+          for (int j = 0; j < 16; j++) t[j] = 0.0;
+#pragma unroll
+          for (int lev = 0; lev < E::NL; lev++) {  // Horner over the levels, top first
+            uint32_t rr[16];
+            tc_ld16_raw(lane_addr + b * BUFCOLS + lev * E::N + c, rr);
+#pragma unroll
+            for (int j = 0; j < 16; j++) t[j] = t[j] * 256.0 + (double)__uint_as_float(rr[j]);
+          }
+#pragma unroll
+          for (int j = 0; j < 16; j++) sum[c + j] += t[j];
+        }
+        tc_fence_before();
+        mbar_arrive(tempty0 + 8 * b);
       }
-      tc_fence_before();
-      mbar_arrive(tempty);
       chunk++;
       if (seg_last) {
         const unsigned long long r = u / KT;
@@ -237,13 +253,13 @@ __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) 
         const double scale = g.scale;
         if (m < g.m_valid) {
 #pragma unroll
-          for (int j = 0; j < 32; j++) {
-            const uint32_t n = nt * XN + h * 32 + j;
-            if (n < g.n_valid) atomicAdd(g.out + (size_t)n * g.ldo + m, sum[j] * scale);
+          for (int j = 0; j < COLS; j++) {
+            const uint32_t n = nt * E::N + (E::ALT ? 0u : h * 32u) + j;
+            if (n < g.n_valid && sum[j] != 0.0) atomicAdd(g.out + (size_t)n * g.ldo + m, sum[j] * scale);
           }
         }
 #pragma unroll
-        for (int j = 0; j < 32; j++) sum[j] = 0.0;
+        for (int j = 0; j < COLS; j++) sum[j] = 0.0;
       }
     }
   }
@@ -303,15 +319,15 @@ __global__ void pack_sinc_digits_kernel(const double *__restrict__ q, uint32_t n
   }
 }
 
-// One CTA per (nt, kt) tile of XN rows (histogram columns).  Sets *overflow when a count needs more
+// One CTA per (nt, kt) tile of N rows (histogram columns).  Sets *overflow when a count needs more
 // than NH digits.
-template <int NH>
+template <int NH, int N>
 __global__ void pack_count_digits_kernel(const unsigned long long *__restrict__ hist, uint32_t ncols, uint32_t nh,
                                          size_t ldh, uint32_t KT, uint8_t *__restrict__ B, size_t b_plane,
                                          int *overflow) {
   const uint32_t tile = blockIdx.x, nt = tile / KT, kt = tile % KT;
-  for (uint32_t c = threadIdx.x; c < XN * 8; c += blockDim.x) {
-    const uint32_t row = c >> 3, ch = c & 7, n = nt * XN + row, k0 = kt * XK + ch * 8;
+  for (uint32_t c = threadIdx.x; c < N * 8; c += blockDim.x) {
+    const uint32_t row = c >> 3, ch = c & 7, n = nt * N + row, k0 = kt * XK + ch * 8;
     float dig[NH][8];
     bool big = false;
 #pragma unroll
@@ -323,7 +339,7 @@ __global__ void pack_count_digits_kernel(const unsigned long long *__restrict__ 
       for (int e = 0; e < NH; e++) dig[e][i] = (float)((v >> (8 * e)) & 255u);
     }
     if (big) atomicOr(overflow, 1);
-    const size_t off = (size_t)tile * XB + chunk_offset(row, ch);
+    const size_t off = (size_t)tile * (N * XK * 2) + chunk_offset(row, ch);
 #pragma unroll
     for (int e = 0; e < NH; e++) *(uint4 *)(B + e * b_plane + off) = pack8(dig[e]);
   }
@@ -354,10 +370,10 @@ int launch_digit_gemm(xns_ctx *ctx, const XArgs &g, unsigned grid) {
   return XNS_OK;
 }
 
-template <int NH>
+template <int NH, int N>
 int enqueue_exact(xns_ctx *ctx, const ExactLaunch &X) {
-  pack_count_digits_kernel<NH><<<X.NT * X.KT, 256, 0, ctx->stream>>>(X.hist, X.ncols, X.nh, X.ldh, X.KT, X.B, X.b_plane,
-                                                                      X.flags + 1);
+  pack_count_digits_kernel<NH, N><<<X.NT * X.KT, 256, 0, ctx->stream>>>(X.hist, X.ncols, X.nh, X.ldh, X.KT, X.B,
+                                                                         X.b_plane, X.flags + 1);
   XNS_LAUNCHED(ctx);
   XArgs g{};
   g.A = X.A;
@@ -374,7 +390,12 @@ int enqueue_exact(xns_ctx *ctx, const ExactLaunch &X) {
   g.err = X.flags;
   // level l holds 256^(NH-1-l)/128; the Horner sum weights it 256^(NL-1-l): one unit is 256^-(NDS-1)/128
   g.scale = ldexp(1.0, -8 * (NDS - 1)) / 128.0;
-  return launch_digit_gemm<SincScheme<NH>>(ctx, g, 0);
+  return launch_digit_gemm<SincScheme<NH, N>>(ctx, g, 0);
+}
+
+template <int NH>
+int enqueue_exact_n(xns_ctx *ctx, const ExactLaunch &X) {
+  return X.ntile == 16 ? enqueue_exact<NH, 16>(ctx, X) : enqueue_exact<NH, 32>(ctx, X);
 }
 
 // ---- 2D amplitude on a Cartesian q plane ---------------------------------------------------------
@@ -387,7 +408,9 @@ int enqueue_exact(xns_ctx *ctx, const ExactLaunch &X) {
 // (PlaneScheme).  Three digits (residual 2^-24) leave 1e-5..3e-5 of I at the dim points of a crystal's
 // pattern, where the rounding of the lattice's repeated phases adds coherently; four leave 2^-32.
 constexpr int PD = 4;
-using PlaneScheme = Scheme<PD, PD, PD, 1>;
+constexpr int PN = 64;                 // plane: B tile rows (qy rows for Re, then for Im)
+constexpr int PXB = PN * XK * 2;
+using PlaneScheme = Scheme<PD, PD, PD, 1, PN>;
 
 __device__ __forceinline__ void put_digits(uint8_t *plane0, size_t plane, size_t off, double v) {
   double r = v * 128.0;
@@ -427,9 +450,9 @@ __global__ void plane_pack_b_kernel(const double *__restrict__ y, uint32_t n, do
   const double yj = use ? y[second ? k - n : k] : 0.0;
   double s = 0, c = 1, sd, cd;
   sincos(dq * yj, &sd, &cd);
-  uint8_t *t0 = B + (size_t)tile * XB;
-  for (uint32_t row = 0; row < XN; row++) {
-    const uint32_t np = nt * XN + row, part = np >= nq ? 1u : 0u, iy = np - part * nq;
+  uint8_t *t0 = B + (size_t)tile * PXB;
+  for (uint32_t row = 0; row < PN; row++) {
+    const uint32_t np = nt * PN + row, part = np >= nq ? 1u : 0u, iy = np - part * nq;
     if (row == 0 || iy == 0) sincos((q0 + (double)iy * dq) * yj, &s, &c);  // new run of qy
     double v = 0.0;
     if (use && np < 2 * nq) v = part == 0 ? (second ? -s : c) : (second ? c : s);
@@ -481,7 +504,9 @@ int xns_tc_exact_plan(xns_ctx *ctx, const unsigned long long *d_hist, uint32_t n
   X->G = d_G;
   X->MT = (nq + XM - 1) / XM;
   X->KT = (nh + XK - 1) / XK;
-  X->NT = (ncols + XN - 1) / XN;
+  // narrow N tiles: the accumulators of two chunks must fit in tensor memory (2 x levels x N <= 512)
+  X->ntile = ncols <= 16 ? 16 : 32;
+  X->NT = (ncols + X->ntile - 1) / X->ntile;
   int st;
   void *flags;
   if ((st = xns_scratch(ctx, SLOT_FLAGS, 64, &flags))) return st;
@@ -504,7 +529,7 @@ int xns_tc_exact_plan(xns_ctx *ctx, const unsigned long long *d_hist, uint32_t n
     ctx->x_kt = X->KT;
   }
   X->A = (const uint8_t *)A;
-  X->b_plane = (size_t)X->NT * X->KT * XB;
+  X->b_plane = (size_t)X->NT * X->KT * X->ntile * XK * 2;
   void *B;
   if ((st = xns_scratch(ctx, SLOT_TC_B, X->digits * X->b_plane, &B))) return st;
   X->B = (uint8_t *)B;
@@ -516,9 +541,9 @@ int xns_tc_exact_enqueue(xns_ctx *ctx, const ExactLaunch &X) {
   XNS_CUDA(ctx, cudaMemsetAsync(X.flags, 0, 2 * sizeof(int), ctx->stream));
   XNS_CUDA(ctx, cudaMemsetAsync(X.G, 0, sizeof(double) * X.ncols * X.nq, ctx->stream));
   switch (X.digits) {
-    case 2: return enqueue_exact<2>(ctx, X);
-    case 3: return enqueue_exact<3>(ctx, X);
-    default: return enqueue_exact<4>(ctx, X);
+    case 2: return enqueue_exact_n<2>(ctx, X);
+    case 3: return enqueue_exact_n<3>(ctx, X);
+    default: return enqueue_exact_n<4>(ctx, X);
   }
 }
 
@@ -607,12 +632,12 @@ extern "C" int xns_calc_amp_plane(xns_ctx *ctx, const double *const *xyz_el, con
   if ((st = xns_stage_begin(ctx, STAGE_2D))) return st;
   XNS_CUDA(ctx, cudaMemsetAsync(vacc, 0, sizeof(double) * 2 * npix, ctx->stream));
   XNS_CUDA(ctx, cudaMemsetAsync(flags, 0, sizeof(int), ctx->stream));
-  const uint32_t MT = (nqx + XM - 1) / XM, NT = (2 * nqy + XN - 1) / XN;
+  const uint32_t MT = (nqx + XM - 1) / XM, NT = (2 * nqy + PN - 1) / PN;
   for (uint32_t e = 0; e < nel; e++) {
     const uint32_t n = dc.n_el[e];
     if (!n) continue;
     const uint32_t KT = (2 * n + XK - 1) / XK;
-    const size_t a_plane = (size_t)MT * KT * XA, b_plane = (size_t)NT * KT * XB;
+    const size_t a_plane = (size_t)MT * KT * XA, b_plane = (size_t)NT * KT * PXB;
     void *A, *B;
     if ((st = xns_scratch(ctx, SLOT_X_A, PD * a_plane, &A))) return st;
     if ((st = xns_scratch(ctx, SLOT_TC_B, PD * b_plane, &B))) return st;

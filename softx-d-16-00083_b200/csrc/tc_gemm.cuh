@@ -69,6 +69,7 @@ struct ExactLaunch {
   uint32_t ncols = 0, nh = 0, nq = 0, MT = 0, NT = 0, KT = 0;
   size_t ldh = 0, a_plane = 0, b_plane = 0;
   int digits = 0;  // count digits: 2, 3 or 4 (counts below 2^16, 2^24, 2^32)
+  uint32_t ntile = 0;  // columns per N tile: 16 or 32
   const uint8_t *A = nullptr;
   uint8_t *B = nullptr;
   double *G = nullptr;
