@@ -72,6 +72,7 @@ struct XArgs {
   uint32_t ldo, m_valid, n_valid;
   double scale;  // value of one unit of the Horner sum over the levels
   int *err;
+  uint32_t ksplit;  // 0: stream-K over all units; else K parts per output tile (grid = parts x tiles)
 };
 
 template <class E>
@@ -115,7 +116,17 @@ __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) 
 
   const unsigned long long KT = g.KT;
   const unsigned long long units = (unsigned long long)g.NT * g.MT * KT;
-  const unsigned long long u0 = units * blockIdx.x / gridDim.x, u1 = units * (blockIdx.x + 1) / gridDim.x;
+  // ksplit 0: the units are cut into gridDim.x equal ranges (stream-K); ksplit > 0: CTA b takes K part
+  // b / tiles of output tile b % tiles (CTAs that run together work on the same K part)
+  unsigned long long u0, u1;
+  if (g.ksplit) {
+    const unsigned long long tiles = (unsigned long long)g.NT * g.MT, t = blockIdx.x % tiles, kq = blockIdx.x / tiles;
+    u0 = t * KT + KT * kq / g.ksplit;
+    u1 = t * KT + KT * (kq + 1) / g.ksplit;
+  } else {
+    u0 = units * blockIdx.x / gridDim.x;
+    u1 = units * (blockIdx.x + 1) / gridDim.x;
+  }
 
   if (warp == 0) {
     if (lane == 0) {  // loader
@@ -662,8 +673,23 @@ extern "C" int xns_calc_amp_plane(xns_ctx *ctx, const double *const *xyz_el, con
     g.n_valid = 2 * nqy;
     g.scale = ldexp(1.0, -14 - 8 * (PD - 1));  // (1/128)^2 per unit of level 0, Horner over PD levels
     g.err = (int *)flags;
-    // one CTA per output tile: CTAs that run together read the same k tiles, which stay in L2
-    if ((st = launch_digit_gemm<PlaneScheme>(ctx, g, MT * NT))) return st;
+    // CTAs that run together work on the same K part of neighbouring output tiles, so they read the same
+    // k tiles, which stay in L2.  K is cut into parts so that the last wave of CTAs is nearly full.
+    uint32_t ks = 1;
+    {
+      const uint32_t tiles = MT * NT, sms = (uint32_t)ctx->num_sms;
+      double best = 0;
+      for (uint32_t c = 1; c <= 8 && c <= KT; c++) {
+        const uint32_t n = c * tiles, waves = (n + sms - 1) / sms;
+        const double fill = (double)n / ((double)waves * sms);
+        if (fill > best + 0.02) {
+          best = fill;
+          ks = c;
+        }
+      }
+    }
+    g.ksplit = ks;
+    if ((st = launch_digit_gemm<PlaneScheme>(ctx, g, ks * MT * NT))) return st;
     plane_accum_kernel<<<(unsigned)((npix + 255) / 256), 256, 0, ctx->stream>>>(
         (const double *)vC, nqx, nqy, qx0, dqx, qy0, dqy, vcoef ? (const double *)vcoef + 9 * e : nullptr,
         vcoef ? 0.0 : sl[e], Ar, Ai);
