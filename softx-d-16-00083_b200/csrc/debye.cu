@@ -17,7 +17,7 @@ using namespace xns_sinc;
 
 namespace {
 
-constexpr int DB_TI = 16, DB_TJ = 96;
+constexpr int DB_TI = 8, DB_TJ = 48;
 static_assert(DB_TI * DB_TJ == SE_TILE, "tile pair must fill one record tile");
 
 struct AtomPairSrc {

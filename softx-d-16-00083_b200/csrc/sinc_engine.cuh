@@ -29,7 +29,10 @@
 namespace xns_sinc {
 
 constexpr int SE_THREADS = 128;
-constexpr int SE_TILE = 1536;
+// Records per tile.  With M = 64 the FP64 totals take 64 KB of shared memory per CTA; 384 records
+// (9 KB) keep a CTA under a third of the SM's shared memory, so that three CTAs (12 warps, at most 168
+// registers a thread) share an SM.
+constexpr int SE_TILE = 384;
 // q values per lane: M_UNIFORM for the recurrence (a seed costs ~30 instructions, the recurrence 2.75
 // per term), M_DIRECT for the per-term sine of a non-uniform mesh.
 constexpr int SE_M_UNIFORM = 64;
@@ -74,7 +77,7 @@ struct SincParams {
 // Shared memory: [M][SE_THREADS] FP64 totals (one column per thread), then SE_TILE records, then the
 // Source's own staging area.
 template <int M, bool DIRECT, class Src>
-__global__ void __launch_bounds__(SE_THREADS, 2) sinc_tiles_kernel(SincParams p, Src src, int lanes_per_slot) {
+__global__ void __launch_bounds__(SE_THREADS, 3) sinc_tiles_kernel(SincParams p, Src src, int lanes_per_slot) {
   extern __shared__ double acc64[];
   PairRec *pr = reinterpret_cast<PairRec *>(acc64 + M * SE_THREADS);
   void *stage = reinterpret_cast<void *>(pr + SE_TILE);
