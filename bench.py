@@ -424,7 +424,7 @@ def debye_workload(args):
         while True:
             sub = [els[0][:m]]
             t = time.perf_counter()
-            R.int_debye(sub, q, 0, sl=[7.63])
+            Iref = R.int_debye(sub, q, 0, sl=[7.63])
             dt = time.perf_counter() - t
             if dt > 3.0 or m >= n:
                 break
@@ -432,6 +432,15 @@ def debye_workload(args):
         sp = m * (m - 1) // 2
         line["cpu_baseline"] = {"value": sp / dt, "unit": "pairs/s", "cores": cores, "kind": kind,
                                 "sample": "calcIntDebye on the first %d atoms of the sphere, 1024 q, %.2f s" % (m, dt)}
+        # accuracy of the whole pattern against the reference's FP64 sum
+        if m < n:
+            sub = els
+            Iref = R.int_debye(sub, q, 0, sl=[7.63])
+        I = ctx.calc_int_debye(sub, q, xns_b200.NEUTRON, sl=[7.63])
+        rel = np.abs(I - Iref) / np.abs(Iref)
+        line["max_rel_err_vs_reference"] = {"atoms": n, "max": float(rel.max()), "q_at_max": float(q[int(rel.argmax())]),
+                                            "I_at_max_over_max_I": float(abs(Iref[int(rel.argmax())]) / np.abs(Iref).max()),
+                                            "points_above_1e-5": int((rel > 1e-5).sum()), "points": len(q)}
     print(json.dumps(line))
     ctx.close()
     return 0
