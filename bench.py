@@ -75,6 +75,26 @@ def config_block(els, nh, extra=None, cells=CELLS):
     return c
 
 
+# ---- ranks ------------------------------------------------------------------------------------------
+def rank_max(x, device=None):
+    """The largest x over the ranks of the default process group (x itself without one): every rank
+    reports the slowest rank's time, so the whole job's rate is the units all ranks processed divided by
+    it."""
+    import torch
+    import torch.distributed as tdist
+    if not (tdist.is_available() and tdist.is_initialized()):
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, units_per_rank, ms_max):
+    """Whole-job throughput of weak-scaling replicas: world ranks of units_per_rank each, in the slowest
+    rank's time."""
+    return world * units_per_rank / (ms_max * 1e-3)
+
+
 # ---- clocks -----------------------------------------------------------------------------------------
 class Clocks:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
@@ -265,11 +285,7 @@ def ours(args, rank, world, local_rank):
     barrier()
     launches = ctx.kernel_launches - launches0
     clk = clocks.stop()
-    ms_step = total_ms / args.steps
-    if dist:
-        t = torch.tensor([ms_step], device=dev)
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        ms_step = float(t.item())
+    ms_step = rank_max(total_ms / args.steps, dev)
 
     # end-to-end through the host-buffer C ABI from pinned host memory
     pin_xyz = [torch.from_numpy(np.ascontiguousarray(e)).pin_memory() for e in els]
@@ -297,11 +313,7 @@ def ours(args, rank, world, local_rank):
         ev1.record(stream)
         ev1.synchronize()
         e2e_ms += ev0.elapsed_time(ev1)
-    e2e_ms /= args.steps
-    if dist:
-        t = torch.tensor([e2e_ms], device=dev)
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = rank_max(e2e_ms / args.steps, dev)
     h2d = int(xyz.nbytes + q.nbytes + sl.nbytes)
     d2h = int(NQ * 8 + (1 + P) * nh * 8)
 
@@ -317,7 +329,7 @@ def ours(args, rank, world, local_rank):
     lib.xns_measure_fma_peak(ctx.handle, 1, C.byref(peak))
     hist_avg = hist_ms / args.steps
     inc = pairs / (hist_avg * 1e-3) / 1e9
-    line = {"metric": METRIC, "value": world * pairs / (ms_step * 1e-3), "unit": "pairs/s", "n_gpus": world,
+    line = {"metric": METRIC, "value": job_rate(world, pairs, ms_step), "unit": "pairs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 distance estimate + f64 exact re-binning near bin edges, u64 counts (histogram); integer-digit "
@@ -334,7 +346,7 @@ def ours(args, rank, world, local_rank):
                          "peak_source": "measured in-process (conflict-free atomicAdd loop, xns_measure_smem_atomic_peak)",
                          "fp64_view": {"flops_per_pair": HIST_FLOPS_PER_PAIR, "peak_tflops": peak.value,
                                        "frac": HIST_FLOPS_PER_PAIR * pairs / (hist_avg * 1e-3) / 1e12 / peak.value}},
-            "e2e": {"value": world * pairs / (e2e_ms * 1e-3), "unit": "pairs/s", "ms_per_step": e2e_ms,
+            "e2e": {"value": job_rate(world, pairs, e2e_ms), "unit": "pairs/s", "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches), "clocks": clk}
     if world == 1 and not args.no_cpu_baseline:
