@@ -294,21 +294,44 @@ __device__ __forceinline__ uint32_t pair_key(const KeyParams &p, unsigned long l
   return g.cls * p.nbuckets + min(tp->kmin, p.nhist) / BUCKET;
 }
 
+// Consecutive tile pairs (a tile against its neighbours' tiles) mostly share a distance bucket, so the
+// lanes of a warp group by key (match.any) and one lane per key does the warp's atomic.
 __global__ void pair_key_kernel(KeyParams p, uint32_t *__restrict__ kcnt) {
-  for (unsigned long long w = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; w < p.ntp;
-       w += (unsigned long long)gridDim.x * blockDim.x) {
-    TilePair tp;
-    atomicAdd(kcnt + pair_key(p, w, &tp), 1u);
+  const uint32_t lane = threadIdx.x & 31;
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  for (unsigned long long w0 = blockIdx.x * (unsigned long long)blockDim.x + (threadIdx.x & ~31u); w0 < p.ntp;
+       w0 += stride) {
+    const unsigned long long w = w0 + lane;
+    const bool act = w < p.ntp;
+    const unsigned act_mask = __ballot_sync(0xffffffffu, act);
+    if (act) {
+      TilePair tp;
+      const uint32_t key = pair_key(p, w, &tp);
+      const unsigned same = __match_any_sync(act_mask, key);
+      if (lane == (uint32_t)(__ffs(same) - 1)) atomicAdd(kcnt + key, (uint32_t)__popc(same));
+    }
   }
 }
 
 __global__ void pair_scatter_kernel(KeyParams p, const uint32_t *__restrict__ koff, uint32_t *__restrict__ kcur,
                                     TilePair *__restrict__ list) {
-  for (unsigned long long w = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; w < p.ntp;
-       w += (unsigned long long)gridDim.x * blockDim.x) {
-    TilePair tp;
-    const uint32_t key = pair_key(p, w, &tp);
-    list[koff[key] + atomicAdd(kcur + key, 1u)] = tp;
+  const uint32_t lane = threadIdx.x & 31;
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  for (unsigned long long w0 = blockIdx.x * (unsigned long long)blockDim.x + (threadIdx.x & ~31u); w0 < p.ntp;
+       w0 += stride) {
+    const unsigned long long w = w0 + lane;
+    const bool act = w < p.ntp;
+    const unsigned act_mask = __ballot_sync(0xffffffffu, act);
+    if (act) {
+      TilePair tp;
+      const uint32_t key = pair_key(p, w, &tp);
+      const unsigned same = __match_any_sync(act_mask, key);
+      const uint32_t leader = (uint32_t)(__ffs(same) - 1);
+      uint32_t at = 0;
+      if (lane == leader) at = atomicAdd(kcur + key, (uint32_t)__popc(same));
+      at = __shfl_sync(same, at, leader) + (uint32_t)__popc(same & ((1u << lane) - 1u));
+      list[koff[key] + at] = tp;
+    }
   }
 }
 
