@@ -13,8 +13,8 @@
 // which is the Chebyshev recurrence s_{k+1} = 2cos(t) s_k - s_{k-1} with 2cos(t) kept as 2 - lam: lam
 // carries full relative precision even for small t, so the phase does not drift the way a rounded
 // 2cos(t) (error 2^-24 / sin t per step) would on fine q meshes.  A lane runs four records side by
-// side: per (record, q) term one FFMA and one FADD for the sine, plus 3/4 FADD for the pairwise sum of
-// the four, no transcendental.  Sums run in FP32 over SE_FP32_GROUPS groups and are then added to
+// side, as two packed pairs (f32x2.cuh): per (record, q) term one FFMA and one FADD for the sine, plus
+// 3/4 FADD for the pairwise sum of the four, no transcendental, in 7 instructions per four terms.  Sums run in FP32 over SE_FP32_GROUPS groups and are then added to
 // per-thread FP64 totals in shared memory (compensated block accumulation); CTAs then reduce in FP64
 // in the epilogue.  1/q_k is applied in the epilogue.  A mesh that is not uniform takes an accurate
 // sine per term (DIRECT).
@@ -23,6 +23,7 @@
 
 #include <algorithm>
 
+#include "f32x2.cuh"
 #include "xmath.cuh"
 #include "xns_internal.cuh"
 
@@ -150,15 +151,20 @@ __global__ void __launch_bounds__(SE_THREADS, 3) sinc_tiles_kernel(SincParams p,
             d[g] = R[g].h2 * fmaf(cx, R[g].ch, sx * (0.5f * R[g].h2)) * R[g].w_r;
             lam[g] = R[g].lam;
           }
-          blk[0] += (s[0] + s[1]) + (s[2] + s[3]);
+          // the recurrence on packed pairs of records (0, 1) and (2, 3): the same roundings as scalar
+          // FFMA / FADD, half the instructions
+          using namespace xns_f2;
+          f2 S01 = pack(s[0], s[1]), S23 = pack(s[2], s[3]), D01 = pack(d[0], d[1]), D23 = pack(d[2], d[3]);
+          const f2 L01 = pack(-lam[0], -lam[1]), L23 = pack(-lam[2], -lam[3]);
+          blk[0] += (s[0] + s[2]) + (s[1] + s[3]);
 #pragma unroll
           for (int k = 1; k < M; k++) {
-#pragma unroll
-            for (int g = 0; g < 4; g++) {
-              d[g] = fmaf(-lam[g], s[g], d[g]);
-              s[g] += d[g];
-            }
-            blk[k] += (s[0] + s[1]) + (s[2] + s[3]);
+            D01 = xns_f2::fma(L01, S01, D01);
+            D23 = xns_f2::fma(L23, S23, D23);
+            S01 = add(S01, D01);
+            S23 = add(S23, D23);
+            const f2 u = add(S01, S23);  // (s0 + s2, s1 + s3)
+            blk[k] += lo(u) + hi(u);
           }
         }
       }
