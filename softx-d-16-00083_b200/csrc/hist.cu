@@ -30,6 +30,7 @@
 #include <cmath>
 
 #include "hist_bin.cuh"
+#include "f32x2.cuh"
 #include "hist_set.cuh"
 #include "schedule.cuh"
 
@@ -449,7 +450,10 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
                                                       uint8_t *stage, uint32_t *win, uint32_t base,
                                                       unsigned long long *h) {
   double *wI = reinterpret_cast<double *>(stage);
-  float4 *wI4 = reinterpret_cast<float4 *>(wI + 3 * TILE_MAX);  // per I atom: offsets (+ P_i, centred)
+  // I rows in pairs (2p, 2p + 1), 8 floats a pair: x x' y y' z z' w w' (offsets; w = P_i, centred), so
+  // that two 16-byte loads give both rows' values as packed pairs
+  float *wIf = reinterpret_cast<float *>(wI + 3 * TILE_MAX);
+  float4 *wI4 = reinterpret_cast<float4 *>(wIf);
   uint16_t *queue = reinterpret_cast<uint16_t *>(wI4 + TILE_MAX);
   const uint32_t lane = threadIdx.x & 31;
   const Tile TI = p.tiles[tp.I], TJ = p.tiles[tp.J];
@@ -491,7 +495,11 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
     const double ax = (x - cI[0]) * ib, ay = (y - cI[1]) * ib, az = (z - cI[2]) * ib;
     float P = 0.f;
     if (CENTRED) P = (float)(2.0 * (g.D[0] * ax + g.D[1] * ay + g.D[2] * az) + (ax * ax + ay * ay + az * az));
-    wI4[i] = make_float4((float)ax, (float)ay, (float)az, P);
+    float *row = wIf + (i >> 1) * 8 + (i & 1);
+    row[0] = (float)ax;
+    row[2] = (float)ay;
+    row[4] = (float)az;
+    row[6] = P;
   }
   const uint32_t j0 = lane, j1 = lane + 32;
   const bool c0 = j0 < nj, c1 = j1 < nj;
@@ -530,13 +538,33 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
       zj1 = (float)bz1 - dl[2];
     }
   }
+  // centred: the J atoms' values and the tile pair's constants as packed pairs (both halves equal)
+  xns_f2::f2 XJ0 = 0, YJ0 = 0, ZJ0 = 0, QJ0 = 0, XJ1 = 0, YJ1 = 0, ZJ1 = 0, QJ1 = 0;
+  xns_f2::f2 R0SQ2 = 0, R0F2 = 0, R0FR2 = 0, MAGIC2 = 0, NK1_2 = 0, MC2 = 0;
+  if (CENTRED) {
+    using xns_f2::splat;
+    XJ0 = splat(xj0);
+    YJ0 = splat(yj0);
+    ZJ0 = splat(zj0);
+    QJ0 = splat(qj0);
+    XJ1 = splat(xj1);
+    YJ1 = splat(yj1);
+    ZJ1 = splat(zj1);
+    QJ1 = splat(qj1);
+    R0SQ2 = splat(cc.R0sq);
+    R0F2 = splat(cc.R0f);
+    R0FR2 = splat(cc.R0fr);
+    MAGIC2 = splat(MAGIC);
+    NK1_2 = splat(-cc.K1);
+    MC2 = splat(cc.mc);
+  }
   __syncwarp();
   const uint32_t below = (1u << lane) - 1u;  // lanes below this one
   const double nhm1 = (double)p.nhist - 1.0;
   uint32_t qn = 0, qd = 0;  // entries queued / binned (warp-uniform)
   unsigned bad = 0;
   // Lane l bins the pairs of queued entry qd + l exactly (l < n), then n entries are done.  An entry is
-  // one lane's near pairs of one step: rows i, i + 1 against that lane's J atoms (lane, lane + 32),
+  // one lane's near pairs of one row pair: rows i, i + 1 against that lane's J atoms (lane, lane + 32),
   // bit k of the mask standing for row i + k / 2 and J atom lane + 32 (k & 1).  The warp drains full
   // batches of 32 while it counts, so every lane has an entry.
   auto drain = [&](uint32_t n) {
@@ -568,7 +596,7 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
   };
   // FAST: the estimate's bin is certain and its slot is below Wl; a lane without a fast pair adds 0 to
   // its own spare slot (branch-free), near pairs set their bit K of the step's mask.
-#define XNS_COUNT(FAST, SLOT, VALID, K)                                                     \
+#define XNS_COUNT(FAST, SLOT, VALID, K, NM)                                                 \
   {                                                                                         \
     const bool fast = (VALID) && (FAST) && (SLOT) < Wl;                                     \
     if (WINDOW) {                                                                           \
@@ -576,9 +604,9 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
     } else if (fast) {                                                                      \
       atomicAdd(h + (SLOT), 1ull);                                                          \
     }                                                                                       \
-    nm |= ((VALID) && !fast) ? (1u << (K)) : 0u;                                            \
+    NM |= ((VALID) && !fast) ? (1u << (K)) : 0u;                                            \
   }
-#define XNS_DIRECT(RA, XJ, YJ, ZJ, VALID, K)                                                \
+#define XNS_DIRECT(RA, XJ, YJ, ZJ, VALID, K, NM)                                            \
   {                                                                                         \
     const float dx = dh[0] + (RA.x - XJ), dy = dh[1] + (RA.y - YJ), dz = dh[2] + (RA.z - ZJ); \
     const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));                                   \
@@ -589,52 +617,82 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
     const float t = r + MAGIC;                                                              \
     const float d = r - (t - MAGIC);                                                        \
     const uint32_t slot = (uint32_t)(__float_as_int(t) - tbase) - (d < 0.f ? 1u : 0u);      \
-    XNS_COUNT(fabsf(d) >= fmaf(r, mr, m0), slot, VALID, K)                                  \
+    XNS_COUNT(fabsf(d) >= fmaf(r, mr, m0), slot, VALID, K, NM)                              \
   }
-#define XNS_CENTRED(RA, XJ, YJ, ZJ, QJ, VALID, K)                                           \
+// Two pairs at once (rows i, i + 1 against one J atom) on packed f32x2 pairs: the scalar operations
+// in the same order, so the same roundings and the same bound, in half the instructions.
+#define XNS_CENTRED2(RX, RY, RZ, RW, XJ, YJ, ZJ, QJ, VLO, VHI, KLO, KHI, NM)                \
   {                                                                                         \
-    const float num = (RA.w - QJ) + fmaf(RA.x, XJ, fmaf(RA.y, YJ, RA.z * ZJ));              \
-    const float d2 = num + cc.R0sq;                                                         \
-    float y, rc;                                                                            \
-    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(d2));                                \
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rc) : "f"(fmaf(d2, y, cc.R0f)));                \
-    const float t = fmaf(num, rc, cc.R0fr); /* r - floor(R0) - 0.5 */                       \
-    const float tm = t + MAGIC;                                                             \
-    const float d = t - (tm - MAGIC);                                                       \
-    const uint32_t slot = (uint32_t)(__float_as_int(tm) - tbase);                           \
-    XNS_COUNT(fabsf(d) <= fmaf(fabsf(t), -cc.K1, cc.mc), slot, VALID, K)                    \
+    using namespace xns_f2;                                                                 \
+    const f2 num = add(sub(RW, QJ), xns_f2::fma(RX, XJ, xns_f2::fma(RY, YJ, mul(RZ, ZJ)))); \
+    const f2 d2 = add(num, R0SQ2);                                                          \
+    float y0, y1, c0_, c1_;                                                                 \
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y0) : "f"(lo(d2)));                           \
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y1) : "f"(hi(d2)));                           \
+    const f2 den = xns_f2::fma(d2, pack(y0, y1), R0F2);                                     \
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(c0_) : "f"(lo(den)));                           \
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(c1_) : "f"(hi(den)));                           \
+    const f2 t = xns_f2::fma(num, pack(c0_, c1_), R0FR2); /* r - floor(R0) - 0.5 */         \
+    const f2 tm = add(t, MAGIC2);                                                           \
+    const f2 d = sub(t, sub(tm, MAGIC2));                                                   \
+    const f2 m = xns_f2::fma(xns_f2::abs(t), NK1_2, MC2);                                   \
+    const uint32_t slo = (uint32_t)(__float_as_int(lo(tm)) - tbase);                        \
+    const uint32_t shi = (uint32_t)(__float_as_int(hi(tm)) - tbase);                        \
+    XNS_COUNT(fabsf(lo(d)) <= lo(m), slo, VLO, KLO, NM)                                     \
+    XNS_COUNT(fabsf(hi(d)) <= hi(m), shi, VHI, KHI, NM)                                     \
   }
-  for (uint32_t i = 0; i < ni; i += 2) {
-    const uint32_t i1 = min(i + 1, ni - 1);
-    const float4 ra = wI4[i], rb = wI4[i1];
-    const bool r1 = i + 1 < ni;
-    bool v0 = c0, v1 = c1, v2 = c0 && r1, v3 = c1 && r1;
+  // lanes with near pairs in the step's row pair ROW, ROW + 1 append one entry each, in lane order;
+  // fewer than 32 entries wait between pushes and a push adds at most 32: never more than 63 queued
+#define XNS_PUSH(NM, ROW)                                                                   \
+  {                                                                                         \
+    const unsigned nb = __ballot_sync(0xffffffffu, NM != 0);                                \
+    if (NM) queue[(qn + __popc(nb & below)) & (QUEUE - 1)] = (uint16_t)((((ROW) >> 1) << 9) | (lane << 4) | NM); \
+    qn += __popc(nb);                                                                       \
+    while (qn - qd >= 32) drain(32);                                                        \
+  }
+  // a step: rows i .. i + 3 (two row pairs) against the lane's two J atoms; rows at or beyond ni hold
+  // stale data, their pairs are not valid
+  for (uint32_t i = 0; i < ni; i += 4) {
+    const float4 pa = wI4[i], pb = wI4[i + 1], pc = wI4[i + 2], pd = wI4[i + 3];  // (x x' y y'), (z z' w w')
+    bool va0 = c0, va1 = c1, vb0 = c0 && i + 1 < ni, vb1 = c1 && i + 1 < ni;
+    bool vc0 = c0 && i + 2 < ni, vc1 = c1 && i + 2 < ni, vd0 = c0 && i + 3 < ni, vd1 = c1 && i + 3 < ni;
     if (SAME) {
-      v0 = v0 && i < j0;
-      v1 = v1 && i < j1;
-      v2 = v2 && i + 1 < j0;
-      v3 = v3 && i + 1 < j1;
+      va0 = va0 && i < j0;
+      va1 = va1 && i < j1;
+      vb0 = vb0 && i + 1 < j0;
+      vb1 = vb1 && i + 1 < j1;
+      vc0 = vc0 && i + 2 < j0;
+      vc1 = vc1 && i + 2 < j1;
+      vd0 = vd0 && i + 3 < j0;
+      vd1 = vd1 && i + 3 < j1;
     }
-    uint32_t nm = 0;  // this step's near pairs (bit k: row i + k / 2, J atom lane + 32 (k & 1))
+    // near pairs of the row pairs (i, i + 1) and (i + 2, i + 3): bit k is row + k / 2, J atom lane + 32 (k & 1)
+    uint32_t nmA = 0, nmB = 0;
     if (CENTRED) {
-      XNS_CENTRED(ra, xj0, yj0, zj0, qj0, v0, 0)
-      XNS_CENTRED(ra, xj1, yj1, zj1, qj1, v1, 1)
-      XNS_CENTRED(rb, xj0, yj0, zj0, qj0, v2, 2)
-      XNS_CENTRED(rb, xj1, yj1, zj1, qj1, v3, 3)
+      using xns_f2::pack;
+      const xns_f2::f2 XA = pack(pa.x, pa.y), YA = pack(pa.z, pa.w), ZA = pack(pb.x, pb.y), WA = pack(pb.z, pb.w);
+      const xns_f2::f2 XB = pack(pc.x, pc.y), YB = pack(pc.z, pc.w), ZB = pack(pd.x, pd.y), WB = pack(pd.z, pd.w);
+      XNS_CENTRED2(XA, YA, ZA, WA, XJ0, YJ0, ZJ0, QJ0, va0, vb0, 0, 2, nmA)
+      XNS_CENTRED2(XA, YA, ZA, WA, XJ1, YJ1, ZJ1, QJ1, va1, vb1, 1, 3, nmA)
+      XNS_CENTRED2(XB, YB, ZB, WB, XJ0, YJ0, ZJ0, QJ0, vc0, vd0, 0, 2, nmB)
+      XNS_CENTRED2(XB, YB, ZB, WB, XJ1, YJ1, ZJ1, QJ1, vc1, vd1, 1, 3, nmB)
     } else {
-      XNS_DIRECT(ra, xj0, yj0, zj0, v0, 0)
-      XNS_DIRECT(ra, xj1, yj1, zj1, v1, 1)
-      XNS_DIRECT(rb, xj0, yj0, zj0, v2, 2)
-      XNS_DIRECT(rb, xj1, yj1, zj1, v3, 3)
+      const float4 ra = make_float4(pa.x, pa.z, pb.x, pb.z), rb = make_float4(pa.y, pa.w, pb.y, pb.w);
+      const float4 rc = make_float4(pc.x, pc.z, pd.x, pd.z), rd = make_float4(pc.y, pc.w, pd.y, pd.w);
+      XNS_DIRECT(ra, xj0, yj0, zj0, va0, 0, nmA)
+      XNS_DIRECT(ra, xj1, yj1, zj1, va1, 1, nmA)
+      XNS_DIRECT(rb, xj0, yj0, zj0, vb0, 2, nmA)
+      XNS_DIRECT(rb, xj1, yj1, zj1, vb1, 3, nmA)
+      XNS_DIRECT(rc, xj0, yj0, zj0, vc0, 0, nmB)
+      XNS_DIRECT(rc, xj1, yj1, zj1, vc1, 1, nmB)
+      XNS_DIRECT(rd, xj0, yj0, zj0, vd0, 2, nmB)
+      XNS_DIRECT(rd, xj1, yj1, zj1, vd1, 3, nmB)
     }
-    // lanes with near pairs append one entry each, in lane order
-    const unsigned nb = __ballot_sync(0xffffffffu, nm != 0);
-    if (nm) queue[(qn + __popc(nb & below)) & (QUEUE - 1)] = (uint16_t)(((i >> 1) << 9) | (lane << 4) | nm);
-    qn += __popc(nb);
-    // fewer than 32 entries wait here and a step adds at most 32: the queue never holds more than 63
-    while (qn - qd >= 32) drain(32);
+    XNS_PUSH(nmA, i)
+    XNS_PUSH(nmB, i + 2)
   }
-#undef XNS_CENTRED
+#undef XNS_PUSH
+#undef XNS_CENTRED2
 #undef XNS_DIRECT
 #undef XNS_COUNT
   if (qn != qd) drain(qn - qd);
