@@ -538,23 +538,26 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
       zj1 = (float)bz1 - dl[2];
     }
   }
-  // centred: the J atoms' values and the tile pair's constants as packed pairs (both halves equal)
-  xns_f2::f2 XJ0 = 0, YJ0 = 0, ZJ0 = 0, QJ0 = 0, XJ1 = 0, YJ1 = 0, ZJ1 = 0, QJ1 = 0;
-  xns_f2::f2 R0SQ2 = 0, R0F2 = 0, R0FR2 = 0, MAGIC2 = 0, NK1_2 = 0, MC2 = 0;
+  // the J atoms' values and the tile pair's constants as packed pairs (both halves equal)
+  using xns_f2::splat;
+  const xns_f2::f2 XJ0 = splat(xj0), YJ0 = splat(yj0), ZJ0 = splat(zj0), XJ1 = splat(xj1), YJ1 = splat(yj1),
+                   ZJ1 = splat(zj1), MAGIC2 = splat(MAGIC);
+  xns_f2::f2 QJ0 = 0, QJ1 = 0, R0SQ2 = 0, R0F2 = 0, R0FR2 = 0, NK1_2 = 0, MC2 = 0;
+  xns_f2::f2 DH0 = 0, DH1 = 0, DH2 = 0, MR2 = 0, M02 = 0;
+  const xns_f2::f2 HALF2 = splat(0.5f), SIGN2 = 0x8000000080000000ull;  // SIGN2: flips both signs
+  if (!CENTRED) {
+    DH0 = splat(dh[0]);
+    DH1 = splat(dh[1]);
+    DH2 = splat(dh[2]);
+    MR2 = splat(mr);
+    M02 = splat(m0);
+  }
   if (CENTRED) {
-    using xns_f2::splat;
-    XJ0 = splat(xj0);
-    YJ0 = splat(yj0);
-    ZJ0 = splat(zj0);
     QJ0 = splat(qj0);
-    XJ1 = splat(xj1);
-    YJ1 = splat(yj1);
-    ZJ1 = splat(zj1);
     QJ1 = splat(qj1);
     R0SQ2 = splat(cc.R0sq);
     R0F2 = splat(cc.R0f);
     R0FR2 = splat(cc.R0fr);
-    MAGIC2 = splat(MAGIC);
     NK1_2 = splat(-cc.K1);
     MC2 = splat(cc.mc);
   }
@@ -606,21 +609,28 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
     }                                                                                       \
     NM |= ((VALID) && !fast) ? (1u << (K)) : 0u;                                            \
   }
-#define XNS_DIRECT(RA, XJ, YJ, ZJ, VALID, K, NM)                                            \
+// The direct estimate for two pairs at once (rows i, i + 1 against one J atom), packed: per half, the
+// scalar operations dx = dh + (x_i - x_j) (each axis), d2 by FMAs, r0 = d2 rsqrt(d2), one Newton
+// step, the magic-number rounding, in that order.
+#define XNS_DIRECT2(RX, RY, RZ, XJ, YJ, ZJ, VLO, VHI, KLO, KHI, NM)                          \
   {                                                                                         \
-    const float dx = dh[0] + (RA.x - XJ), dy = dh[1] + (RA.y - YJ), dz = dh[2] + (RA.z - ZJ); \
-    const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));                                   \
-    float y;                                                                                \
-    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(d2));                                \
-    const float r0 = d2 * y; /* NaN for d2 == 0: not fast */                                \
-    const float r = fmaf(fmaf(-r0, r0, d2), 0.5f * y, r0); /* one Newton step */            \
-    const float t = r + MAGIC;                                                              \
-    const float d = r - (t - MAGIC);                                                        \
-    const uint32_t slot = (uint32_t)(__float_as_int(t) - tbase) - (d < 0.f ? 1u : 0u);      \
-    XNS_COUNT(fabsf(d) >= fmaf(r, mr, m0), slot, VALID, K, NM)                              \
+    using namespace xns_f2;                                                                 \
+    const f2 dx = add(DH0, sub(RX, XJ)), dy = add(DH1, sub(RY, YJ)), dz = add(DH2, sub(RZ, ZJ)); \
+    const f2 d2 = xns_f2::fma(dx, dx, xns_f2::fma(dy, dy, mul(dz, dz)));                    \
+    float y0, y1;                                                                           \
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y0) : "f"(lo(d2)));                           \
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y1) : "f"(hi(d2)));                           \
+    const f2 y = pack(y0, y1);                                                              \
+    const f2 r0 = mul(d2, y); /* NaN for d2 == 0: not fast */                               \
+    const f2 r = xns_f2::fma(xns_f2::fma(r0 ^ SIGN2, r0, d2), mul(HALF2, y), r0);           \
+    const f2 t = add(r, MAGIC2);                                                            \
+    const f2 d = sub(r, sub(t, MAGIC2));                                                    \
+    const f2 m = xns_f2::fma(r, MR2, M02);                                                  \
+    const uint32_t slo = (uint32_t)(__float_as_int(lo(t)) - tbase) - (lo(d) < 0.f ? 1u : 0u); \
+    const uint32_t shi = (uint32_t)(__float_as_int(hi(t)) - tbase) - (hi(d) < 0.f ? 1u : 0u); \
+    XNS_COUNT(fabsf(lo(d)) >= lo(m), slo, VLO, KLO, NM)                                     \
+    XNS_COUNT(fabsf(hi(d)) >= hi(m), shi, VHI, KHI, NM)                                     \
   }
-// Two pairs at once (rows i, i + 1 against one J atom) on packed f32x2 pairs: the scalar operations
-// in the same order, so the same roundings and the same bound, in half the instructions.
 #define XNS_CENTRED2(RX, RY, RZ, RW, XJ, YJ, ZJ, QJ, VLO, VHI, KLO, KHI, NM)                \
   {                                                                                         \
     using namespace xns_f2;                                                                 \
@@ -677,23 +687,20 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
       XNS_CENTRED2(XB, YB, ZB, WB, XJ0, YJ0, ZJ0, QJ0, vc0, vd0, 0, 2, nmB)
       XNS_CENTRED2(XB, YB, ZB, WB, XJ1, YJ1, ZJ1, QJ1, vc1, vd1, 1, 3, nmB)
     } else {
-      const float4 ra = make_float4(pa.x, pa.z, pb.x, pb.z), rb = make_float4(pa.y, pa.w, pb.y, pb.w);
-      const float4 rc = make_float4(pc.x, pc.z, pd.x, pd.z), rd = make_float4(pc.y, pc.w, pd.y, pd.w);
-      XNS_DIRECT(ra, xj0, yj0, zj0, va0, 0, nmA)
-      XNS_DIRECT(ra, xj1, yj1, zj1, va1, 1, nmA)
-      XNS_DIRECT(rb, xj0, yj0, zj0, vb0, 2, nmA)
-      XNS_DIRECT(rb, xj1, yj1, zj1, vb1, 3, nmA)
-      XNS_DIRECT(rc, xj0, yj0, zj0, vc0, 0, nmB)
-      XNS_DIRECT(rc, xj1, yj1, zj1, vc1, 1, nmB)
-      XNS_DIRECT(rd, xj0, yj0, zj0, vd0, 2, nmB)
-      XNS_DIRECT(rd, xj1, yj1, zj1, vd1, 3, nmB)
+      using xns_f2::pack;
+      const xns_f2::f2 XA = pack(pa.x, pa.y), YA = pack(pa.z, pa.w), ZA = pack(pb.x, pb.y);
+      const xns_f2::f2 XB = pack(pc.x, pc.y), YB = pack(pc.z, pc.w), ZB = pack(pd.x, pd.y);
+      XNS_DIRECT2(XA, YA, ZA, XJ0, YJ0, ZJ0, va0, vb0, 0, 2, nmA)
+      XNS_DIRECT2(XA, YA, ZA, XJ1, YJ1, ZJ1, va1, vb1, 1, 3, nmA)
+      XNS_DIRECT2(XB, YB, ZB, XJ0, YJ0, ZJ0, vc0, vd0, 0, 2, nmB)
+      XNS_DIRECT2(XB, YB, ZB, XJ1, YJ1, ZJ1, vc1, vd1, 1, 3, nmB)
     }
     XNS_PUSH(nmA, i)
     XNS_PUSH(nmB, i + 2)
   }
 #undef XNS_PUSH
 #undef XNS_CENTRED2
-#undef XNS_DIRECT
+#undef XNS_DIRECT2
 #undef XNS_COUNT
   if (qn != qd) drain(qn - qd);
   return bad;
