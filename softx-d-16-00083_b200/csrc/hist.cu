@@ -597,13 +597,14 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
     }
     qd += n;
   };
-  // FAST: the estimate's bin is certain and its slot is below Wl; a lane without a fast pair adds 0 to
-  // its own spare slot (branch-free), near pairs set their bit K of the step's mask.
+  // FAST: the estimate's bin is certain and its slot is below Wl; a lane without a fast pair adds 1 to
+  // its own spare slot instead (branch-free; the 32 spare slots are never flushed or read), near pairs
+  // set their bit K of the step's mask.
 #define XNS_COUNT(FAST, SLOT, VALID, K, NM)                                                 \
   {                                                                                         \
     const bool fast = (VALID) && (FAST) && (SLOT) < Wl;                                     \
     if (WINDOW) {                                                                           \
-      atomicAdd(win + (fast ? (SLOT) : W + lane), fast ? 1u : 0u);                          \
+      atomicAdd(win + (fast ? (SLOT) : W + lane), 1u);                                      \
     } else if (fast) {                                                                      \
       atomicAdd(h + (SLOT), 1ull);                                                          \
     }                                                                                       \
