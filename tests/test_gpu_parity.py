@@ -58,6 +58,16 @@ def test_hist_edge_cases(gpu_ctx, oracle):
     assert np.array_equal(gpu_ctx.calc_hist(els, nh, 0.003), oracle.hist(els, nh, 0.003))
 
 
+@pytest.mark.parametrize("a,bin", [(5.0, 0.001), (4.0, 0.0025), (5.64, 0.001)])
+def test_hist_perfect_lattice(gpu_ctx, oracle, a, bin):
+    """An undisplaced crystal: lattice distances a sqrt(n) / 2 fall on bin edges or within rounding of
+    them for many shells (a = 5 A and 4 A make r / bin an integer in exact arithmetic), so the FP32
+    estimates send whole shells to the exact path and its correctly rounded branch decides them."""
+    els = synth.rocksalt_cube(cells=12, a=a, vacancy=0.0, sigma=0.0)
+    nh = synth.hist_size(els, bin)
+    assert np.array_equal(gpu_ctx.calc_hist(els, nh, bin), oracle.hist(els, nh, bin))
+
+
 def test_hist_out_of_range_is_an_error(gpu_ctx):
     import xns_b200
     els = [np.array([[0, 0, 0], [1.0, 0, 0]])]
