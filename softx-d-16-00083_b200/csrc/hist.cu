@@ -4,25 +4,28 @@
 // Counts are bit-identical to the reference's.  At the reference's 0.001 A bins a 2e5-atom structure
 // has ~3e5 bins per element pair: far more than a shared-memory histogram holds, and one global atomic
 // per pair leaves the kernel bound by L2 atomics.  So the pairs are ordered by distance first:
-//   1. atoms of each element are counting-sorted into cubic cells of ~CELL_TARGET atoms
-//      (cell_count / scan / cell_scatter kernels); each cell is cut into tiles of <= 64 atoms with a
-//      bounding box (tile_build / tile_bbox);
+//   1. atoms of each element are counting-sorted into cells of ~cell_target atoms, on the one of six
+//      candidate grids whose tiles waste the fewest warp lanes (cand_count / cand_slots, then
+//      cell_count / scan / cell_scatter); each cell is cut into tiles of <= 64 atoms with a bounding
+//      box (tile_build / tile_bbox);
 //   2. every tile pair (upper triangle within an element, all pairs across elements of the same
 //      structure) gets the bin range [kmin, kmax] its bounding boxes allow, and is counting-sorted by
 //      (class, kmin / BUCKET), a class being one element pair of one structure (pair_key / scan /
 //      pair_scatter);
 //   3. the sorted list is cut into runs of one class; hist_window_kernel is persistent (one CTA per
 //      SM) and takes runs from a work queue, largest first, one tile pair per warp, counting into a
-//      WIN-bin u32 window of shared memory that slides up the distance axis (bins that leave the
+//      window of u32 bins in shared memory that slides up the distance axis (bins that leave the
 //      window are added to the u64 global histogram once per run);
 //   4. hist_wide_kernel: tile pairs whose range is wider than the window (sparse elements) count
 //      straight into the global histogram.
 //
-// Bin decision, per pair: an FP32 estimate of r/bin from tile-local offsets, with a proven error bound
-// (count_tile_pair_t); pairs whose estimate lies within that bound of a bin edge (about 9 % at 0.001 A
-// bins and 1e5-bin distances), or near the last bin, are queued per warp and binned exactly, 32 at a
-// time, with FP64 in the reference's operation order (hist_bin.cuh).  Atom order inside a cell and list order
-// inside a bucket come from atomics, but counts do not depend on either.
+// Bin decision, per pair: an FP32 estimate of r/bin with a proven error bound (count_tile_pair_t: a
+// centred estimate for tile pairs far apart, whose error scales with the tile size; a direct one
+// otherwise), computed for two pairs at a time on packed f32x2 pairs.  Pairs whose estimate lies
+// within the bound of a bin edge (about 1.5 % of the benchmark's), near the last bin or outside the
+// window are queued per warp and binned exactly, 32 at a time, with FP64 in the reference's operation
+// order (hist_bin.cuh).  Atom order inside a cell and list order inside a bucket come from atomics,
+// but counts do not depend on either.
 #include <math.h>
 #include <string.h>
 
