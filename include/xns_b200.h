@@ -256,6 +256,50 @@ int xns_binning_features(xns_ctx *ctx, const double *h, uint32_t nh, float *X);
 int xns_binning_correction(xns_ctx *ctx, const double *h, const float *mu, uint32_t nh, double bin, const double *q,
                            uint32_t nq, double s0, double *dI);
 
+/* ---- structure builder ------------------------------------------------------------------------------ */
+
+/* One block of the structure, as block::calcAtoms (CalcFunctions.cpp:251-392) reads it after the XML
+ * reader prepared it (ReadXML.cpp:254-303: redefAtoms / redefSymm to Cartesian, centerAtoms, sortAtoms,
+ * calcMean, calcRotMatrix of each copy).  Arrays are borrowed for the duration of the call. */
+typedef struct xns_block {
+  uint32_t natom;          /* sites of the asymmetric unit (block::Natom), element-sorted */
+  uint32_t nid;            /* elements present in the block (block::Nid) */
+  uint32_t nsymm;          /* symmetry operations (block::Nsymm, >= 1) */
+  uint32_t ncopy;          /* copies (block::Ncopy, >= 1) */
+  uint32_t ncell[3];       /* unit cells along e[0], e[1], e[2] (block::Ncell) */
+  int32_t cutoff;          /* block::cutoff, radius rcut about r_mean */
+  int32_t cutoff_copies;   /* block::cutoffcopies, radius rcut_copies about the mean copy position */
+  int32_t ro_mol;          /* block::ro_mol: a random rotation per symmetry-equivalent molecule */
+  const uint32_t *natom_el; /* [nid] sites of each element, in order (block::NatomEl) */
+  const uint32_t *id;       /* [nid] global element index of each (block::id) */
+  const double *r_atom;     /* [natom][3] site coordinates, Cartesian (block::rAtom) */
+  const double *occ;        /* [natom] occupancies (block::occ) */
+  const double *dev;        /* [natom] displacement widths (block::dev) */
+  const double *p_symm;     /* [nsymm][3][3] rotation part, row k of operation s at [s][k] (block::pSymm[k][s]) */
+  const double *r_symm;     /* [nsymm][3] translation part, Cartesian (block::rSymm) */
+  const double *r_copy;     /* [ncopy][3] copy positions (block::rCopy) */
+  const double *cf;         /* [ncopy][3][3] copy rotations, row k of copy c at [c][k] (block::cf[k][c]) */
+  double e[3][3];           /* cell vectors (block::e) */
+  double r_mean[3];         /* block::rMean */
+  double rcut, rcut_copies, dev_mol;
+} xns_block;
+
+/* block::calcAtoms for each block in turn on the GPU.  The atoms of every block are appended, element
+ * by element, in the reference's order (copy, cell x, y, z, site), and the result is kept in the
+ * context as one device array of sum(n_el) x y z double triples, element-major (the xyz_dev layout of
+ * xns_pdf_and_debye_device); *xyz_dev points at it until the next build or xns_destroy.
+ *   n_el[nel]: atoms of each global element;  n_all (optional): atoms of each block element, blocks
+ *   in order (block::NatomElAll, sum of nid entries).
+ * Sites closer than 0.5 A (also across the +-2 neighbouring cells of every replicated axis) are merged
+ * and filled by one random draw against their cumulative occupancy, as the reference does; the
+ * random numbers come from Philox4x32-10 keyed by seed and indexed by (block, copy and cell, site,
+ * purpose), so a build is reproducible for a seed (the reference seeds from the clock).
+ * Sites per block below 2^31, atoms in all below 2^32 - 1, nel <= 64. */
+int xns_build_atoms(xns_ctx *ctx, const xns_block *blocks, uint32_t nblocks, uint32_t nel, uint64_t seed,
+                    uint32_t *n_el, uint32_t *n_all, const double **xyz_dev);
+/* Copies the last build's atoms into host arrays: xyz_el[e] receives n_el[e] x y z triples. */
+int xns_copy_atoms(xns_ctx *ctx, double *const *xyz_el);
+
 /* ---- utilities (no reference counterpart) -------------------------------------------------------- */
 
 /* Measured FMA-pipe throughput of this device in TFLOP/s (an FMA counts 2 flops): FP64 when fp64 != 0,

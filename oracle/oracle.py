@@ -41,6 +41,47 @@ def _f64(a):
     return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
 
 
+class _BlockStruct(C.Structure):
+    """xo_block / the harness's xr_block: the same layout as the library's xns_block."""
+    _fields_ = [("natom", _u32), ("nid", _u32), ("nsymm", _u32), ("ncopy", _u32), ("ncell", _u32 * 3),
+                ("cutoff", C.c_int32), ("cutoff_copies", C.c_int32), ("ro_mol", C.c_int32),
+                ("natom_el", _p), ("id", _p), ("r_atom", _p), ("occ", _p), ("dev", _p), ("p_symm", _p),
+                ("r_symm", _p), ("r_copy", _p), ("cf", _p),
+                ("e", _dbl * 9), ("r_mean", _dbl * 3), ("rcut", _dbl), ("rcut_copies", _dbl), ("dev_mol", _dbl)]
+
+
+def _blocks(blocks):
+    """C array of block descriptions from objects with the attributes of xns_b200.structure.Block."""
+    arr = (_BlockStruct * max(1, len(blocks)))()
+    keep = []
+    for i, b in enumerate(blocks):
+        s = arr[i]
+        a = [np.ascontiguousarray(b.natom_el, dtype=np.uint32), np.ascontiguousarray(b.id, dtype=np.uint32)] + [
+            np.ascontiguousarray(x, dtype=np.float64) for x in (b.r_atom, b.occ, b.dev, b.p_symm, b.r_symm, b.r_copy, b.cf)]
+        keep.append(a)
+        s.natom, s.nid, s.nsymm, s.ncopy = len(a[2]), len(a[1]), len(a[5]), len(a[7])
+        s.ncell[:] = [int(c) for c in b.ncell]
+        s.cutoff, s.cutoff_copies, s.ro_mol = int(b.rcut is not None), int(b.rcut_copies is not None), int(b.ro_mol)
+        s.natom_el, s.id, s.r_atom, s.occ, s.dev, s.p_symm, s.r_symm, s.r_copy, s.cf = [x.ctypes.data_as(_p) for x in a]
+        s.e[:] = [float(v) for v in np.asarray(b.e, dtype=np.float64).ravel()]
+        s.r_mean[:] = [float(v) for v in b.r_mean]
+        s.rcut = 0.0 if b.rcut is None else float(b.rcut)
+        s.rcut_copies = 0.0 if b.rcut_copies is None else float(b.rcut_copies)
+        s.dev_mol = float(b.dev_mol)
+    return arr, keep
+
+
+def _split(ptr, n_el, free):
+    tot = int(np.sum(n_el))
+    flat = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(_dbl)), shape=(max(tot, 1) * 3,))[:tot * 3].copy()
+    free(ptr)
+    out, o = [], 0
+    for n in n_el:
+        out.append(flat[3 * o:3 * (o + int(n))].reshape(-1, 3))
+        o += int(n)
+    return out
+
+
 class Oracle:
     def __init__(self, path=ORACLE_SO):
         if not os.path.exists(path):
@@ -57,7 +98,25 @@ class Oracle:
         L.xo_int_1d_hist.argtypes = [_p, _p, _u32, _u32, _dbl, _p, _u32, _int, _p, _p, _int, _dbl, _p]
         L.xo_pdf.argtypes = [_p, _p, _u32, _u32, _dbl, _int, _dbl, _p, _p]
         L.xo_int_2d.argtypes = [_p, _p, _u32, _p, _u32, _u32, _p, _p, _p, _u32, _dbl, _int, _p, _p, _int, _p, _p]
+        L.xo_build_atoms.argtypes = [_p, _u32, _u32, C.c_uint64, _p, _p]
+        L.xo_build_atoms.restype = _p
+        L.xo_free.argtypes = [_p]
+        L.xo_philox.argtypes = [_p, _p, _p]
         L.xo_amp_plane.argtypes = [_p, _p, _u32, _dbl, _dbl, _u32, _dbl, _dbl, _u32, _int, _p, _p, _p]
+
+    def philox(self, ctr, key):
+        c, k, o = np.array(ctr, dtype=np.uint32), np.array(key, dtype=np.uint32), np.zeros(4, dtype=np.uint32)
+        self.lib.xo_philox(_ptr(c), _ptr(k), _ptr(o))
+        return o
+
+    def build_atoms(self, blocks, nel, seed=0):
+        """(list of per-element (n, 3) arrays, n_all) from xo_build_atoms."""
+        arr, keep = _blocks(blocks)
+        n_el = np.zeros(nel, dtype=np.uint32)
+        n_all = np.zeros(max(1, sum(len(b.id) for b in blocks)), dtype=np.uint32)
+        ptr = self.lib.xo_build_atoms(C.cast(arr, _p), len(blocks), nel, seed, _ptr(n_el), _ptr(n_all))
+        del keep
+        return _split(ptr, n_el, self.lib.xo_free), n_all[:sum(len(b.id) for b in blocks)]
 
     def rot_matrix(self, euler, convention):
         e = _f64(euler)
@@ -144,6 +203,9 @@ class Reference:
         self.threads = threads or os.cpu_count() or 1
         L = self.lib = C.CDLL(path)
         L.xnsref_rot_matrix.argtypes = [_p, _u32, _p]
+        L.xnsref_calc_atoms.argtypes = [_p, _u32, _u32, _p, _p]
+        L.xnsref_calc_atoms.restype = _p
+        L.xnsref_free.argtypes = [_p]
         L.xnsref_hist_size.argtypes = [_p, _p, _u32, _dbl]
         L.xnsref_hist_size.restype = _u32
         L.xnsref_atomic_density.argtypes = [_p, _p, _u32]
@@ -156,6 +218,15 @@ class Reference:
                                                 _dbl, _int, _p, _p]
         L.xnsref_calc_int_2d.argtypes = [_p, _p, _u32, _p, _u32, _u32, _p, _p, _p, _u32, _dbl, _int, _p, _p, _int, _int,
                                          _p, _p]
+
+    def calc_atoms(self, blocks, nel):
+        """(list of per-element (n, 3) arrays, n_all) from the reference's own block::calcAtoms."""
+        arr, keep = _blocks(blocks)
+        n_el = np.zeros(nel, dtype=np.uint32)
+        n_all = np.zeros(max(1, sum(len(b.id) for b in blocks)), dtype=np.uint32)
+        ptr = self.lib.xnsref_calc_atoms(C.cast(arr, _p), len(blocks), nel, _ptr(n_el), _ptr(n_all))
+        del keep
+        return _split(ptr, n_el, self.lib.xnsref_free), n_all[:sum(len(b.id) for b in blocks)]
 
     def rot_matrix(self, euler, convention):
         e = _f64(euler)

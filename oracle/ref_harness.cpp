@@ -259,4 +259,82 @@ int xnsref_calc_int_2d(const double *xyz, const uint32_t *n_el, uint32_t nel, co
   return 0;
 }
 
+// block::calcAtoms, CalcFunctions.cpp:251-392, for each block in turn (as CalcAndPrintAtoms does,
+// :397).  The blocks arrive as the library's xns_block (the same layout is declared here) and are
+// copied into the reference's own block objects.  Returns a malloc'd element-major x y z array (free
+// with xnsref_free); n_el[nel] atoms per element; n_all (optional) the blocks' NatomElAll.  The
+// reference seeds its generator from the clock, so only draw-free inputs repeat.
+struct xr_block {
+  uint32_t natom, nid, nsymm, ncopy;
+  uint32_t ncell[3];
+  int32_t cutoff, cutoff_copies, ro_mol;
+  const uint32_t *natom_el, *id;
+  const double *r_atom, *occ, *dev, *p_symm, *r_symm, *r_copy, *cf;
+  double e[3][3];
+  double r_mean[3];
+  double rcut, rcut_copies, dev_mol;
+};
+
+void xnsref_free(void *p) { free(p); }
+
+double *xnsref_calc_atoms(const xr_block *blocks, uint32_t nblocks, uint32_t nel, uint32_t *n_el, uint32_t *n_all) {
+  vector<vect3d<double> > *ra = new vector<vect3d<double> >[nel];
+  uint32_t o_all = 0;
+  for (uint32_t ib = 0; ib < nblocks; ib++) {
+    const xr_block &x = blocks[ib];
+    block b;
+    b.Natom = x.natom;
+    b.Nsymm = x.nsymm;
+    b.Ncopy = x.ncopy;
+    b.create();
+    b.Nid = x.nid;
+    b.id = new unsigned int[x.nid];
+    for (uint32_t k = 0; k < x.nid; k++) {
+      b.id[k] = x.id[k];
+      b.NatomEl.push_back(x.natom_el[k]);
+    }
+    b.NatomElAll.resize(x.nid);
+    for (uint32_t i = 0; i < x.natom; i++) {
+      b.rAtom[i].assign(x.r_atom[3 * i], x.r_atom[3 * i + 1], x.r_atom[3 * i + 2]);
+      b.occ[i] = x.occ[i];
+      b.dev[i] = x.dev[i];
+    }
+    for (uint32_t s = 0; s < x.nsymm; s++) {
+      for (int k = 0; k < 3; k++) b.pSymm[k][s].assign(x.p_symm[9 * s + 3 * k], x.p_symm[9 * s + 3 * k + 1], x.p_symm[9 * s + 3 * k + 2]);
+      b.rSymm[s].assign(x.r_symm[3 * s], x.r_symm[3 * s + 1], x.r_symm[3 * s + 2]);
+    }
+    for (uint32_t c = 0; c < x.ncopy; c++) {
+      for (int k = 0; k < 3; k++) b.cf[k][c].assign(x.cf[9 * c + 3 * k], x.cf[9 * c + 3 * k + 1], x.cf[9 * c + 3 * k + 2]);
+      b.rCopy[c].assign(x.r_copy[3 * c], x.r_copy[3 * c + 1], x.r_copy[3 * c + 2]);
+    }
+    for (int k = 0; k < 3; k++) b.e[k].assign(x.e[k][0], x.e[k][1], x.e[k][2]);
+    b.Ncell.assign(x.ncell[0], x.ncell[1], x.ncell[2]);
+    b.rMean.assign(x.r_mean[0], x.r_mean[1], x.r_mean[2]);
+    b.cutoff = x.cutoff != 0;
+    b.Rcut = x.rcut;
+    b.cutoffcopies = x.cutoff_copies != 0;
+    b.RcutCopies = x.rcut_copies;
+    b.dev_mol = x.dev_mol;
+    b.ro_mol = x.ro_mol != 0;
+    if (x.natom) b.calcAtoms(ra);
+    for (uint32_t k = 0; k < x.nid; k++)
+      if (n_all) n_all[o_all + k] = x.natom ? b.NatomElAll[k] : 0;
+    o_all += x.nid;
+  }
+  size_t tot = 0;
+  for (uint32_t e = 0; e < nel; e++) tot += ra[e].size();
+  double *xyz = (double *)malloc(24 * (tot ? tot : 1));
+  size_t o = 0;
+  for (uint32_t e = 0; e < nel; e++) {
+    n_el[e] = (uint32_t)ra[e].size();
+    for (size_t i = 0; i < ra[e].size(); i++, o++) {
+      xyz[3 * o] = ra[e][i].x;
+      xyz[3 * o + 1] = ra[e][i].y;
+      xyz[3 * o + 2] = ra[e][i].z;
+    }
+  }
+  delete[] ra;
+  return xyz;
+}
+
 }  // extern "C"

@@ -427,3 +427,219 @@ void xo_amp_plane(const double *xyz, const uint32_t *n_el, uint32_t nel, double 
     }
   }
 }
+
+/* ---- structure builder ------------------------------------------------------------------------ */
+
+void xo_free(void *p) { free(p); }
+
+void xo_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+  uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3], k0 = key[0], k1 = key[1];
+  for (int r = 0; r < 10; r++) {
+    if (r) {
+      k0 += 0x9E3779B9u;
+      k1 += 0xBB67AE85u;
+    }
+    uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+    uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0, n1 = (uint32_t)p1, n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1,
+             n3 = (uint32_t)p0;
+    c0 = n0, c1 = n1, c2 = n2, c3 = n3;
+  }
+  out[0] = c0, out[1] = c1, out[2] = c2, out[3] = c3;
+}
+
+enum { XO_P_OCC = 0, XO_P_DISP_ANG = 1, XO_P_DISP_RAD = 2, XO_P_MOL_ANG = 3, XO_P_MOL_RAD = 4, XO_P_ROT_A = 5,
+       XO_P_ROT_B = 6 };
+
+typedef struct {
+  uint32_t key[2], blk;
+} xo_rng;
+
+static void rng_draw(const xo_rng *g, uint32_t item, uint64_t unit, uint32_t purpose, double *u0, double *u1) {
+  uint32_t c[4] = {item, (uint32_t)unit, (uint32_t)(unit >> 32), (g->blk << 8) | purpose}, r[4];
+  xo_philox(c, g->key, r);
+  *u0 = (double)(((uint64_t)r[0] << 21) | (r[1] >> 11)) * 0x1.0p-53;
+  *u1 = (double)(((uint64_t)r[2] << 21) | (r[3] >> 11)) * 0x1.0p-53;
+}
+
+/* CalcFunctions.cpp:335-340 and :366-370: direction phi = 2 pi U, theta = pi U (as the reference draws
+ * it), radius |N(0, dev)|; the normal deviate by Box-Muller from two uniforms */
+static void rng_displacement(const xo_rng *g, uint32_t item, uint64_t unit, uint32_t p_ang, uint32_t p_rad, double dev,
+                             double d[3]) {
+  double uf, ut, ua, ub;
+  rng_draw(g, item, unit, p_ang, &uf, &ut);
+  rng_draw(g, item, unit, p_rad, &ua, &ub);
+  double fi = 2.0 * XO_PI * uf, theta = XO_PI * ut;
+  double n = sqrt(-2.0 * log(1.0 - ua)) * cos(2.0 * XO_PI * ub);
+  double R = fabs(dev * n);
+  d[0] = R * sin(theta) * cos(fi);
+  d[1] = R * sin(theta) * sin(fi);
+  d[2] = R * cos(theta);
+}
+
+static double dot3(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+typedef struct {
+  double *xyz;
+  size_t n, cap;
+} xo_list;
+
+static void list_push(xo_list *l, const double r[3]) {
+  if (l->n == l->cap) {
+    l->cap = l->cap ? 2 * l->cap : 1024;
+    l->xyz = (double *)realloc(l->xyz, 3 * l->cap * sizeof(double));
+  }
+  memcpy(l->xyz + 3 * l->n, r, 3 * sizeof(double));
+  l->n++;
+}
+
+/* one block, appending to the per-element lists (CalcFunctions.cpp:251-392) */
+static void build_block(const xo_block *b, uint32_t blk, uint64_t seed, xo_list *out, uint32_t *n_all) {
+  const uint32_t S = b->natom * b->nsymm;
+  xo_rng g = {{(uint32_t)seed, (uint32_t)(seed >> 32)}, blk};
+  double *ra0 = (double *)malloc(3 * (size_t)S * sizeof(double)), *cell = (double *)malloc(3 * (size_t)S * sizeof(double));
+  uint32_t *type = (uint32_t *)malloc((size_t)S * sizeof(uint32_t));
+  /* :268-274, site order iAtom * Nsymm + iSymm */
+  for (uint32_t ia = 0, it = 0, end = b->natom_el[0]; ia < b->natom; ia++) {
+    while (ia >= end) end += b->natom_el[++it];
+    for (uint32_t is = 0; is < b->nsymm; is++) {
+      const uint32_t s = ia * b->nsymm + is;
+      const double *p = b->p_symm + 9 * is, *r = b->r_atom + 3 * ia;
+      for (int k = 0; k < 3; k++) {
+        ra0[3 * s + k] = dot3(p + 3 * k, r);
+        cell[3 * s + k] = ra0[3 * s + k] + b->r_symm[3 * is + k];
+      }
+      type[s] = it;
+    }
+  }
+  /* :275-319: the list of each site -- itself, then every later site within 0.5 A under some cell
+   * translation, in site order (a site matched by several translations appears once: the repeats
+   * the reference appends carry the same element and occupancy and never change a choice) */
+  int st[3], fin[3];
+  for (int k = 0; k < 3; k++) {
+    st[k] = b->ncell[k] == 1 ? 0 : -2;
+    fin[k] = b->ncell[k] == 1 ? 1 : 3;
+  }
+  size_t *off = (size_t *)malloc(((size_t)S + 1) * sizeof(size_t)), cap = 2 * (size_t)S + 16, L = 0;
+  uint32_t *list = (uint32_t *)malloc(cap * sizeof(uint32_t));
+  double *cum = (double *)malloc(cap * sizeof(double));
+  for (uint32_t i = 0; i < S; i++) {
+    off[i] = L;
+    if (L + 1 > cap) cap *= 2, list = (uint32_t *)realloc(list, cap * 4), cum = (double *)realloc(cum, cap * 8);
+    list[L] = i;
+    cum[L] = b->occ[i / b->nsymm];
+    L++;
+    for (uint32_t j = i + 1; j < S; j++) {
+      int hit = 0;
+      for (int cx = st[0]; cx < fin[0] && !hit; cx++)
+        for (int cy = st[1]; cy < fin[1] && !hit; cy++)
+          for (int cz = st[2]; cz < fin[2] && !hit; cz++) {
+            double d[3];
+            for (int k = 0; k < 3; k++) {
+              double ct = b->e[0][k] * (double)cx + b->e[1][k] * (double)cy + b->e[2][k] * (double)cz;
+              d[k] = cell[3 * i + k] - cell[3 * j + k] + ct;
+            }
+            hit = d[0] * d[0] + d[1] * d[1] + d[2] * d[2] < 0.25;
+          }
+      if (!hit) continue;
+      if (L + 1 > cap) cap *= 2, list = (uint32_t *)realloc(list, cap * 4), cum = (double *)realloc(cum, cap * 8);
+      /* :305-306: add the occupancy only when the element differs from the previous entry's */
+      cum[L] = type[j] != type[list[L - 1]] ? cum[L - 1] + b->occ[j / b->nsymm] : cum[L - 1];
+      list[L] = j;
+      L++;
+    }
+  }
+  off[S] = L;
+  double rmc[3] = {0, 0, 0};
+  for (uint32_t c = 0; c < b->ncopy; c++)
+    for (int k = 0; k < 3; k++) rmc[k] += b->r_copy[3 * c + k];
+  for (int k = 0; k < 3; k++) rmc[k] /= (double)b->ncopy;
+  unsigned char *claimed = (unsigned char *)malloc(S ? S : 1);
+  for (uint32_t k = 0; k < b->nid; k++) n_all[k] = 0;
+  uint64_t unit = 0;
+  for (uint32_t c = 0; c < b->ncopy; c++)
+    for (uint32_t cx = 0; cx < b->ncell[0]; cx++)
+      for (uint32_t cy = 0; cy < b->ncell[1]; cy++)
+        for (uint32_t cz = 0; cz < b->ncell[2]; cz++, unit++) {
+          double ct[3];
+          for (int k = 0; k < 3; k++) ct[k] = b->e[0][k] * (double)cx + b->e[1][k] * (double)cy + b->e[2][k] * (double)cz;
+          memset(claimed, 0, S);
+          for (uint32_t i = 0; i < S; i++) {
+            if (claimed[i]) continue;
+            for (size_t m = off[i]; m < off[i + 1]; m++) claimed[list[m]] = 1;
+            double randval, unused;
+            rng_draw(&g, i, unit, XO_P_OCC, &randval, &unused);
+            size_t m = off[i];
+            while (m < off[i + 1] && !(randval <= cum[m])) m++;
+            if (m == off[i + 1]) continue;
+            const uint32_t s = list[m], ia = s / b->nsymm, is = s % b->nsymm;
+            double ra1[3] = {ra0[3 * s], ra0[3 * s + 1], ra0[3 * s + 2]};
+            if (b->ro_mol) { /* :341-347, :358 */
+              double u0, u1, u2, u3;
+              rng_draw(&g, is, unit, XO_P_ROT_A, &u0, &u1);
+              rng_draw(&g, is, unit, XO_P_ROT_B, &u2, &u3);
+              double ex = 2.0 * XO_PI * u0, ey = XO_PI * u1, ez = 2.0 * XO_PI * u2;
+              double cx_ = cos(ex), cy_ = cos(ey), cz_ = cos(ez), sx = sin(ex), sy = sin(ey), sz = sin(ez);
+              double r0[3] = {cx_ * cy_ - sx * sy * cz_, -cx_ * sy - sx * cz_ * cy_, sx * sz};
+              double r1[3] = {sx * cy_ + cx_ * sy * cz_, -sx * sy + cx_ * cy_ * cz_, -cx_ * sz};
+              double r2[3] = {sz * sy, sz * cy_, cz_};
+              double t[3] = {dot3(ra1, r0), dot3(ra1, r1), dot3(ra1, r2)};
+              memcpy(ra1, t, sizeof t);
+            }
+            double rmd[3] = {0, 0, 0};
+            if (b->dev_mol >= 1.e-7) rng_displacement(&g, is, unit, XO_P_MOL_ANG, XO_P_MOL_RAD, b->dev_mol, rmd);
+            for (int k = 0; k < 3; k++) ra1[k] += b->r_symm[3 * is + k] + ct[k] + rmd[k]; /* :360 */
+            double d[3];
+            for (int k = 0; k < 3; k++) d[k] = ra1[k] - b->r_mean[k];
+            if (b->cutoff && !(dot3(d, d) <= b->rcut * b->rcut)) continue; /* :361 */
+            const double *cf = b->cf + 9 * c;
+            double tr[3] = {dot3(d, cf), dot3(d, cf + 3), dot3(d, cf + 6)};
+            for (int k = 0; k < 3; k++) ra1[k] = b->r_copy[3 * c + k] + tr[k];
+            if (b->dev[ia] >= 1.e-7) { /* :364-371 */
+              double dd[3];
+              rng_displacement(&g, i, unit, XO_P_DISP_ANG, XO_P_DISP_RAD, b->dev[ia], dd);
+              for (int k = 0; k < 3; k++) ra1[k] += dd[k];
+            }
+            if (b->cutoff_copies) { /* :372 */
+              double e3[3];
+              for (int k = 0; k < 3; k++) e3[k] = ra1[k] - rmc[k];
+              if (!(dot3(e3, e3) <= b->rcut_copies * b->rcut_copies)) continue;
+            }
+            list_push(&out[b->id[type[s]]], ra1);
+            n_all[type[s]]++;
+          }
+        }
+  free(claimed);
+  free(off);
+  free(list);
+  free(cum);
+  free(ra0);
+  free(cell);
+  free(type);
+}
+
+double *xo_build_atoms(const xo_block *blocks, uint32_t nblocks, uint32_t nel, uint64_t seed, uint32_t *n_el,
+                       uint32_t *n_all) {
+  xo_list *out = (xo_list *)calloc(nel, sizeof(xo_list));
+  uint32_t o_all = 0;
+  for (uint32_t ib = 0; ib < nblocks; ib++) {
+    uint32_t tmp[64];
+    uint32_t *na = n_all ? n_all + o_all : tmp;
+    if (blocks[ib].natom)
+      build_block(&blocks[ib], ib, seed, out, na);
+    else
+      for (uint32_t k = 0; k < blocks[ib].nid; k++) na[k] = 0;
+    o_all += blocks[ib].nid;
+  }
+  size_t tot = 0;
+  for (uint32_t e = 0; e < nel; e++) tot += out[e].n;
+  double *xyz = (double *)malloc(3 * (tot ? tot : 1) * sizeof(double));
+  size_t o = 0;
+  for (uint32_t e = 0; e < nel; e++) {
+    n_el[e] = (uint32_t)out[e].n;
+    if (out[e].n) memcpy(xyz + 3 * o, out[e].xyz, 3 * out[e].n * sizeof(double));
+    o += out[e].n;
+    free(out[e].xyz);
+  }
+  free(out);
+  return xyz;
+}

@@ -69,6 +69,31 @@ void xo_amp_plane(const double *xyz, const uint32_t *n_el, uint32_t nel, double 
 /* Form factor model used by xo_amp_plane. */
 double xo_ff_gauss(const double *coef9, double q);
 
+/* One block as block::calcAtoms reads it (CalcFunctions.cpp:251-392); the same layout as the
+ * library's xns_block. */
+typedef struct xo_block {
+  uint32_t natom, nid, nsymm, ncopy;
+  uint32_t ncell[3];
+  int32_t cutoff, cutoff_copies, ro_mol;
+  const uint32_t *natom_el, *id;
+  const double *r_atom, *occ, *dev, *p_symm, *r_symm, *r_copy, *cf;
+  double e[3][3];
+  double r_mean[3];
+  double rcut, rcut_copies, dev_mol;
+} xo_block;
+
+/* Philox4x32-10 (Salmon et al., SC 2011): ctr and key as four and two 32-bit words. */
+void xo_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+/* block::calcAtoms (CalcFunctions.cpp:251-392) for each block in turn, in the reference's loop order,
+ * with the random draws of the library's builder (Philox4x32-10 keyed by seed, counter = (site or
+ * symmetry index, copy-and-cell index low and high words, block << 8 | purpose)) in place of the
+ * clock-seeded std::default_random_engine.  Returns a malloc'd element-major x y z array (free with
+ * xo_free), n_el[nel] atoms per element, n_all (optional) atoms per block element. */
+double *xo_build_atoms(const xo_block *blocks, uint32_t nblocks, uint32_t nel, uint64_t seed, uint32_t *n_el,
+                       uint32_t *n_all);
+void xo_free(void *p);
+
 #ifdef __cplusplus
 }
 #endif

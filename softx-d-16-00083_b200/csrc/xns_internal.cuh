@@ -35,6 +35,7 @@ enum ScratchSlot {
   SLOT_HFLAGS,          // histogram: out-of-range count and run queue
   SLOT_BATCH,           // batched ensemble: coordinates, schedules and per-structure tables
   SLOT_BATCH_HIST,      // batched ensemble: histograms
+  SLOT_ATOMS,           // structure builder: the last build's atoms (x y z doubles, element-major)
   SLOT_COUNT
 };
 
@@ -66,6 +67,8 @@ struct xns_ctx {
   uint32_t x_kt = 0;
   // private batch reused by the one-shot batched entry point (batch.cu)
   struct xns_batch *batch_cache = nullptr;
+  // atoms per element of the last structure build (SLOT_ATOMS)
+  std::vector<uint32_t> atoms_n;
 };
 void xns_batch_release_cache(xns_ctx *ctx);
 

@@ -88,6 +88,10 @@ lib.xns_mlp_train.argtypes = [_p, _p, _p, _p, _int, _int, _int, C.c_float, C.POI
 lib.xns_calc_amp_plane.argtypes = [_p, _PP, _p, _u32, _dbl, _dbl, _u32, _dbl, _dbl, _u32, _int, _p, _p, _p]
 lib.xns_binning_features.argtypes = [_p, _p, _u32, _p]
 lib.xns_binning_correction.argtypes = [_p, _p, _p, _u32, _dbl, _p, _u32, _dbl, _p]
+lib.xns_build_atoms.argtypes = [_p, _p, _u32, _u32, C.c_uint64, _p, _p, C.POINTER(_p)]
+lib.xns_copy_atoms.argtypes = [_p, _PP]
+lib.xns_pdf_and_debye_device.argtypes = [_p, _p, _p, _u32, _u32, _dbl, _int, _int, _dbl, _p, _u32, _int, _PP, _p, _int,
+                                         _dbl, _p, _p, _p]
 
 
 def _ptr(a):
@@ -282,6 +286,28 @@ class Context:
 
     def set_stream(self, stream_ptr):
         self._check(lib.xns_set_stream(self._h, stream_ptr))
+
+    # -- structure builder -----------------------------------------------------------------------
+    def build_atoms(self, blocks, nel, seed=0):
+        """block::calcAtoms on the GPU for a list of structure.Block.  Returns (device address of the
+        element-major x y z doubles, n_el per element, n_all per block element); the device array stays
+        valid until the next build."""
+        from .structure import block_array
+        arr, keep = block_array(blocks)
+        n_el = np.zeros(nel, dtype=np.uint32)
+        n_all = np.zeros(max(1, sum(len(b.id) for b in blocks)), dtype=np.uint32)
+        dev = _p()
+        self._check(lib.xns_build_atoms(self._h, C.cast(arr, _p), len(blocks), nel, seed, _ptr(n_el), _ptr(n_all),
+                                        C.byref(dev)))
+        del keep
+        return dev.value, n_el, n_all[:sum(len(b.id) for b in blocks)]
+
+    def copy_atoms(self, n_el):
+        """The last build's atoms as a list of (n_e, 3) float64 arrays."""
+        out = [np.zeros((int(n), 3), dtype=np.float64) for n in n_el]
+        table = (_p * max(1, len(out)))(*[o.ctypes.data_as(_p) for o in out])
+        self._check(lib.xns_copy_atoms(self._h, C.cast(table, _PP)))
+        return out
 
     # -- calc functions --------------------------------------------------------------------------
     def calc_hist(self, elements, nhist, bin):
