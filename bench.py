@@ -396,7 +396,7 @@ def _fma_peaks(ctx):
 
 
 def debye_workload(args):
-    """Config 1: exact Debye double sum, fcc sphere a = 4.078 A cropped to 5000 atoms, Gaussian
+    """Exact Debye double sum, fcc sphere a = 4.078 A cropped to 5000 atoms, Gaussian
     displacement 0.05 A, neutron b = 7.63 fm, 1024 q in [0.1, 10).  Metric atom-pairs/s per pattern;
     roofline: FP32 pipe at 4 flops per (pair, q) term."""
     import torch
@@ -459,7 +459,7 @@ def debye_workload(args):
 
 
 def batch_workload(args):
-    """Config 4: an ensemble of fcc spheres (a = 4.078 A), atom counts log-uniform in [1e3, 2e5], each
+    """An ensemble of fcc spheres (a = 4.078 A), atom counts log-uniform in [1e3, 2e5], each
     with its own Gaussian displacement sigma in [0.02, 0.1] A; 0.001 A bins, 4096 q in [0.1, 25),
     neutron b = 7.63 fm.  Metric: patterns (I(q) of one structure) per second of the batched pass
     (one plan, one persistent histogram launch, one exact tensor-core transform), next to the plain
@@ -540,7 +540,7 @@ def batch_workload(args):
 
 
 def twod_workload(args):
-    """Config 3: 2D intensity of a 1,000,188-atom fcc crystallite (a = 3.61 A, 63^3 cells, 5 % second
+    """2D intensity of a 1,000,188-atom fcc crystallite (a = 3.61 A, 63^3 cells, 5 % second
     species, seeded random orientation), X-ray form factors from seeded 4-Gaussian coefficients, one
     orientation, on two meshes:
       * the Cartesian q plane normal to the beam, 1024 x 1024 points over [-8, 8)^2 A^-1 (the
@@ -612,6 +612,98 @@ def twod_workload(args):
     return 0
 
 
+def build_workload(args):
+    """Structure builder (block::calcAtoms, CalcFunctions.cpp:251-392): an atom-list block of 200,000
+    sites, where the O(sites^2) merge of sites closer than 0.5 A dominates.  Metric site pairs/s (one
+    build examines S(S-1)/2 site pairs); roofline: the merge kernel's FP32 prefilter, 8 flops per pair
+    (3 subtractions, a multiply and two FMAs), on the FP32 pipe."""
+    import ctypes as C
+
+    import torch
+    import xns_b200
+    from xns_b200 import lib, synth
+    torch.cuda.set_device(0)
+    lib.xns_last_stage_ms.argtypes = [C.c_void_p, C.c_int]
+    lib.xns_last_stage_ms.restype = C.c_double
+    ctx = xns_b200.Context(0)
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    n = args.build_sites
+    blk = synth.atom_file_block(n)
+    S = n
+    pairs = S * (S - 1) // 2
+    for w in range(args.warmup):
+        ctx.build_atoms([blk], 2, w)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    clocks = Clocks(0)
+    clocks.start()
+    l0 = ctx.kernel_launches
+    call = merge = fill = e2e = 0.0
+    atoms = 0
+    for k in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dev, n_el, _ = ctx.build_atoms([blk], 2, 100 + k)
+        call += ctx.last_kernel_ms
+        merge += lib.xns_last_stage_ms(ctx.handle, 5)
+        fill += lib.xns_last_stage_ms(ctx.handle, 6)
+        xs = ctx.copy_atoms(n_el)  # the atoms to the host, as the reference's ra[] vectors
+        e2e += (time.perf_counter() - t0) * 1e3
+        atoms = int(n_el.sum())
+    launches = ctx.kernel_launches - l0
+    clk = clocks.stop()
+    call, merge, fill, e2e = call / args.steps, merge / args.steps, fill / args.steps, e2e / args.steps
+    p64, p32 = _fma_peaks(ctx)
+    achieved = 8.0 * pairs / (merge * 1e-3) / 1e12
+    # the crystal case and the 1e7-atom scale case, timed the same way (device events of the call)
+    extra = {}
+    for name, b, nel in (("rock-salt 30^3 cells, 10% vacancies, sigma 0.07 A", synth.rocksalt_block(30), 2),):
+        for w in range(2):
+            ctx.build_atoms([b], nel, w)
+        ms = []
+        for k in range(3):
+            _, ne, _ = ctx.build_atoms([b], nel, 10 + k)
+            ms.append(ctx.last_kernel_ms)
+        extra[name] = {"atoms": int(ne.sum()), "ms": float(np.median(ms)), "atoms_per_s": float(ne.sum() / np.median(ms) * 1e3)}
+    line = {"metric": "site pairs/s (structure build)", "value": pairs / (call * 1e-3), "unit": "pairs/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": call, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 prefilter, f64 exact test and coordinates", "data": "synthetic (seeded)",
+            "config": {"workload": "structure builder: atom-list block of %d sites (density 0.05 A^-3, 2%% planted "
+                                   "within 0.1 A, occupancy 0.6 on every third site) -> %d atoms" % (n, atoms),
+                       "site_pairs_per_step": pairs, "merge_ms": merge, "write_ms": fill,
+                       "l2": "flushed (512 MB write) before every timed step", "also": extra},
+            "roofline": {"kernel": "merge_kernel", "bound": "fp32", "achieved": achieved, "peak": p32, "unit": "TFLOP/s",
+                         "frac": achieved / p32, "traffic": None, "flops_per_pair": 8,
+                         "peak_source": "measured in-process (FFMA loop, xns_measure_fma_peak)"},
+            "e2e": {"value": pairs / (e2e * 1e-3), "unit": "pairs/s", "ms_per_step": e2e, "h2d_bytes_per_step": S * 40,
+                    "d2h_bytes_per_step": atoms * 24},
+            "gpu_launches": int(launches), "clocks": clk}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as orc
+        try:
+            R, kind = orc.Reference(), "reference"
+            run = lambda b: R.calc_atoms([b], 2)  # noqa: E731
+        except FileNotFoundError:
+            R, kind = orc.Oracle(), "port"
+            run = lambda b: R.build_atoms([b], 2, 1)  # noqa: E731
+        m = 10000
+        while True:
+            b = synth.atom_file_block(m)
+            t = time.perf_counter()
+            run(b)
+            dt = time.perf_counter() - t
+            if dt > 4.0 or m >= n:
+                break
+            m = min(n, int(m * min(2.0, max(1.2, (12.0 / max(dt, 1e-3)) ** 0.5))))
+        line["cpu_baseline"] = {"value": m * (m - 1) // 2 / dt, "unit": "pairs/s", "cores": 1, "kind": kind,
+                                "sample": "block::calcAtoms on an atom-list block of %d sites of the same generator, "
+                                          "%.2f s (the reference's builder is single-threaded)" % (m, dt)}
+    print(json.dumps(line))
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -621,12 +713,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cells", type=int, default=CELLS,
                     help="cube edge in unit cells (default 30, the benchmark; smaller only for profiler captures)")
-    ap.add_argument("--workload", default="histogram", choices=["histogram", "debye", "2d", "batch"],
-                    help="histogram (default, the headline: config 2); debye (config 1), 2d (config 3) and batch "
-                         "(config 4) run on one GPU")
+    ap.add_argument("--workload", default="histogram", choices=["histogram", "debye", "2d", "batch", "build"],
+                    help="histogram (default, the headline: rock-salt cube histogram + rPDF + I(q)); debye (fcc "
+                         "sphere exact Debye sum), 2d (q plane), batch (ensemble of spheres) and build (structure "
+                         "builder on an atom-list block) run on one GPU")
     ap.add_argument("--batch-count", type=int, default=256, help="batch workload: structures in the ensemble")
     ap.add_argument("--cells2d", type=int, default=63, help="2d workload: crystallite edge in fcc cells (63: 1e6 atoms)")
     ap.add_argument("--mesh2d", type=int, default=1024, help="2d workload: q and phi points")
+    ap.add_argument("--build-sites", type=int, default=200000, help="build workload: sites of the atom-list block")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -637,6 +731,8 @@ def main():
         return twod_workload(args)
     if args.workload == "batch" and args.impl == "ours":
         return batch_workload(args)
+    if args.workload == "build" and args.impl == "ours":
+        return build_workload(args)
     if args.impl == "reference":
         return reference_arm(args, rank, world)
     if world > 1:

@@ -61,7 +61,8 @@ double xns_last_kernel_ms(const xns_ctx *ctx);
 /* Number of kernels the library launched since the context was created. */
 uint64_t xns_kernel_launches(const xns_ctx *ctx);
 /* Kernel-only device time (CUDA events on the library's stream) of one stage of the most recent call:
- * 0 histogram, 1 PDF, 2 histogram -> I(q), 3 Debye double sum, 4 2D amplitude; -1 if it did not run. */
+ * 0 histogram, 1 PDF, 2 histogram -> I(q), 3 Debye double sum, 4 2D amplitude, 5 the structure
+ * builder's site merge, 6 its atom-writing pass (the last block's); -1 if it did not run. */
 double xns_last_stage_ms(const xns_ctx *ctx, int stage);
 
 /* ---- host-buffer entry points (what the reference's calc functions become) ---------------------- */

@@ -30,11 +30,12 @@
 #include <algorithm>
 #include <vector>
 
+#include "f32x2.cuh"
 #include "xns_internal.cuh"
 
 namespace {
 
-constexpr int MT = 64;          // sites per merge tile
+constexpr int MT = 128;         // sites per merge tile (one thread per I row)
 constexpr int MAX_T = 125;      // translations: +-2 cells on three axes
 constexpr int GEN_THREADS = 256;
 constexpr int MAX_NID = 64;
@@ -214,10 +215,21 @@ __global__ void tile_box_kernel(const double *px, const double *py, const double
 }
 
 // ---- step 2: pairs of sites closer than 0.5 A -----------------------------------------------------------
+//
+// FP32 first: each site is stored as float offsets from its tile's box corner, and a tile pair with
+// translation t brings tile J's frame into tile I's by delta = oI - oJ + ct (FP64, rounded once).  The
+// FP32 squared distance d~^2 = |(a_i + delta) - a_j|^2 then differs from the FP64 one by a bounded
+// amount: each component by at most E_k = 2^-23 (2 wI_k + 2 wJ_k + 2 |delta_k| + 1) + 1e-9 (the
+// roundings of a_i, a_j, delta and the two subtractions, each at most half an FP32 ulp of a magnitude
+// below the bracket, with a factor 2 to spare), so a pair the reference accepts (|d| < 0.5) has
+// |d~| < 0.5 + E_x + E_y + E_z and d~^2 below thr = (0.5 + sum E)^2 (1 + 2^-20).  Pairs under thr -- a
+// few in a million -- are tested exactly in FP64 with the reference's operations.  Pairs of J rows go
+// through the packed f32x2 pipe, four pairs of rows per branch.
 
 struct MergeArgs {
   const double *px, *py, *pz, *box;
-  double ct[3 * MAX_T];  // translations e0 cx + e1 cy + e2 cz in the reference's loop order
+  const float *lx, *ly, *lz;  // offsets of each site from its tile's box corner
+  double ct[3 * MAX_T];       // translations e0 cx + e1 cy + e2 cz in the reference's loop order
   uint32_t S, ntile, T;
   unsigned long long npairs;  // tile pairs ti <= tj
   unsigned long long *hits;
@@ -225,9 +237,23 @@ struct MergeArgs {
   uint32_t *nhit, *outdeg, *indeg;
 };
 
-// (rAtomCell[i] - rAtomCell[j] + celltrans).sqr() < 0.25 for some translation (CalcFunctions.cpp:302)
+__global__ void local_coords_kernel(const double *px, const double *py, const double *pz, const double *box, uint32_t S,
+                                    float *lx, float *ly, float *lz) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S) return;
+  const double *b = box + 6 * (s / MT);
+  lx[s] = (float)(px[s] - b[0]), ly[s] = (float)(py[s] - b[1]), lz[s] = (float)(pz[s] - b[2]);
+}
+
+// exact test of (rAtomCell[i] - rAtomCell[j] + celltrans).sqr() < 0.25 (CalcFunctions.cpp:302)
+__device__ __forceinline__ bool exact_hit(const MergeArgs &a, D3 d0, int t) {
+  return sqr3(add3(d0, D3{a.ct[3 * t], a.ct[3 * t + 1], a.ct[3 * t + 2]})) < 0.25;
+}
+
 __global__ void __launch_bounds__(128) merge_kernel(const __grid_constant__ MergeArgs a) {
-  __shared__ double jx[MT], jy[MT], jz[MT];
+  using namespace xns_f2;
+  __shared__ f2 jx2[MT / 2], jy2[MT / 2], jz2[MT / 2];
+  __shared__ float sdel[MAX_T][4];  // delta x y z and thr per live translation
   __shared__ uint8_t alive[MAX_T];
   __shared__ int nalive;
   for (unsigned long long p = blockIdx.x; p < a.npairs; p += gridDim.x) {
@@ -238,42 +264,83 @@ __global__ void __launch_bounds__(128) merge_kernel(const __grid_constant__ Merg
     __syncthreads();
     if (threadIdx.x == 0) nalive = 0;
     __syncthreads();
-    // a translation can only give a hit when the boxes come closer than 0.5 A (with slack for rounding)
+    // a translation can only give a hit when the boxes come closer than 0.5 A (with slack for rounding);
+    // live translations are kept in loop order, so the first one that hits a pair is found first
     const double *bi = a.box + 6 * ti, *bj = a.box + 6 * tj;
-    for (uint32_t t = threadIdx.x; t < a.T; t += blockDim.x) {
-      double g2 = 0;
-      for (int k = 0; k < 3; k++) {
-        const double c = a.ct[3 * t + k];
-        const double dlo = bi[k] - bj[3 + k] + c, dhi = bi[3 + k] - bj[k] + c;  // d = ri - rj + c in [dlo, dhi]
-        const double g = fmax(0.0, fmax(dlo, -dhi));
-        g2 += g * g;
+    if (threadIdx.x < 32) {
+      for (uint32_t t0 = 0; t0 < a.T; t0 += 32) {
+        const uint32_t t = t0 + threadIdx.x;
+        bool live = false;
+        double del[3], esum = 0;
+        if (t < a.T) {
+          double g2 = 0;
+          for (int k = 0; k < 3; k++) {
+            const double c = a.ct[3 * t + k];
+            const double dlo = bi[k] - bj[3 + k] + c, dhi = bi[3 + k] - bj[k] + c;  // d = ri - rj + c in [dlo, dhi]
+            const double g = fmax(0.0, fmax(dlo, -dhi));
+            g2 += g * g;
+            del[k] = bi[k] - bj[k] + c;
+            esum += 0x1.0p-23 * (2.0 * (bi[3 + k] - bi[k]) + 2.0 * (bj[3 + k] - bj[k]) + 2.0 * fabs(del[k]) + 1.0) + 1e-9;
+          }
+          live = g2 < 0.25 * (1.0 + 1e-9) + 1e-9;
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, live);
+        if (live) {
+          const int slot = nalive + __popc(m & ((1u << threadIdx.x) - 1));
+          alive[slot] = (uint8_t)t;
+          for (int k = 0; k < 3; k++) sdel[slot][k] = (float)del[k];
+          sdel[slot][3] = __double2float_ru((0.5 + esum) * (0.5 + esum) * (1.0 + 0x1.0p-20));
+        }
+        __syncwarp();
+        if (threadIdx.x == 0) nalive += __popc(m);
+        __syncwarp();
       }
-      if (g2 < 0.25 * (1.0 + 1e-9) + 1e-9) alive[atomicAdd(&nalive, 1)] = (uint8_t)t;
     }
-    if (threadIdx.x < MT) {
-      const size_t j = tj * MT + threadIdx.x;
-      if (j < a.S) jx[threadIdx.x] = a.px[j], jy[threadIdx.x] = a.py[j], jz[threadIdx.x] = a.pz[j];
+    if (threadIdx.x < MT / 2) {
+      const size_t j = tj * MT + 2 * threadIdx.x;
+      // rows past the end sit far away and never pass the FP32 test
+      const float x0 = j < a.S ? a.lx[j] : 1e30f, y0 = j < a.S ? a.ly[j] : 1e30f, z0 = j < a.S ? a.lz[j] : 1e30f;
+      const float x1 = j + 1 < a.S ? a.lx[j + 1] : 1e30f, y1 = j + 1 < a.S ? a.ly[j + 1] : 1e30f,
+                  z1 = j + 1 < a.S ? a.lz[j + 1] : 1e30f;
+      jx2[threadIdx.x] = pack(x0, x1), jy2[threadIdx.x] = pack(y0, y1), jz2[threadIdx.x] = pack(z0, z1);
     }
     __syncthreads();
     const int na = nalive;
     if (na == 0) continue;
-    const uint32_t i = (uint32_t)(ti * MT) + (threadIdx.x & (MT - 1));
+    const uint32_t i = (uint32_t)(ti * MT) + threadIdx.x;
     if (i >= a.S) continue;
-    const D3 ri{a.px[i], a.py[i], a.pz[i]};
-    for (int jj = threadIdx.x / MT; jj < MT; jj += blockDim.x / MT) {
-      const uint32_t j = (uint32_t)(tj * MT) + jj;
-      if (j <= i || j >= a.S) continue;
-      const D3 d0 = sub3(ri, D3{jx[jj], jy[jj], jz[jj]});
-      bool hit = false;
-      for (int k = 0; k < na && !hit; k++) {
-        const int t = alive[k];
-        hit = sqr3(add3(d0, D3{a.ct[3 * t], a.ct[3 * t + 1], a.ct[3 * t + 2]})) < 0.25;
-      }
-      if (hit) {
-        const uint32_t pos = atomicAdd(a.nhit, 1u);
-        if (pos < a.cap) a.hits[pos] = ((unsigned long long)i << 32) | j;
-        atomicAdd(a.outdeg + i, 1u);
-        atomicAdd(a.indeg + j, 1u);
+    const float xi = a.lx[i], yi = a.ly[i], zi = a.lz[i];
+    for (int s = 0; s < na; s++) {
+      const f2 xd = splat(xi + sdel[s][0]), yd = splat(yi + sdel[s][1]), zd = splat(zi + sdel[s][2]);
+      const f2 nthr = splat(-sdel[s][3]);
+      // d~^2 - thr, evaluated as one FMA chain: its rounding stays within 2^-21 thr, inside the 2^-20 thr
+      // of slack in thr, so every pair under the FP32 bound comes out negative
+      auto excess = [&](int k) {
+        const f2 dx = sub(xd, jx2[k]), dy = sub(yd, jy2[k]), dz = sub(zd, jz2[k]);
+        return fma(dz, dz, fma(dy, dy, fma(dx, dx, nthr)));
+      };
+      for (int k0 = 0; k0 < MT / 2; k0 += 4) {
+        unsigned long long any = 0;  // sign bits of four pairs of J rows
+#pragma unroll
+        for (int u = 0; u < 4; u++) any |= excess(k0 + u);
+        if (!(any & 0x8000000080000000ull)) continue;
+        for (int u = 0; u < 4; u++) {
+          const unsigned long long e2 = excess(k0 + u);
+          for (int h = 0; h < 2; h++) {
+            const uint32_t j = (uint32_t)(tj * MT) + 2 * (k0 + u) + h;
+            if (!((e2 >> (32 * h + 31)) & 1) || j <= i || j >= a.S) continue;
+            const D3 d0 = sub3(D3{a.px[i], a.py[i], a.pz[i]}, D3{a.px[j], a.py[j], a.pz[j]});
+            // record the pair once: at the first live translation that hits it
+            if (!exact_hit(a, d0, alive[s])) continue;
+            bool earlier = false;
+            for (int e = 0; e < s && !earlier; e++) earlier = exact_hit(a, d0, alive[e]);
+            if (earlier) continue;
+            const uint32_t pos = atomicAdd(a.nhit, 1u);
+            if (pos < a.cap) a.hits[pos] = ((unsigned long long)i << 32) | j;
+            atomicAdd(a.outdeg + i, 1u);
+            atomicAdd(a.indeg + j, 1u);
+          }
+        }
       }
     }
   }
@@ -638,6 +705,11 @@ int plan_block(xns_ctx *ctx, Arena &ar, const xns_block &bk, uint32_t blk, uint6
   XNS_TRY(ar.get(6 * (size_t)ntile, &box));
   tile_box_kernel<<<blocks_for(ntile, 128), 128, 0, st>>>(px, py, pz, S, ntile, box);
   XNS_LAUNCHED(ctx);
+  float *loc;
+  XNS_TRY(ar.get(3 * (size_t)S, &loc));
+  local_coords_kernel<<<blocks_for(S, 256), 256, 0, st>>>(px, py, pz, box, S, loc, loc + S, loc + 2 * (size_t)S);
+  XNS_LAUNCHED(ctx);
+  ma.lx = loc, ma.ly = loc + S, ma.lz = loc + 2 * (size_t)S;
   uint32_t *deg, *nhit;
   XNS_TRY(ar.get(2 * (size_t)S + 1, &deg));
   uint32_t *outdeg = deg, *indeg = deg + S;
@@ -652,8 +724,10 @@ int plan_block(xns_ctx *ctx, Arena &ar, const xns_block &bk, uint32_t blk, uint6
     ma.hits = hits, ma.cap = cap;
     XNS_CUDA(ctx, cudaMemsetAsync(deg, 0, (2 * (size_t)S + 1) * 4, st));
     const unsigned grid = (unsigned)std::min<unsigned long long>(ma.npairs, (unsigned long long)ctx->num_sms * 16);
+    XNS_TRY(xns_stage_begin(ctx, STAGE_MERGE));
     merge_kernel<<<grid, 128, 0, st>>>(ma);
     XNS_LAUNCHED(ctx);
+    XNS_TRY(xns_stage_end(ctx, STAGE_MERGE));
     XNS_CUDA(ctx, cudaMemcpyAsync(&h_nhit, nhit, 4, cudaMemcpyDeviceToHost, st));
     XNS_CUDA(ctx, cudaStreamSynchronize(st));
     if (h_nhit <= cap) break;
@@ -773,8 +847,10 @@ extern "C" int xns_build_atoms(xns_ctx *ctx, const xns_block *blocks, uint32_t n
       unsigned long long *d_dst;
       XNS_TRY(ar.get(bk.nid, &d_dst));
       XNS_CUDA(ctx, cudaMemcpyAsync(d_dst, dst.data(), 8 * (size_t)bk.nid, cudaMemcpyHostToDevice, ctx->stream));
+      XNS_TRY(xns_stage_begin(ctx, STAGE_FILL));
       gen_write_kernel<<<r.ncta, GEN_THREADS, 0, ctx->stream>>>(r.g, r.cta_cnt, d_dst, out);
       XNS_LAUNCHED(ctx);
+      XNS_TRY(xns_stage_end(ctx, STAGE_FILL));
       XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // dst lives on this host frame
     }
     for (uint32_t k = 0; k < bk.nid; k++) {

@@ -46,8 +46,9 @@ struct xns_ctx {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // kernel-only events of the last call: stage k (0 histogram, 1 PDF, 2 I(q) transform, 3 Debye
-  // sum, 4 2D amplitude) ran between ev_stage[2k] and ev_stage[2k+1]
-  static const int NSTAGE = 5;
+  // sum, 4 2D amplitude, 5 structure builder's site merge, 6 its atom-writing pass) ran between
+  // ev_stage[2k] and ev_stage[2k+1]
+  static const int NSTAGE = 7;
   cudaEvent_t ev_stage[2 * NSTAGE] = {};
   unsigned stage_mask = 0;
   double last_ms = 0;
@@ -136,7 +137,7 @@ bool xns_uniform_mesh(const double *q, uint32_t nq, double *q0, double *dq);
 int xns_timer_start(xns_ctx *ctx);
 int xns_timer_stop(xns_ctx *ctx);
 // Kernel-only stage timing (see xns_ctx::ev_stage).
-enum { STAGE_HIST = 0, STAGE_PDF = 1, STAGE_IQ = 2, STAGE_DEBYE = 3, STAGE_2D = 4 };
+enum { STAGE_HIST = 0, STAGE_PDF = 1, STAGE_IQ = 2, STAGE_DEBYE = 3, STAGE_2D = 4, STAGE_MERGE = 5, STAGE_FILL = 6 };
 int xns_stage_begin(xns_ctx *ctx, int k);
 int xns_stage_end(xns_ctx *ctx, int k);
 

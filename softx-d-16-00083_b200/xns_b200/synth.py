@@ -12,6 +12,11 @@ Workloads (sizes as stated, reduced sizes for tests):
                  sigma 0.07 A, b = 3.63 / 9.58 fm)
   fcc_crystallite fcc cube with random substitution by a second species, rotated by a seeded
                  quaternion (2D amplitude: a = 3.61 A, ~1e6 atoms, 5 % substitution)
+  atom_file_block a structure read from an atom list (one cell, no symmetry) as a builder block: sites
+                 at random in a cube of the given density, a fraction planted within N(0, 0.1 A) of
+                 earlier sites, partial occupancy on every third site (structure builder: 2e5 sites)
+  rocksalt_block the rock-salt cube as the reference's XML describes it: a two-site cell with the four
+                 fcc translations, replicated, with occupancy and displacement per site
 """
 import numpy as np
 
@@ -120,3 +125,21 @@ def hist_size(elements, bin):
     xyz = np.concatenate([np.asarray(e).reshape(-1, 3) for e in elements])
     d = xyz.max(axis=0) - xyz.min(axis=0)
     return int(np.sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) / bin) + 1
+
+
+def atom_file_block(n=200000, density=0.05, planted=0.02, occ=0.6, seed=1):
+    """A builder block for an atom list of n sites (two elements, halves), see the module docstring."""
+    from .structure import Block
+    rng = np.random.default_rng(seed)
+    pts = rng.uniform(0, (n / density) ** (1 / 3), (n, 3))
+    k = int(n * planted)
+    pts[n // 2:n // 2 + k] = pts[:k] + rng.normal(0, 0.1, (k, 3))
+    return Block(pts, [n // 2, n - n // 2], [0, 1], occ=np.where(np.arange(n) % 3 == 0, occ, 1.0))
+
+
+def rocksalt_block(cells=30, a=5.64, vacancy=0.1, sigma=0.07):
+    """The rock-salt cube as a builder block (Na at 0 0 0, Cl at 1/2 0 0, fcc translations)."""
+    from .structure import Block
+    fcc = [(np.eye(3), t) for t in [(0, 0, 0), (0, .5, .5), (.5, 0, .5), (.5, .5, 0)]]
+    return Block.crystal(np.eye(3) * a, [(0, 0, 0), (0.5, 0, 0)], [1, 1], [0, 1], (cells, cells, cells), symm=fcc,
+                         occ=[1 - vacancy] * 2, dev=[sigma] * 2)

@@ -122,3 +122,23 @@ def test_bad_blocks_are_rejected(gpu_ctx):
     b.natom_el = np.array([1, 0], dtype=np.uint32)
     with pytest.raises(xns_b200.XnsError):
         gpu_ctx.build_atoms([b], 2, 0)  # natom_el does not sum to natom
+
+
+def test_merge_threshold_far_from_origin(gpu_ctx):
+    """pairs a hair either side of 0.5 A at coordinates up to 900 A, where an FP32 ulp is 6e-5 A: the
+    FP32 prefilter must pass every pair the FP64 test accepts, and nothing else gets merged"""
+    rng = np.random.default_rng(8)
+    base = rng.uniform(-900, 900, (600, 3))
+    u = rng.normal(size=(600, 3))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    eps = np.concatenate([-np.logspace(-15, -4, 300), np.logspace(-15, -4, 300)])
+    partner = base + u * (0.5 + eps)[:, None]
+    pts = np.empty((1200, 3))
+    pts[0::2], pts[1::2] = base, partner
+    b = Block(pts, [1200], [0], occ=np.where(np.arange(1200) % 2 == 0, 0.0, 1.0))
+    xg, _, _, _ = _build(gpu_ctx, [b], 1, 2)
+    xo, _ = oracle().build_atoms([b], 1, seed=2)
+    assert np.array_equal(xg[0], xo[0])
+    # merged pairs place the partner (occupancy 1) once; unmerged ones place it alone too, but the
+    # base site (occupancy 0) then draws nothing: the count shows nothing about the merge, the order does
+    assert 250 < sum(np.linalg.norm(pts[1::2] - pts[0::2], axis=1) < 0.5) < 350
