@@ -87,6 +87,13 @@ def build_shim(ref):
     exe = os.path.join(LIB, "XaNSoNS_B200")
     if _newer(exe, objs + [shim_so]):
         _run([cxx, "-o", exe] + objs + ["-L" + LIB, "-lxns_calc_shim", "-lxns_b200", "-Wl,-rpath,$ORIGIN"])
+    # test program for the drop-in structure builder (tests/shim/build_atoms_check.cpp)
+    chk_src = os.path.join(ROOT, "tests", "shim", "build_atoms_check.cpp")
+    chk = os.path.join(LIB, "xns_build_atoms_check")
+    ref_cf = [o for o in objs if o.endswith("ref_CalcFunctions.o") or o.endswith("ref_IO.o")]
+    if os.path.exists(chk_src) and _newer(chk, [chk_src, shim_so] + ref_cf):
+        _run([cxx, "-O2", "-std=c++11", "-w", "-I" + ref, chk_src] + ref_cf +
+             ["-o", chk, "-L" + LIB, "-lxns_calc_shim", "-lxns_b200", "-Wl,-rpath,$ORIGIN"])
     return exe
 
 

@@ -512,17 +512,23 @@ __global__ void __launch_bounds__(GEN_THREADS) gen_count_kernel(const __grid_con
   for (uint32_t k = threadIdx.x; k < g.b.nid; k += blockDim.x) cta_cnt[(size_t)blockIdx.x * g.b.nid + k] = cnt[k];
 }
 
-// per element: exclusive offsets of the CTAs' counts and the block's total
+// per element (one warp each): exclusive offsets of the CTAs' counts and the block's total
 __global__ void gen_offsets_kernel(uint32_t *cta_cnt, uint32_t ncta, uint32_t nid, uint32_t *total) {
-  const uint32_t k = threadIdx.x;
-  if (k >= nid) return;
+  const uint32_t k = blockIdx.x, lane = threadIdx.x;
   uint32_t run = 0;
-  for (uint32_t c = 0; c < ncta; c++) {
-    const uint32_t v = cta_cnt[(size_t)c * nid + k];
-    cta_cnt[(size_t)c * nid + k] = run;
-    run += v;
+  for (uint32_t c0 = 0; c0 < ncta; c0 += 32) {
+    const uint32_t c = c0 + lane;
+    const uint32_t v = c < ncta ? cta_cnt[(size_t)c * nid + k] : 0;
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (c < ncta) cta_cnt[(size_t)c * nid + k] = run + incl - v;
+    run += __shfl_sync(0xffffffffu, incl, 31);
   }
-  total[k] = run;
+  if (lane == 0) total[k] = run;
 }
 
 // dst[k]: first atom slot of block element k in the output
@@ -807,7 +813,7 @@ int plan_block(xns_ctx *ctx, Arena &ar, const xns_block &bk, uint32_t blk, uint6
   XNS_TRY(ar.get(bk.nid, &tot));
   gen_count_kernel<<<run->ncta, GEN_THREADS, 0, st>>>(g, run->cta_cnt);
   XNS_LAUNCHED(ctx);
-  gen_offsets_kernel<<<1, MAX_NID, 0, st>>>(run->cta_cnt, run->ncta, bk.nid, tot);
+  gen_offsets_kernel<<<bk.nid, 32, 0, st>>>(run->cta_cnt, run->ncta, bk.nid, tot);
   XNS_LAUNCHED(ctx);
   XNS_CUDA(ctx, cudaMemcpyAsync(run->total.data(), tot, 4 * (size_t)bk.nid, cudaMemcpyDeviceToHost, st));
   XNS_CUDA(ctx, cudaStreamSynchronize(st));

@@ -143,3 +143,69 @@ void calcInt2D(double ***I2D, double **I, const config *cfg, const unsigned int 
   }
   cout << "2D pattern calculation time: " << seconds_since(t1) << " s" << endl;
 }
+
+// block::calcAtoms (CalcFunctions.cpp:251-392) of every block on the GPU, for CalcAndPrintAtoms
+// (:397), whose loop `for (iB...) Block[iB].calcAtoms(*ra);` this call replaces: the atoms are appended
+// to ra[] per element in the reference's order, and each block's NatomElAll and N are set as
+// calcAtoms sets them.  The random draws are Philox4x32-10 keyed by the XNS_SEED environment variable;
+// without it the seed comes from the clock, as the reference's generator does (CalcFunctions.cpp:259).
+void calcAtomsB200(block *Block, unsigned int Nblocks, vector<vect3d<double> > *ra, unsigned int Nel) {
+  static_assert(sizeof(vect3d<double>) == 3 * sizeof(double), "vect3d<double> must be three packed doubles");
+  const char *s = getenv("XNS_SEED");
+  const uint64_t seed = s ? strtoull(s, nullptr, 10)
+                          : (uint64_t)chrono::system_clock::now().time_since_epoch().count();
+  vector<xns_block> xb(Nblocks);
+  vector<vector<double> > store(Nblocks);  // pSymm, rSymm, rCopy and cf of each block as flat rows
+  for (unsigned int iB = 0; iB < Nblocks; iB++) {
+    const block &b = Block[iB];
+    xns_block &x = xb[iB];
+    memset(&x, 0, sizeof(x));
+    x.natom = b.Natom;
+    x.nid = b.Nid;
+    x.nsymm = b.Nsymm;
+    x.ncopy = b.Ncopy;
+    x.ncell[0] = b.Ncell.x, x.ncell[1] = b.Ncell.y, x.ncell[2] = b.Ncell.z;
+    x.cutoff = b.cutoff, x.cutoff_copies = b.cutoffcopies, x.ro_mol = b.ro_mol;
+    x.natom_el = b.NatomEl.empty() ? nullptr : &b.NatomEl[0];
+    x.id = b.id;
+    x.r_atom = b.Natom ? &b.rAtom[0].x : nullptr;
+    x.occ = b.occ;
+    x.dev = b.dev;
+    vector<double> &f = store[iB];
+    for (unsigned int is = 0; is < b.Nsymm; is++)
+      for (int k = 0; k < 3; k++) f.insert(f.end(), {b.pSymm[k][is].x, b.pSymm[k][is].y, b.pSymm[k][is].z});
+    const size_t o_rs = f.size();
+    for (unsigned int is = 0; is < b.Nsymm; is++) f.insert(f.end(), {b.rSymm[is].x, b.rSymm[is].y, b.rSymm[is].z});
+    const size_t o_rc = f.size();
+    for (unsigned int ic = 0; ic < b.Ncopy; ic++) f.insert(f.end(), {b.rCopy[ic].x, b.rCopy[ic].y, b.rCopy[ic].z});
+    const size_t o_cf = f.size();
+    for (unsigned int ic = 0; ic < b.Ncopy; ic++)
+      for (int k = 0; k < 3; k++) f.insert(f.end(), {b.cf[k][ic].x, b.cf[k][ic].y, b.cf[k][ic].z});
+    f.push_back(0.0);  // keeps every offset inside the vector
+    x.p_symm = f.data(), x.r_symm = f.data() + o_rs, x.r_copy = f.data() + o_rc, x.cf = f.data() + o_cf;
+    for (int k = 0; k < 3; k++) {
+      x.e[k][0] = b.e[k].x, x.e[k][1] = b.e[k].y, x.e[k][2] = b.e[k].z;
+    }
+    x.r_mean[0] = b.rMean.x, x.r_mean[1] = b.rMean.y, x.r_mean[2] = b.rMean.z;
+    x.rcut = b.Rcut, x.rcut_copies = b.RcutCopies, x.dev_mol = b.dev_mol;
+  }
+  vector<uint32_t> n_el(Nel), n_all;
+  for (unsigned int iB = 0; iB < Nblocks; iB++) n_all.resize(n_all.size() + Block[iB].Nid);
+  const double *dev = nullptr;
+  check(xns_build_atoms(context(), xb.data(), Nblocks, Nel, seed, n_el.data(), n_all.empty() ? nullptr : n_all.data(), &dev));
+  vector<double *> dst(Nel, nullptr);
+  vector<size_t> before(Nel);
+  for (unsigned int e = 0; e < Nel; e++) {
+    before[e] = ra[e].size();
+    ra[e].resize(before[e] + n_el[e]);
+    if (n_el[e]) dst[e] = &ra[e][before[e]].x;
+  }
+  check(xns_copy_atoms(context(), dst.data()));
+  for (unsigned int iB = 0, o = 0; iB < Nblocks; iB++) {
+    Block[iB].NatomElAll.resize(Block[iB].Nid);
+    for (unsigned int k = 0; k < Block[iB].Nid; k++, o++) {
+      Block[iB].NatomElAll[k] = n_all[o];
+      Block[iB].N += n_all[o];
+    }
+  }
+}

@@ -142,3 +142,19 @@ def test_merge_threshold_far_from_origin(gpu_ctx):
     # merged pairs place the partner (occupancy 1) once; unmerged ones place it alone too, but the
     # base site (occupancy 0) then draws nothing: the count shows nothing about the merge, the order does
     assert 250 < sum(np.linalg.norm(pts[1::2] - pts[0::2], axis=1) < 0.5) < 350
+
+
+def test_drop_in_builder_matches_reference_program_objects():
+    """calcAtomsB200 (the drop-in for CalcAndPrintAtoms' calcAtoms loop) on the reference's own block
+    objects against the reference's block::calcAtoms, in one program linked with the reference's
+    compiled CalcFunctions object: same atoms, order, NatomElAll and N"""
+    import os
+    import subprocess
+    from conftest import ROOT
+    exe = os.path.join(ROOT, "softx-d-16-00083_b200", "lib", "xns_build_atoms_check")
+    if not os.path.exists(exe):
+        pytest.skip("drop-in check program not built (needs the reference sources at build time)")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    lines = r.stdout.strip().splitlines()
+    assert len(lines) == 2 and all(l.endswith("identical") for l in lines)
