@@ -301,6 +301,25 @@ int xns_build_atoms(xns_ctx *ctx, const xns_block *blocks, uint32_t nblocks, uin
 /* Copies the last build's atoms into host arrays: xyz_el[e] receives n_el[e] x y z triples. */
 int xns_copy_atoms(xns_ctx *ctx, double *const *xyz_el);
 
+/* ---- output writers ---------------------------------------------------------------------------------- */
+
+/* The reference's text outputs, byte for byte, formatted on all host threads (no device needed).
+ * Every number is printed as printf's "%.6e", as the reference's ios::scientific streams print it.
+ * Each returns 0, or -1 when the file cannot be written.  The file names are the caller's; the
+ * reference builds them as <name>_<xray|neut>_<kind>.txt (IO.cpp:55-57, :112-113, :150-151).
+ *   xns_write_i      printI (IO.cpp:109-124) and, per block pair, printPartialI (:125-147):
+ *                    "q<TAB>I" per q point.
+ *   xns_write_i2     printI2 (IO.cpp:148-167): one row per q, nfi values each followed by a TAB.
+ *   xns_write_pdf    printPDF (IO.cpp:51-73, partial = 0) and, per element pair, printPartialPDF
+ *                    (:74-108, partial = 1): "r<TAB>value" for r = (i + 0.5) bin, rows up to the last
+ *                    one whose |value| (total) or value (partial) exceeds 1e-10.
+ *   xns_write_atoms  printAtoms (IO.cpp:273-295): Ntot, an empty line, then "name x  y  z" per atom,
+ *                    elements in the order given (the reference's ID map order). */
+int xns_write_i(const char *path, const double *q, const double *I, uint32_t nq);
+int xns_write_i2(const char *path, const double *I2D, uint32_t nq, uint32_t nfi);
+int xns_write_pdf(const char *path, const double *pdf, uint32_t nhist, double bin, int partial);
+int xns_write_atoms(const char *path, const double *xyz, const uint32_t *n_el, uint32_t nel, const char *const *names);
+
 /* ---- utilities (no reference counterpart) -------------------------------------------------------- */
 
 /* Measured FMA-pipe throughput of this device in TFLOP/s (an FMA counts 2 flops): FP64 when fp64 != 0,

@@ -206,6 +206,12 @@ class Reference:
         L.xnsref_calc_atoms.argtypes = [_p, _u32, _u32, _p, _p]
         L.xnsref_calc_atoms.restype = _p
         L.xnsref_free.argtypes = [_p]
+        L.xnsref_print_i.argtypes = [C.c_char_p, _p, _p, _u32, _u32]
+        L.xnsref_print_partial_i.argtypes = [C.c_char_p, _p, _p, _u32, _u32, _u32]
+        L.xnsref_print_i2.argtypes = [C.c_char_p, _p, _u32, _u32, _u32]
+        L.xnsref_print_pdf.argtypes = [C.c_char_p, _p, _u32, _dbl, _u32, _u32]
+        L.xnsref_print_partial_pdf.argtypes = [C.c_char_p, _p, _u32, _dbl, _u32, _u32, _u32, _p]
+        L.xnsref_print_atoms.argtypes = [C.c_char_p, _p, _p, _u32, _p]
         L.xnsref_hist_size.argtypes = [_p, _p, _u32, _dbl]
         L.xnsref_hist_size.restype = _u32
         L.xnsref_atomic_density.argtypes = [_p, _p, _u32]
@@ -218,6 +224,37 @@ class Reference:
                                                 _dbl, _int, _p, _p]
         L.xnsref_calc_int_2d.argtypes = [_p, _p, _u32, _p, _u32, _u32, _p, _p, _p, _u32, _dbl, _int, _p, _p, _int, _int,
                                          _p, _p]
+
+    # the reference's writers: name is the path prefix; they return the reference's status
+    def print_i(self, name, q, I, source):
+        q, I = _f64(q), _f64(I)
+        return self.lib.xnsref_print_i(name.encode(), _ptr(q), _ptr(I), len(q), source)
+
+    def print_partial_i(self, name, q, I, source, nblocks):
+        q, I = _f64(q), _f64(I)
+        return self.lib.xnsref_print_partial_i(name.encode(), _ptr(q), _ptr(I), len(q), source, nblocks)
+
+    def print_i2(self, name, I2D, source):
+        a = np.ascontiguousarray(I2D, dtype=np.float64)
+        return self.lib.xnsref_print_i2(name.encode(), _ptr(a), a.shape[0], a.shape[1], source)
+
+    def print_pdf(self, name, pdf, bin, source, pdftype):
+        a = _f64(pdf)
+        return self.lib.xnsref_print_pdf(name.encode(), _ptr(a), len(a), bin, source, pdftype)
+
+    @staticmethod
+    def _names(names):
+        nm = [n.encode() for n in names]
+        return (C.c_char_p * max(1, len(nm)))(*nm)
+
+    def print_partial_pdf(self, name, pdf, nhist, bin, source, pdftype, names):
+        a = _f64(pdf)
+        return self.lib.xnsref_print_partial_pdf(name.encode(), _ptr(a), nhist, bin, source, pdftype, len(names),
+                                                 C.cast(self._names(names), _p))
+
+    def print_atoms(self, name, elements, names):
+        xyz, n = _flat(elements)
+        return self.lib.xnsref_print_atoms(name.encode(), _ptr(xyz), _ptr(n), len(n), C.cast(self._names(names), _p))
 
     def calc_atoms(self, blocks, nel):
         """(list of per-element (n, 3) arrays, n_all) from the reference's own block::calcAtoms."""

@@ -22,6 +22,12 @@ void calcIntPartialDebye(double **I, const config *cfg, const unsigned int *Nato
 void calcHist(unsigned long long int **rij_hist, const vector<vect3d<double> > *ra, const unsigned int *NatomEl, unsigned int Nel, unsigned int Nhist, double bin, int NumOMPthreads);
 void calcInt1DHist(double **I, unsigned long long int *rij_hist, const unsigned int *NatomEl, unsigned int Nel, const config *cfg, vector<double *> FF, vector<double> SL, const double *q, unsigned int Ntot, int NumOMPthreads);
 void calcPDFandDebye(double **I, double **PDF, const config *cfg, const unsigned int *NatomEl, const vector<vect3d<double> > *ra, vector<double *> FF, vector<double> SL, const double *q, unsigned int Ntot, int NumOMPthreads);
+int printI(const double *I, unsigned int Nq, const double *q, string name, unsigned int source);
+int printI2(const double *const *I2D, unsigned int Nq, unsigned int Nfi, string name, unsigned int source);
+int printPartialI(const double *I, unsigned int Nq, const double *q, string name, unsigned int source, unsigned int Nblocks);
+int printPDF(const double *PDF, unsigned int Nhist, double hist_bin, string name, unsigned int source, unsigned int PDFtype);
+int printPartialPDF(const double *PDF, unsigned int Nhist, double hist_bin, string name, unsigned int source, unsigned int PDFtype, unsigned int Nel, map<string, unsigned int> ID);
+int printAtoms(const vector<vect3d<double> > *ra, string name, map<string, unsigned int> ID, unsigned int Ntot);
 void calcInt2D(double ***I2D, double **I, const config *cfg, const unsigned int *NatomEl, const vector<vect3d<double> > *ra, vector<double *> FF, vector<double> SL, const double *q, unsigned int Ntot, int NumOMPthreads);
 
 namespace {
@@ -335,6 +341,39 @@ double *xnsref_calc_atoms(const xr_block *blocks, uint32_t nblocks, uint32_t nel
   }
   delete[] ra;
   return xyz;
+}
+
+// The reference's writers (IO.cpp:51-167, 273-295), called unchanged; name is the path prefix the
+// reference appends its suffixes to.  I2D is nq x nfi row-major; names: nel element names in the
+// reference's ID map order.
+int xnsref_print_i(const char *name, const double *q, const double *I, uint32_t nq, uint32_t source) {
+  return printI(I, nq, q, string(name), source);
+}
+int xnsref_print_partial_i(const char *name, const double *q, const double *I, uint32_t nq, uint32_t source, uint32_t nblocks) {
+  return printPartialI(I, nq, q, string(name), source, nblocks);
+}
+int xnsref_print_i2(const char *name, const double *I2D, uint32_t nq, uint32_t nfi, uint32_t source) {
+  vector<const double *> rows(nq);
+  for (uint32_t i = 0; i < nq; i++) rows[i] = I2D + (size_t)i * nfi;
+  return printI2(rows.data(), nq, nfi, string(name), source);
+}
+int xnsref_print_pdf(const char *name, const double *pdf, uint32_t nhist, double bin, uint32_t source, uint32_t pdftype) {
+  return printPDF(pdf, nhist, bin, string(name), source, pdftype);
+}
+static map<string, unsigned int> id_map(const char *const *names, uint32_t nel) {
+  map<string, unsigned int> ID;
+  for (uint32_t e = 0; e < nel; e++) ID[names[e]] = e;
+  return ID;
+}
+int xnsref_print_partial_pdf(const char *name, const double *pdf, uint32_t nhist, double bin, uint32_t source, uint32_t pdftype,
+                             uint32_t nel, const char *const *names) {
+  return printPartialPDF(pdf, nhist, bin, string(name), source, pdftype, nel, id_map(names, nel));
+}
+int xnsref_print_atoms(const char *name, const double *xyz, const uint32_t *n_el, uint32_t nel, const char *const *names) {
+  vector<vect3d<double> > *ra = make_ra(xyz, n_el, nel);
+  int r = printAtoms(ra, string(name), id_map(names, nel), total(n_el, nel));
+  delete[] ra;
+  return r;
 }
 
 }  // extern "C"

@@ -24,6 +24,7 @@ GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = GENCODE + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC,
                         "-Xptxas", "-warn-spills"]
 
+HOST_SOURCES = ["writers.cpp"]  # host-only parts of the library, in host/
 SOURCES = ["context.cu", "schedule.cu", "hist.cu", "sinc_engine.cu", "debye.cu", "hist_iq.cu", "pdf.cu",
            "amp2d.cu", "noalloc.cu", "tc_gemm.cu", "tc_exact.cu", "batch.cu", "mlp.cu", "learned.cu", "builder.cu"]
 
@@ -52,6 +53,12 @@ def build_lib(verbose_ptxas=False):
         if _newer(o, [s] + headers):
             flags = NVCC_FLAGS + (["-Xptxas", "-v"] if verbose_ptxas else [])
             _run([NVCC] + flags + ["-c", s, "-o", o])
+        objs.append(o)
+    for src in HOST_SOURCES:
+        s = os.path.join(PKG, "host", src)
+        o = os.path.join(BUILD, src.replace(".cpp", ".o"))
+        if _newer(o, [s, os.path.join(INCLUDE, "xns_b200.h")]):
+            _run(["g++", "-O2", "-std=c++17", "-fPIC", "-Wall", "-I" + INCLUDE, "-c", s, "-o", o])
         objs.append(o)
     so = os.path.join(LIB, "libxns_b200.so")
     if _newer(so, objs):

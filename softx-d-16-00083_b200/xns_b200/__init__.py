@@ -90,6 +90,10 @@ lib.xns_binning_features.argtypes = [_p, _p, _u32, _p]
 lib.xns_binning_correction.argtypes = [_p, _p, _p, _u32, _dbl, _p, _u32, _dbl, _p]
 lib.xns_build_atoms.argtypes = [_p, _p, _u32, _u32, C.c_uint64, _p, _p, C.POINTER(_p)]
 lib.xns_copy_atoms.argtypes = [_p, _PP]
+lib.xns_write_i.argtypes = [C.c_char_p, _p, _p, _u32]
+lib.xns_write_i2.argtypes = [C.c_char_p, _p, _u32, _u32]
+lib.xns_write_pdf.argtypes = [C.c_char_p, _p, _u32, _dbl, _int]
+lib.xns_write_atoms.argtypes = [C.c_char_p, _p, _p, _u32, _PP]
 lib.xns_pdf_and_debye_device.argtypes = [_p, _p, _p, _u32, _u32, _dbl, _int, _int, _dbl, _p, _u32, _int, _PP, _p, _int,
                                          _dbl, _p, _p, _p]
 
@@ -421,3 +425,37 @@ class Context:
                                         _ptr(emax), _ptr(en), convention, lam, source, fft, _ptr(sl), int(polar),
                                         _ptr(I2D), _ptr(I)))
         return I2D, I
+
+
+# -- output writers (host threads; byte-identical to the reference's IO.cpp writers) ---------------------
+def _wcheck(rc, path):
+    if rc:
+        raise OSError("xns_b200: cannot write %s" % path)
+
+
+def write_i(path, q, I):
+    """printI / printPartialI (IO.cpp:109-147): q<TAB>I per line, %.6e."""
+    q, I = np.ascontiguousarray(q, dtype=np.float64), np.ascontiguousarray(I, dtype=np.float64)
+    _wcheck(lib.xns_write_i(path.encode(), _ptr(q), _ptr(I), len(q)), path)
+
+
+def write_i2(path, I2D):
+    """printI2 (IO.cpp:148-167): one row per q, each value followed by a TAB."""
+    a = np.ascontiguousarray(I2D, dtype=np.float64)
+    _wcheck(lib.xns_write_i2(path.encode(), _ptr(a), a.shape[0], a.shape[1]), path)
+
+
+def write_pdf(path, pdf, bin, partial=False):
+    """printPDF (partial=False) / one element pair of printPartialPDF (IO.cpp:51-108)."""
+    a = np.ascontiguousarray(pdf, dtype=np.float64)
+    _wcheck(lib.xns_write_pdf(path.encode(), _ptr(a), len(a), bin, int(partial)), path)
+
+
+def write_atoms(path, elements, names):
+    """printAtoms (IO.cpp:273-295) for per-element (n, 3) arrays, in the order given."""
+    arrs = [np.ascontiguousarray(e, dtype=np.float64).reshape(-1, 3) for e in elements]
+    n_el = np.array([len(a) for a in arrs], dtype=np.uint32)
+    xyz = np.ascontiguousarray(np.concatenate(arrs) if arrs else np.zeros((0, 3)))
+    nm = [n.encode() for n in names]
+    table = (C.c_char_p * max(1, len(nm)))(*nm)
+    _wcheck(lib.xns_write_atoms(path.encode(), _ptr(xyz), _ptr(n_el), len(n_el), C.cast(table, _PP)), path)
