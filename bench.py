@@ -225,7 +225,8 @@ def ours(args, rank, world, local_rank):
     stream = torch.cuda.current_stream(dev)
     ctx.set_stream(stream.cuda_stream)
 
-    els, nh, q, p0 = workload(rank, args.cells)
+    # replicas: one structure per rank (seeded by the rank); --shard: one structure split over the ranks
+    els, nh, q, p0 = workload(0 if args.shard else rank, args.cells)
     n_el = np.array([len(e) for e in els], dtype=np.uint32)
     P = 3
     pairs = npairs(els)
@@ -239,6 +240,10 @@ def ours(args, rank, world, local_rank):
     p = C.c_void_p
 
     def step_device():
+        if args.shard:
+            from xns_b200 import shard
+            shard.pdf_and_debye(ctx, d_xyz, n_el, nh, BIN, 4, 2, p0, q, 0, sl, d_hist, d_I, d_pdf, rank, world)
+            return
         st = lib.xns_pdf_and_debye_device(ctx.handle, p(d_xyz.data_ptr()), n_el.ctypes.data_as(p), len(n_el), nh, BIN, 4, 2,
                                           p0, q.ctypes.data_as(p), NQ, 0, None, sl.ctypes.data_as(p), 0, 0.0,
                                           p(d_I.data_ptr()), p(d_pdf.data_ptr()), p(d_hist.data_ptr()))
@@ -295,7 +300,15 @@ def ours(args, rank, world, local_rank):
     lib.xns_calc_pdf_and_debye.argtypes = [p, p, p, C.c_uint32, C.c_uint32, C.c_double, C.c_int, C.c_int, C.c_double, p,
                                            C.c_uint32, C.c_int, p, p, C.c_int, C.c_double, p, p, p]
 
+    pin_all = torch.from_numpy(xyz).pin_memory()
+
     def step_e2e():
+        if args.shard:  # host coordinates in, the whole I(q) and PDF out on every rank
+            d_xyz.copy_(pin_all, non_blocking=True)
+            step_device()
+            pin_I.copy_(d_I, non_blocking=True)
+            pin_pdf.copy_(d_pdf, non_blocking=True)
+            return
         st = lib.xns_calc_pdf_and_debye(ctx.handle, table, n_el.ctypes.data_as(p), len(n_el), nh, BIN, 4, 2, p0,
                                         q.ctypes.data_as(p), NQ, 0, None, sl.ctypes.data_as(p), 0, 0.0,
                                         p(pin_I.data_ptr()), p(pin_pdf.data_ptr()), None)
@@ -329,14 +342,18 @@ def ours(args, rank, world, local_rank):
     lib.xns_measure_fma_peak(ctx.handle, 1, C.byref(peak))
     hist_avg = hist_ms / args.steps
     inc = pairs / (hist_avg * 1e-3) / 1e9
-    line = {"metric": METRIC, "value": job_rate(world, pairs, ms_step), "unit": "pairs/s", "n_gpus": world,
+    # pairs of the job: every rank's structure (replicas) or the one shared structure (--shard)
+    units = 1 if args.shard else world
+    par = ("one structure over %d ranks (histogram shards + NCCL all-reduce of the counts)" % world if args.shard
+           else "replicas x%d (one structure per rank)" % world)
+    line = {"metric": METRIC, "value": job_rate(units, pairs, ms_step), "unit": "pairs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None,
+            "scaling": "strong" if args.shard else "weak", "vs_baseline": None,
             "dtype": "f32 distance estimate + f64 exact re-binning near bin edges, u64 counts (histogram); integer-digit "
                      "tensor-core transform with exact sums (I(q)); f64 (PDF)",
             "data": "synthetic (seeded)",
-            "patterns_per_s": world / (ms_step * 1e-3),
-            "config": config_block(els, nh, {"parallelism": "replicas x%d (one structure per rank)" % world}, args.cells),
+            "patterns_per_s": units / (ms_step * 1e-3),
+            "config": config_block(els, nh, {"parallelism": par}, args.cells),
             "stages_ms": {"histogram": hist_avg, "pdf": pdf_ms / args.steps, "iq": iq_ms / args.steps},
             "roofline": {"kernel": "hist_window_kernel", "bound": "smem_atomic", "achieved": inc, "peak": atom_peak.value,
                          "unit": "1e9 shared-memory increments/s", "frac": inc / atom_peak.value if atom_peak.value else None,
@@ -346,7 +363,7 @@ def ours(args, rank, world, local_rank):
                          "peak_source": "measured in-process (conflict-free atomicAdd loop, xns_measure_smem_atomic_peak)",
                          "fp64_view": {"flops_per_pair": HIST_FLOPS_PER_PAIR, "peak_tflops": peak.value,
                                        "frac": HIST_FLOPS_PER_PAIR * pairs / (hist_avg * 1e-3) / 1e12 / peak.value}},
-            "e2e": {"value": job_rate(world, pairs, e2e_ms), "unit": "pairs/s", "ms_per_step": e2e_ms,
+            "e2e": {"value": job_rate(units, pairs, e2e_ms), "unit": "pairs/s", "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches), "clocks": clk}
     if world == 1 and not args.no_cpu_baseline:
@@ -721,6 +738,9 @@ def main():
     ap.add_argument("--cells2d", type=int, default=63, help="2d workload: crystallite edge in fcc cells (63: 1e6 atoms)")
     ap.add_argument("--mesh2d", type=int, default=1024, help="2d workload: q and phi points")
     ap.add_argument("--build-sites", type=int, default=200000, help="build workload: sites of the atom-list block")
+    ap.add_argument("--shard", action="store_true",
+                    help="histogram workload with N ranks: split one structure over the ranks (strong scaling) "
+                         "instead of one structure per rank")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -132,6 +132,26 @@ int xns_pdf_and_debye_device(xns_ctx *ctx, const double *xyz_dev, const uint32_t
                              const double *const *ff, const double *sl, int polar, double lambda, double *I_dev,
                              double *pdf_dev, uint64_t *hist_dev);
 
+/* ---- one structure over several GPUs ---------------------------------------------------------------- */
+
+/* One shard of calcHist (CalcFunctions.cpp:757-809): the counts of this shard's share of the atom
+ * pairs.  The plan (spatial sort, tile pairs, runs) is the whole structure's; shard s of nshard keeps
+ * every nshard-th run of its size-sorted run list and every nshard-th of the tile pairs too wide for a
+ * window, so the shares balance and the histograms of shards 0..nshard-1 add up, bin by bin, to
+ * xns_calc_hist's exactly.  Each GPU (rank) computes its shard; a sum across ranks (an NCCL all-reduce
+ * of P*nhist u64, the reference's MPI_Reduce of rij_hist, CalcFunctions.cpp:804-807) gives the
+ * histogram, from which I(q) and the PDF follow on any rank.  Host-buffer and device-buffer forms. */
+int xns_calc_hist_shard(xns_ctx *ctx, const double *const *xyz_el, const uint32_t *n_el, uint32_t nel, uint32_t nhist,
+                        double bin, uint32_t shard, uint32_t nshard, uint64_t *hist);
+int xns_hist_shard_device(xns_ctx *ctx, const double *xyz_dev, const uint32_t *n_el, uint32_t nel, uint32_t nhist,
+                          double bin, uint32_t shard, uint32_t nshard, uint64_t *hist_dev);
+/* The rest of calcPDFandDebye (CalcFunctions.cpp:912-968) on a device histogram, e.g. the sum of the
+ * shards: PDF (pdf_dev, (1+P)*nhist) and / or I(q) (I_dev, nq) as xns_pdf_and_debye_device gives them. */
+int xns_pdf_and_debye_from_hist_device(xns_ctx *ctx, const uint64_t *hist_dev, const uint32_t *n_el, uint32_t nel,
+                                       uint32_t nhist, double bin, int scenario, int pdftype, double p0, const double *q,
+                                       uint32_t nq, int source, const double *const *ff, const double *sl, int polar,
+                                       double lambda, double *I_dev, double *pdf_dev);
+
 /* ---- allocation-free entry point ------------------------------------------------------------------ */
 
 /* Histogram -> I(q) that allocates no device memory.  No counterpart in the reference: it serves

@@ -173,13 +173,31 @@ __global__ void __launch_bounds__(SCAN_THREADS) scan_kernel(const uint32_t *__re
 __global__ void cell_scatter_kernel(const double *__restrict__ X, const double *__restrict__ Y, const double *__restrict__ Z,
                                     uint32_t n, const uint32_t *__restrict__ cid, const uint32_t *__restrict__ cell_off,
                                     uint32_t *__restrict__ cursor, double *__restrict__ Xs, double *__restrict__ Ys,
-                                    double *__restrict__ Zs) {
+                                    double *__restrict__ Zs, uint32_t *__restrict__ idx) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint32_t c = cid[i];
     const uint32_t p = cell_off[c] + atomicAdd(cursor + c, 1u);
     Xs[p] = X[i];
     Ys[p] = Y[i];
     Zs[p] = Z[i];
+    if (idx) idx[p] = i;
+  }
+}
+
+// The scatter's order inside a cell depends on the atomics; a sharded plan needs the same tiles in every
+// shard, so it puts each cell's atoms back in input order (one thread per cell, insertion sort).
+__global__ void cell_order_kernel(uint32_t ncells, const uint32_t *__restrict__ cell_off, const uint32_t *__restrict__ cnt,
+                                  double *__restrict__ Xs, double *__restrict__ Ys, double *__restrict__ Zs,
+                                  uint32_t *__restrict__ idx) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells) return;
+  const uint32_t b = cell_off[c], e = b + cnt[c];
+  for (uint32_t m = b + 1; m < e; m++) {
+    const uint32_t k = idx[m];
+    const double x = Xs[m], y = Ys[m], z = Zs[m];
+    uint32_t t = m;
+    for (; t > b && idx[t - 1] > k; t--) idx[t] = idx[t - 1], Xs[t] = Xs[t - 1], Ys[t] = Ys[t - 1], Zs[t] = Zs[t - 1];
+    idx[t] = k, Xs[t] = x, Ys[t] = y, Zs[t] = z;
   }
 }
 
@@ -284,6 +302,7 @@ struct KeyParams {
   double inv_bin;
   uint32_t nhist, nbuckets, nkeys;  // key = class * nbuckets + bucket; nkeys - 1 = the wide key
   uint32_t win;                     // window bins of the counting kernel
+  uint32_t shard, nshard;           // this plan keeps the tile pairs w with w % nshard == shard
 };
 
 __device__ __forceinline__ uint32_t pair_key(const KeyParams &p, unsigned long long w, TilePair *tp) {
@@ -306,7 +325,7 @@ __global__ void pair_key_kernel(KeyParams p, uint32_t *__restrict__ kcnt) {
   for (unsigned long long w0 = blockIdx.x * (unsigned long long)blockDim.x + (threadIdx.x & ~31u); w0 < p.ntp;
        w0 += stride) {
     const unsigned long long w = w0 + lane;
-    const bool act = w < p.ntp;
+    const bool act = w < p.ntp && w % p.nshard == p.shard;
     const unsigned act_mask = __ballot_sync(0xffffffffu, act);
     if (act) {
       TilePair tp;
@@ -324,7 +343,7 @@ __global__ void pair_scatter_kernel(KeyParams p, const uint32_t *__restrict__ ko
   for (unsigned long long w0 = blockIdx.x * (unsigned long long)blockDim.x + (threadIdx.x & ~31u); w0 < p.ntp;
        w0 += stride) {
     const unsigned long long w = w0 + lane;
-    const bool act = w < p.ntp;
+    const bool act = w < p.ntp && w % p.nshard == p.shard;
     const unsigned act_mask = __ballot_sync(0xffffffffu, act);
     if (act) {
       TilePair tp;
@@ -821,6 +840,7 @@ int xns_hist_plan(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, u
   if (nel == 0) return xns_fail(ctx, XNS_ERR_ARG, "histogram: no elements");
   if (tune.win < 2 * BUCKET || tune.win > WIN_MAX || tune.win % 4 || tune.cell_target < 8)
     return xns_fail(ctx, XNS_ERR_ARG, "histogram: tuning outside its range");
+  if (tune.nshard == 0 || tune.shard >= tune.nshard) return xns_fail(ctx, XNS_ERR_ARG, "histogram: shard >= nshard");
   // classes: structure s owns P(nel_s) consecutive classes
   std::vector<ElemCls> ecls(nel);
   uint32_t C = 0;
@@ -949,9 +969,12 @@ int xns_hist_plan(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, u
   if ((st = xns_scratch(ctx, SLOT_HCELL, sizeof(uint32_t) * (4 * (size_t)ncells + 8), &vcell))) return st;
   uint32_t *d_cnt = (uint32_t *)vcell, *d_coff = d_cnt + ncells, *d_toff = d_coff + ncells, *d_cur = d_toff + ncells,
            *d_tot = d_cur + ncells;
-  if ((st = xns_scratch(ctx, SLOT_HSORT, (sizeof(double) * 3 + sizeof(uint32_t)) * (size_t)ntot, &vsort))) return st;
+  const bool ordered = tune.nshard > 1;
+  if ((st = xns_scratch(ctx, SLOT_HSORT, (sizeof(double) * 3 + sizeof(uint32_t) * (ordered ? 2 : 1)) * (size_t)ntot,
+                        &vsort)))
+    return st;
   double *Xs = (double *)vsort, *Ys = Xs + ntot, *Zs = Ys + ntot;
-  uint32_t *d_cid = (uint32_t *)(Zs + ntot);
+  uint32_t *d_cid = (uint32_t *)(Zs + ntot), *d_idx = ordered ? d_cid + ntot : nullptr;
   for (uint32_t e = 0; e < nel; e++) ebase[e] = std::min(eg[e].base, ncells - 1);
   memcpy(vh, eg.data(), sizeof(ElemGrid) * nel);
   memcpy((char *)vh + sizeof(ElemGrid) * nel, ebase.data(), sizeof(uint32_t) * nel);
@@ -965,8 +988,13 @@ int xns_hist_plan(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, u
   XNS_LAUNCHED(ctx);
   scan_kernel<<<1, SCAN_THREADS, 0, ctx->stream>>>(d_cnt, ncells, d_coff, d_toff, d_tot);
   XNS_LAUNCHED(ctx);
-  cell_scatter_kernel<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(hs.x, hs.y, hs.z, ntot, d_cid, d_coff, d_cur, Xs, Ys, Zs);
+  cell_scatter_kernel<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(hs.x, hs.y, hs.z, ntot, d_cid, d_coff, d_cur, Xs, Ys, Zs,
+                                                                  d_idx);
   XNS_LAUNCHED(ctx);
+  if (ordered) {
+    cell_order_kernel<<<(ncells + 127) / 128, 128, 0, ctx->stream>>>(ncells, d_coff, d_cnt, Xs, Ys, Zs, d_idx);
+    XNS_LAUNCHED(ctx);
+  }
   // tiles per element: the tile offsets at the element boundaries
   gather_u32_kernel<<<(nel + 255) / 256, 256, 0, ctx->stream>>>(d_toff, d_ebase, nel, d_estart);
   XNS_LAUNCHED(ctx);
@@ -1018,6 +1046,8 @@ int xns_hist_plan(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, u
   if (nkeys >= (1ull << 31)) return xns_fail(ctx, XNS_ERR_ARG, "histogram: too many classes x distance buckets");
   kp.nkeys = (uint32_t)nkeys;
   kp.win = tune.win;
+  kp.shard = tune.shard;
+  kp.nshard = tune.nshard;
   void *vk, *vl;
   if ((st = xns_scratch(ctx, SLOT_HKEY, sizeof(uint32_t) * (3 * (size_t)kp.nkeys + 8), &vk))) return st;
   uint32_t *d_kcnt = (uint32_t *)vk, *d_koff = d_kcnt + kp.nkeys, *d_kcur = d_koff + kp.nkeys, *d_ktot = d_kcur + kp.nkeys;
@@ -1036,7 +1066,9 @@ int xns_hist_plan(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, u
   // queue balances uneven classes; a CTA's u32 window counts at most 64*64*entries pairs per bin, so a
   // run stays below 2^19 entries
   std::vector<uint32_t> koff(kp.nkeys);
+  uint32_t n_list = 0;  // tile pairs in this plan's list: all of them, or this shard's share
   XNS_CUDA(ctx, cudaMemcpyAsync(koff.data(), d_koff, sizeof(uint32_t) * kp.nkeys, cudaMemcpyDeviceToHost, ctx->stream));
+  XNS_CUDA(ctx, cudaMemcpyAsync(&n_list, d_ktot, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
   XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   const uint32_t n_narrow = koff[kp.nkeys - 1];
   const uint32_t run_len =
@@ -1064,7 +1096,7 @@ int xns_hist_plan(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, u
   hp.nhist = nhist;
   hp.nranges = (uint32_t)ranges.size();
   hp.wide_begin = n_narrow;
-  hp.wide_end = (uint32_t)ntp;
+  hp.wide_end = n_list;
   hp.ranges = nullptr;
   hp.win = tune.win;
   if (!ranges.empty()) {
@@ -1124,6 +1156,57 @@ int xns_hist_set(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, un
   if ((st = xns_hist_enqueue(ctx, L))) return st;
   if ((st = xns_stage_end(ctx, STAGE_HIST))) return st;
   return xns_hist_check(ctx, L);
+}
+
+int xns_hist_device_shard(xns_ctx *ctx, const DevCoords &dc, uint32_t nhist, double bin, uint32_t shard, uint32_t nshard,
+                          unsigned long long *d_hist) {
+  HistSet hs;
+  hs.x = dc.x;
+  hs.y = dc.y;
+  hs.z = dc.z;
+  hs.el_off = dc.off_el;
+  hs.el_n = dc.n_el;
+  hs.st.push_back({0, (uint32_t)dc.n_el.size()});
+  HistTuning t;
+  t.shard = shard;
+  t.nshard = nshard;
+  HistLaunch L;
+  int st;
+  if ((st = xns_hist_plan(ctx, hs, nhist, bin, d_hist, t, &L))) return st;
+  if ((st = xns_stage_begin(ctx, STAGE_HIST))) return st;
+  if ((st = xns_hist_enqueue(ctx, L))) return st;
+  if ((st = xns_stage_end(ctx, STAGE_HIST))) return st;
+  return xns_hist_check(ctx, L);
+}
+
+extern "C" int xns_hist_shard_device(xns_ctx *ctx, const double *xyz_dev, const uint32_t *n_el, uint32_t nel, uint32_t nhist,
+                                     double bin, uint32_t shard, uint32_t nshard, uint64_t *hist_dev) {
+  if (!ctx) return XNS_ERR_ARG;
+  if (!xyz_dev || !hist_dev) return xns_fail(ctx, XNS_ERR_ARG, "hist shard: null device buffer");
+  int st;
+  DevCoords dc;
+  if ((st = xns_timer_start(ctx))) return st;
+  if ((st = xns_coords_from_device(ctx, xyz_dev, n_el, nel, &dc))) return st;
+  if ((st = xns_hist_device_shard(ctx, dc, nhist, bin, shard, nshard, (unsigned long long *)hist_dev))) return st;
+  return xns_timer_stop(ctx);
+}
+
+extern "C" int xns_calc_hist_shard(xns_ctx *ctx, const double *const *xyz_el, const uint32_t *n_el, uint32_t nel,
+                                   uint32_t nhist, double bin, uint32_t shard, uint32_t nshard, uint64_t *hist) {
+  if (!ctx) return XNS_ERR_ARG;
+  if (!hist) return xns_fail(ctx, XNS_ERR_ARG, "hist shard: null output");
+  int st;
+  DevCoords dc;
+  if ((st = xns_upload_coords(ctx, xyz_el, n_el, nel, &dc))) return st;
+  void *d_hist;
+  size_t bytes = sizeof(unsigned long long) * (size_t)xns_npairs(nel) * nhist;
+  if ((st = xns_scratch(ctx, SLOT_HIST, bytes, &d_hist))) return st;
+  if ((st = xns_timer_start(ctx))) return st;
+  if ((st = xns_hist_device_shard(ctx, dc, nhist, bin, shard, nshard, (unsigned long long *)d_hist))) return st;
+  if ((st = xns_timer_stop(ctx))) return st;
+  XNS_CUDA(ctx, cudaMemcpyAsync(hist, d_hist, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return XNS_OK;
 }
 
 int xns_hist_device(xns_ctx *ctx, const DevCoords &dc, uint32_t nhist, double bin, unsigned long long *d_hist) {

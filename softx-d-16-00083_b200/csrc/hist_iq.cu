@@ -87,6 +87,30 @@ extern "C" int xns_pdf_and_debye_device(xns_ctx *ctx, const double *xyz_dev, con
   return xns_timer_stop(ctx);
 }
 
+extern "C" int xns_pdf_and_debye_from_hist_device(xns_ctx *ctx, const uint64_t *hist_dev, const uint32_t *n_el, uint32_t nel,
+                                                  uint32_t nhist, double bin, int scenario, int pdftype, double p0,
+                                                  const double *q, uint32_t nq, int source, const double *const *ff,
+                                                  const double *sl, int polar, double lambda, double *I_dev,
+                                                  double *pdf_dev) {
+  if (!ctx) return XNS_ERR_ARG;
+  if (scenario != XNS_DEBYE_HIST && scenario != XNS_PDF_ONLY && scenario != XNS_DEBYE_PDF)
+    return xns_fail(ctx, XNS_ERR_ARG, "scenario must be Debye_hist (2), PDFonly (3) or DebyePDF (4)");
+  const bool want_iq = scenario != XNS_PDF_ONLY, want_pdf = scenario != XNS_DEBYE_HIST;
+  if (!hist_dev || !n_el || nel == 0 || (want_iq && (!I_dev || !q || nq == 0)) || (want_pdf && (!pdf_dev || !sl)))
+    return xns_fail(ctx, XNS_ERR_ARG, "pdf_and_debye_from_hist_device: missing input, output or weights");
+  int st;
+  double *d_w = nullptr;
+  if (want_iq && (st = xns_upload_weights(ctx, nel, nq, source, ff, sl, &d_w))) return st;
+  if ((st = xns_timer_start(ctx))) return st;
+  if (want_pdf &&
+      (st = xns_pdf_device(ctx, (const unsigned long long *)hist_dev, n_el, nel, nhist, bin, pdftype, p0, sl, pdf_dev)))
+    return st;
+  if (want_iq && (st = xns_hist_iq_device(ctx, (const unsigned long long *)hist_dev, n_el, nel, nhist, bin, q, nq, d_w,
+                                          polar, lambda, I_dev)))
+    return st;
+  return xns_timer_stop(ctx);
+}
+
 extern "C" int xns_calc_pdf_and_debye(xns_ctx *ctx, const double *const *xyz_el, const uint32_t *n_el, uint32_t nel,
                                       uint32_t nhist, double bin, int scenario, int pdftype, double p0, const double *q,
                                       uint32_t nq, int source, const double *const *ff, const double *sl, int polar,

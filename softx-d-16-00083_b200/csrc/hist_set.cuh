@@ -17,9 +17,13 @@ struct HistSet {
 
 // Plan parameters: mean atoms per cell of the spatial sort (sets the tile extent) and the bins of the
 // shared-memory window that slides along the distance axis (its privatisation depth).
+// shard / nshard: this plan counts only its share of the tile pairs (every nshard-th run of the
+// size-sorted run list and every nshard-th wide tile pair); the shares of shards 0..nshard-1 add up to
+// the whole histogram exactly.
 struct HistTuning {
   uint32_t cell_target = 56;
   uint32_t win = 45 * 1024 + 512;
+  uint32_t shard = 0, nshard = 1;
 };
 
 // Everything the counting kernels need, built by xns_hist_plan; the buffers it points to live in the
@@ -42,3 +46,6 @@ int xns_hist_plan(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, u
                   const HistTuning &tune, HistLaunch *L);
 int xns_hist_enqueue(xns_ctx *ctx, const HistLaunch &L);
 int xns_hist_check(xns_ctx *ctx, const HistLaunch &L);
+// One shard of a structure's histogram on device coordinates (plan, count, check).
+int xns_hist_device_shard(xns_ctx *ctx, const DevCoords &dc, uint32_t nhist, double bin, uint32_t shard, uint32_t nshard,
+                          unsigned long long *d_hist);
