@@ -321,6 +321,37 @@ int xns_build_atoms(xns_ctx *ctx, const xns_block *blocks, uint32_t nblocks, uin
 /* Copies the last build's atoms into host arrays: xyz_el[e] receives n_el[e] x y z triples. */
 int xns_copy_atoms(xns_ctx *ctx, double *const *xyz_el);
 
+/* ---- rearrangement correction ------------------------------------------------------------------------ */
+
+/* One block as RearrangementInt (CalcFunctions.cpp:469-545) reads it: the block's sites (element-sorted,
+ * Cartesian), per site the list of its neighbours read from the block's Rearrangement file
+ * (block::readRearrangement, IO.cpp:198-230: positions, global element ids), Rcorr, and
+ * coeff = Ncopy * Ncell.x * Ncell.y * Ncell.z * Nsymm as the reference forms it (unsigned int). */
+typedef struct xns_rearr_block {
+  uint32_t natom, nid;
+  uint32_t rearrangement;     /* 0: the block contributes nothing (block::rearrangement) */
+  uint32_t coeff;
+  const uint32_t *natom_el;   /* [nid] sites per block element */
+  const uint32_t *id;         /* [nid] global element index of each */
+  const double *r_atom;       /* [natom][3] */
+  const uint32_t *neighb_off; /* [natom + 1] CSR offsets into the neighbour arrays */
+  const double *neighb_r;     /* [neighb_off[natom]][3] neighbour positions */
+  const uint32_t *neighb_id;  /* [neighb_off[natom]] global element index of each neighbour */
+  double rcorr;
+} xns_rearr_block;
+
+/* RearrangementInt (CalcFunctions.cpp:469-545) on the GPU: I0 (host, in / out; nq values, or
+ * (1 + nblocks (nblocks + 1) / 2) nq with partial) is the Debye intensity the calc functions returned
+ * for ntot atoms; per block, the sinc sum over site pairs closer than each site's farthest neighbour
+ * plus Rcorr is removed and the sum over its listed neighbours added (weights ff[e][iq] or sl[e], times
+ * coeff), the polarisation factor applied as the reference applies it, and I0 renormalised by the
+ * corrected pair count N (which starts from the reference's SQR(Ntot) in unsigned int arithmetic).  With partial the reference accumulates every block into the first block's
+ * partial slot; that is kept.  FP64 throughout; terms summed in a different order than the
+ * reference's, so within FP64 rounding of it. */
+int xns_rearrangement_int(xns_ctx *ctx, double *I0, const double *q, uint32_t nq, const xns_rearr_block *blocks,
+                          uint32_t nblocks, uint32_t nel, int source, const double *const *ff, const double *sl,
+                          int partial, int polar, double lambda, uint32_t ntot);
+
 /* ---- output writers ---------------------------------------------------------------------------------- */
 
 /* The reference's text outputs, byte for byte, formatted on all host threads (no device needed).

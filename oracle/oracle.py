@@ -71,6 +71,34 @@ def _blocks(blocks):
     return arr, keep
 
 
+class _RearrStruct(C.Structure):
+    """xo_rearr_block / the harness's xr_rearr_block: the library's xns_rearr_block layout."""
+    _fields_ = [("natom", _u32), ("nid", _u32), ("rearrangement", _u32), ("coeff", _u32), ("natom_el", _p), ("id", _p),
+                ("r_atom", _p), ("neighb_off", _p), ("neighb_r", _p), ("neighb_id", _p), ("rcorr", _dbl)]
+
+
+def _rearr(fn, I0, q, blocks, nel, source, ff, sl, partial, polar, lam, ntot):
+    """calls fn (xo_ / xnsref_rearrangement_int) on a copy of I0; blocks: objects with the attributes of
+    xns_b200.structure.RearrBlock"""
+    I = np.array(I0, dtype=np.float64, copy=True)
+    q = _f64(q)
+    arr = (_RearrStruct * max(1, len(blocks)))()
+    keep = []
+    for i, b in enumerate(blocks):
+        a = [np.ascontiguousarray(b.natom_el, dtype=np.uint32), np.ascontiguousarray(b.id, dtype=np.uint32),
+             _f64(b.r_atom), np.ascontiguousarray(b.neighb_off, dtype=np.uint32), _f64(b.neighb_r),
+             np.ascontiguousarray(b.neighb_id, dtype=np.uint32)]
+        keep.append(a)
+        s = arr[i]
+        s.natom, s.nid, s.rearrangement, s.coeff = len(a[2]), len(a[1]), int(b.rearrangement), int(b.coeff)
+        s.natom_el, s.id, s.r_atom, s.neighb_off, s.neighb_r, s.neighb_id = [x.ctypes.data_as(_p) for x in a]
+        s.rcorr = float(b.rcorr)
+    ffm = _ff(ff, len(q))
+    fn(_ptr(I), _ptr(q), len(q), C.cast(arr, _p), len(blocks), nel, source, _ptr(ffm), _ptr(_f64(sl)), int(partial),
+       int(polar), lam, ntot)
+    return I
+
+
 def _split(ptr, n_el, free):
     tot = int(np.sum(n_el))
     flat = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(_dbl)), shape=(max(tot, 1) * 3,))[:tot * 3].copy()
@@ -98,11 +126,15 @@ class Oracle:
         L.xo_int_1d_hist.argtypes = [_p, _p, _u32, _u32, _dbl, _p, _u32, _int, _p, _p, _int, _dbl, _p]
         L.xo_pdf.argtypes = [_p, _p, _u32, _u32, _dbl, _int, _dbl, _p, _p]
         L.xo_int_2d.argtypes = [_p, _p, _u32, _p, _u32, _u32, _p, _p, _p, _u32, _dbl, _int, _p, _p, _int, _p, _p]
+        L.xo_rearrangement_int.argtypes = [_p, _p, _u32, _p, _u32, _u32, _int, _p, _p, _int, _int, _dbl, _u32]
         L.xo_build_atoms.argtypes = [_p, _u32, _u32, C.c_uint64, _p, _p]
         L.xo_build_atoms.restype = _p
         L.xo_free.argtypes = [_p]
         L.xo_philox.argtypes = [_p, _p, _p]
         L.xo_amp_plane.argtypes = [_p, _p, _u32, _dbl, _dbl, _u32, _dbl, _dbl, _u32, _int, _p, _p, _p]
+
+    def rearrangement_int(self, I0, q, blocks, nel, source, ff=None, sl=None, partial=False, polar=False, lam=0.0, ntot=0):
+        return _rearr(self.lib.xo_rearrangement_int, I0, q, blocks, nel, source, ff, sl, partial, polar, lam, ntot)
 
     def philox(self, ctr, key):
         c, k, o = np.array(ctr, dtype=np.uint32), np.array(key, dtype=np.uint32), np.zeros(4, dtype=np.uint32)
@@ -206,6 +238,7 @@ class Reference:
         L.xnsref_calc_atoms.argtypes = [_p, _u32, _u32, _p, _p]
         L.xnsref_calc_atoms.restype = _p
         L.xnsref_free.argtypes = [_p]
+        L.xnsref_rearrangement_int.argtypes = [_p, _p, _u32, _p, _u32, _u32, _int, _p, _p, _int, _int, _dbl, _u32]
         L.xnsref_print_i.argtypes = [C.c_char_p, _p, _p, _u32, _u32]
         L.xnsref_print_partial_i.argtypes = [C.c_char_p, _p, _p, _u32, _u32, _u32]
         L.xnsref_print_i2.argtypes = [C.c_char_p, _p, _u32, _u32, _u32]
@@ -224,6 +257,9 @@ class Reference:
                                                 _dbl, _int, _p, _p]
         L.xnsref_calc_int_2d.argtypes = [_p, _p, _u32, _p, _u32, _u32, _p, _p, _p, _u32, _dbl, _int, _p, _p, _int, _int,
                                          _p, _p]
+
+    def rearrangement_int(self, I0, q, blocks, nel, source, ff=None, sl=None, partial=False, polar=False, lam=0.0, ntot=0):
+        return _rearr(self.lib.xnsref_rearrangement_int, I0, q, blocks, nel, source, ff, sl, partial, polar, lam, ntot)
 
     # the reference's writers: name is the path prefix; they return the reference's status
     def print_i(self, name, q, I, source):

@@ -22,6 +22,7 @@ void calcIntPartialDebye(double **I, const config *cfg, const unsigned int *Nato
 void calcHist(unsigned long long int **rij_hist, const vector<vect3d<double> > *ra, const unsigned int *NatomEl, unsigned int Nel, unsigned int Nhist, double bin, int NumOMPthreads);
 void calcInt1DHist(double **I, unsigned long long int *rij_hist, const unsigned int *NatomEl, unsigned int Nel, const config *cfg, vector<double *> FF, vector<double> SL, const double *q, unsigned int Ntot, int NumOMPthreads);
 void calcPDFandDebye(double **I, double **PDF, const config *cfg, const unsigned int *NatomEl, const vector<vect3d<double> > *ra, vector<double *> FF, vector<double> SL, const double *q, unsigned int Ntot, int NumOMPthreads);
+void RearrangementInt(double *I0, const double *q, const config *cfg, const block *Block, vector<double *> FF, vector<double> SL, unsigned int Ntot);
 int printI(const double *I, unsigned int Nq, const double *q, string name, unsigned int source);
 int printI2(const double *const *I2D, unsigned int Nq, unsigned int Nfi, string name, unsigned int source);
 int printPartialI(const double *I, unsigned int Nq, const double *q, string name, unsigned int source, unsigned int Nblocks);
@@ -374,6 +375,59 @@ int xnsref_print_atoms(const char *name, const double *xyz, const uint32_t *n_el
   int r = printAtoms(ra, string(name), id_map(names, nel), total(n_el, nel));
   delete[] ra;
   return r;
+}
+
+// RearrangementInt, CalcFunctions.cpp:469-545, on reference blocks built from the library's
+// xns_rearr_block layout.  ff: nel x nq row-major (X-ray); I0 in / out.
+struct xr_rearr_block {
+  uint32_t natom, nid, rearrangement, coeff;
+  const uint32_t *natom_el, *id;
+  const double *r_atom;
+  const uint32_t *neighb_off;
+  const double *neighb_r;
+  const uint32_t *neighb_id;
+  double rcorr;
+};
+
+int xnsref_rearrangement_int(double *I0, const double *q, uint32_t nq, const xr_rearr_block *blocks, uint32_t nblocks,
+                             uint32_t nel, int source, const double *ff, const double *sl, int partial, int polar,
+                             double lambda, uint32_t ntot) {
+  config cfg;
+  base_config(&cfg, nel, q, nq, source, polar, lambda);
+  cfg.Nblocks = nblocks;
+  cfg.calcPartialIntensity = partial != 0;
+  vector<double *> FF;
+  vector<double> SL;
+  weights(nel, nq, ff, sl, &FF, &SL);
+  block *B = new block[nblocks];
+  for (uint32_t b = 0; b < nblocks; b++) {
+    const xr_rearr_block &x = blocks[b];
+    // coeff = Ncopy * Ncell.x * Ncell.y * Ncell.z * Nsymm (:482): carried by Ncopy, the rest 1
+    B[b].Natom = x.natom;
+    B[b].Nsymm = 1;
+    B[b].Ncopy = x.coeff;
+    B[b].rearrangement = x.rearrangement != 0;
+    B[b].create();
+    B[b].Nid = x.nid;
+    B[b].id = new unsigned int[x.nid];
+    for (uint32_t k = 0; k < x.nid; k++) B[b].id[k] = x.id[k], B[b].NatomEl.push_back(x.natom_el[k]);
+    for (uint32_t i = 0; i < x.natom; i++) B[b].rAtom[i].assign(x.r_atom[3 * i], x.r_atom[3 * i + 1], x.r_atom[3 * i + 2]);
+    B[b].Rcorr = x.rcorr;
+    if (B[b].rearrangement) {
+      B[b].idNeighb = new vector<unsigned>[x.natom];
+      for (uint32_t i = 0; i < x.natom; i++)
+        for (uint32_t k = x.neighb_off[i]; k < x.neighb_off[i + 1]; k++) {
+          B[b].rAtomNeighb[i].push_back(vect3d<double>(x.neighb_r[3 * k], x.neighb_r[3 * k + 1], x.neighb_r[3 * k + 2]));
+          B[b].idNeighb[i].push_back(x.neighb_id[k]);
+        }
+    }
+  }
+  {
+    Quiet quiet;
+    RearrangementInt(I0, q, &cfg, B, FF, SL, ntot);
+  }
+  delete[] B;
+  return 0;
 }
 
 }  // extern "C"

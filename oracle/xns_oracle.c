@@ -643,3 +643,86 @@ double *xo_build_atoms(const xo_block *blocks, uint32_t nblocks, uint32_t nel, u
   free(out);
   return xyz;
 }
+
+/* ---- rearrangement correction ---------------------------------------------------------------- */
+
+void xo_rearrangement_int(double *I0, const double *q, uint32_t nq, const xo_rearr_block *blocks, uint32_t nblocks,
+                          uint32_t nel, int source, const double *ff, const double *sl, int partial, int polar,
+                          double lambda, uint32_t ntot) {
+  (void)nel;
+  long long N = (long long)(unsigned int)(ntot * ntot); /* SQR(Ntot) in unsigned int, :471 */
+  uint32_t nint = partial ? (nblocks + 1) * nq : nq;
+  double *I = (double *)calloc(nint, sizeof(double)), *Itemp = (double *)malloc(nq * sizeof(double));
+#define XO_W(e, iq) (source == XO_XRAY ? ff[(size_t)(e) * nq + (iq)] : sl[e])
+  for (uint32_t iB = 0; iB < nblocks; iB++) {
+    const xo_rearr_block *b = &blocks[iB];
+    uint32_t iqST = partial ? nq : 0; /* every block writes the first slot, :478-479 */
+    if (!b->rearrangement) continue;
+    unsigned int coeff = b->coeff;
+    uint32_t ibegin = 0;
+    for (uint32_t iEl = 0; iEl < b->nid; iEl++) {
+      uint32_t jbegin = 0, id = b->id[iEl];
+      for (uint32_t jEl = 0; jEl < b->nid; jEl++) {
+        uint32_t jd = b->id[jEl];
+        for (uint32_t iq = 0; iq < nq; iq++) Itemp[iq] = 0;
+        for (uint32_t ia = ibegin; ia < ibegin + b->natom_el[iEl]; ia++) {
+          const double *ri = b->r_atom + 3 * ia;
+          double rmax2 = 0; /* Rmax2, :244-250 */
+          for (uint32_t k = b->neighb_off[ia]; k < b->neighb_off[ia + 1]; k++) {
+            const double *rn = b->neighb_r + 3 * k;
+            double dx = ri[0] - rn[0], dy = ri[1] - rn[1], dz = ri[2] - rn[2];
+            double d2 = dx * dx + dy * dy + dz * dz;
+            rmax2 = rmax2 > d2 ? rmax2 : d2;
+          }
+          rmax2 = rmax2 + b->rcorr * b->rcorr;
+          for (uint32_t ja = jbegin; ja < jbegin + b->natom_el[jEl]; ja++) {
+            const double *rj = b->r_atom + 3 * ja;
+            double dx = ri[0] - rj[0], dy = ri[1] - rj[1], dz = ri[2] - rj[2];
+            double rij2 = dx * dx + dy * dy + dz * dz;
+            if ((rij2 < rmax2) && (rij2 > 0.000001)) {
+              N -= coeff;
+              double rij = sqrt(rij2);
+              for (uint32_t iq = 0; iq < nq; iq++) {
+                double qrij = rij * q[iq];
+                Itemp[iq] += sin(qrij) / (qrij + 0.00000001);
+              }
+            }
+          }
+        }
+        for (uint32_t iq = 0; iq < nq; iq++) I[iqST + iq] -= (coeff * XO_W(id, iq) * XO_W(jd, iq)) * Itemp[iq];
+        jbegin += b->natom_el[jEl];
+      }
+      for (uint32_t ia = ibegin; ia < ibegin + b->natom_el[iEl]; ia++) {
+        const double *ri = b->r_atom + 3 * ia;
+        for (uint32_t k = b->neighb_off[ia]; k < b->neighb_off[ia + 1]; k++) {
+          const double *rn = b->neighb_r + 3 * k;
+          uint32_t idN = b->neighb_id[k];
+          double dx = ri[0] - rn[0], dy = ri[1] - rn[1], dz = ri[2] - rn[2];
+          double rij = sqrt(dx * dx + dy * dy + dz * dz);
+          N += coeff;
+          for (uint32_t iq = 0; iq < nq; iq++) {
+            double qrij = rij * q[iq];
+            I[iqST + iq] += (coeff * XO_W(id, iq) * XO_W(idN, iq)) * sin(qrij) / (qrij + 0.00000001);
+          }
+        }
+      }
+      ibegin += b->natom_el[iEl];
+    }
+  }
+#undef XO_W
+  if (partial) {
+    uint32_t iqST = nq;
+    for (uint32_t iB = 0; iB < nblocks; iB++, iqST += nq) {
+      uint32_t i0qST = nq * (1 + iB * (2 * nblocks - iB + 1) / 2);
+      if (polar) polar_1d(I + iqST, q, lambda, nq);
+      for (uint32_t iq = 0; iq < nq; iq++) {
+        I[iq] += I[iqST + iq];
+        I0[i0qST + iq] = (I0[i0qST + iq] * ntot + I[iqST + iq]) / sqrt((double)N);
+      }
+    }
+  } else if (polar)
+    polar_1d(I, q, lambda, nq);
+  for (uint32_t iq = 0; iq < nq; iq++) I0[iq] = (I0[iq] * ntot + I[iq]) / sqrt((double)N);
+  free(I);
+  free(Itemp);
+}

@@ -94,6 +94,23 @@ double *xo_build_atoms(const xo_block *blocks, uint32_t nblocks, uint32_t nel, u
                        uint32_t *n_all);
 void xo_free(void *p);
 
+/* One block for RearrangementInt; the same layout as the library's xns_rearr_block. */
+typedef struct xo_rearr_block {
+  uint32_t natom, nid, rearrangement, coeff;
+  const uint32_t *natom_el, *id;
+  const double *r_atom;
+  const uint32_t *neighb_off;
+  const double *neighb_r;
+  const uint32_t *neighb_id;
+  double rcorr;
+} xo_rearr_block;
+
+/* RearrangementInt (CalcFunctions.cpp:469-545) in the reference's loop order and grouping.  ff: nel x nq
+ * row-major (X-ray) or NULL; sl: nel (neutron).  I0 in / out as the reference's I. */
+void xo_rearrangement_int(double *I0, const double *q, uint32_t nq, const xo_rearr_block *blocks, uint32_t nblocks,
+                          uint32_t nel, int source, const double *ff, const double *sl, int partial, int polar,
+                          double lambda, uint32_t ntot);
+
 #ifdef __cplusplus
 }
 #endif

@@ -90,6 +90,7 @@ lib.xns_binning_features.argtypes = [_p, _p, _u32, _p]
 lib.xns_binning_correction.argtypes = [_p, _p, _p, _u32, _dbl, _p, _u32, _dbl, _p]
 lib.xns_build_atoms.argtypes = [_p, _p, _u32, _u32, C.c_uint64, _p, _p, C.POINTER(_p)]
 lib.xns_copy_atoms.argtypes = [_p, _PP]
+lib.xns_rearrangement_int.argtypes = [_p, _p, _p, _u32, _p, _u32, _u32, _int, _PP, _p, _int, _int, _dbl, _u32]
 lib.xns_write_i.argtypes = [C.c_char_p, _p, _p, _u32]
 lib.xns_write_i2.argtypes = [C.c_char_p, _p, _u32, _u32]
 lib.xns_write_pdf.argtypes = [C.c_char_p, _p, _u32, _dbl, _int]
@@ -312,6 +313,19 @@ class Context:
         table = (_p * max(1, len(out)))(*[o.ctypes.data_as(_p) for o in out])
         self._check(lib.xns_copy_atoms(self._h, C.cast(table, _PP)))
         return out
+
+    def rearrangement_int(self, I0, q, blocks, nel, source, ff=None, sl=None, partial=False, polar=False, lam=0.0,
+                          ntot=0):
+        """RearrangementInt on the GPU for a list of structure.RearrBlock; returns the corrected copy of I0."""
+        from .structure import rearr_block_array
+        I = np.array(I0, dtype=np.float64, copy=True)
+        q = _f64(q)
+        arr, keep = rearr_block_array(blocks)
+        ffa, fft = _rows(ff, len(q))
+        self._check(lib.xns_rearrangement_int(self._h, _ptr(I), _ptr(q), len(q), C.cast(arr, _p), len(blocks), nel, source,
+                                              fft, _ptr(_f64(sl)), int(partial), int(polar), lam, ntot))
+        del keep, ffa
+        return I
 
     # -- calc functions --------------------------------------------------------------------------
     def calc_hist(self, elements, nhist, bin):

@@ -1,9 +1,11 @@
-"""Structure blocks for the GPU builder (xns_build_atoms).
+"""Structure blocks for the GPU builder (xns_build_atoms) and the rearrangement correction
+(xns_rearrangement_int).
 
 Block mirrors the fields of the reference's block class (typedefs.h:198-278) that block::calcAtoms
 (CalcFunctions.cpp:251-392) reads, after the XML reader prepared them (ReadXML.cpp:254-323): site and
 symmetry coordinates Cartesian, sites sorted by element, copy rotations as matrices.  Block.crystal
 does that preparation for the common case of a unit cell given in fractional coordinates.
+RearrBlock holds what RearrangementInt (CalcFunctions.cpp:469-545) reads of a block.
 """
 import ctypes as C
 
@@ -112,5 +114,49 @@ def block_array(blocks):
     keep = []
     for i, b in enumerate(blocks):
         arr[i], k = b.as_struct()
+        keep.append(k)
+    return arr, keep
+
+
+class RearrBlockStruct(C.Structure):
+    """struct xns_rearr_block (include/xns_b200.h)."""
+    _fields_ = [("natom", _u32), ("nid", _u32), ("rearrangement", _u32), ("coeff", _u32), ("natom_el", _p), ("id", _p),
+                ("r_atom", _p), ("neighb_off", _p), ("neighb_r", _p), ("neighb_id", _p), ("rcorr", _dbl)]
+
+
+class RearrBlock:
+    """A block as RearrangementInt (CalcFunctions.cpp:469-545) reads it: sites (natom x 3, element-sorted),
+    natom_el, global element ids, per site a list of (x, y, z, global element) neighbours from the
+    block's Rearrangement file, Rcorr, and coeff = Ncopy * Ncell.x * Ncell.y * Ncell.z * Nsymm."""
+
+    def __init__(self, r_atom, natom_el, id, neighbours, rcorr, coeff, rearrangement=True):
+        self.r_atom = _f64(r_atom, (-1, 3))
+        self.natom_el = np.ascontiguousarray(natom_el, dtype=np.uint32)
+        self.id = np.ascontiguousarray(id, dtype=np.uint32)
+        if len(neighbours) != len(self.r_atom):
+            raise ValueError("RearrBlock: one neighbour list per site")
+        self.neighb_off = np.ascontiguousarray(np.concatenate([[0], np.cumsum([len(n) for n in neighbours])]),
+                                               dtype=np.uint32)
+        flat = [t for n in neighbours for t in n]
+        self.neighb_r = _f64([t[:3] for t in flat] if flat else np.zeros((0, 3)), (-1, 3))
+        self.neighb_id = np.ascontiguousarray([int(t[3]) for t in flat], dtype=np.uint32)
+        self.rcorr = float(rcorr)
+        self.coeff = int(coeff)
+        self.rearrangement = bool(rearrangement)
+
+    def as_struct(self, struct=RearrBlockStruct):
+        s = struct()
+        s.natom, s.nid, s.rearrangement, s.coeff = len(self.r_atom), len(self.id), int(self.rearrangement), self.coeff
+        keep = [self.natom_el, self.id, self.r_atom, self.neighb_off, self.neighb_r, self.neighb_id]
+        s.natom_el, s.id, s.r_atom, s.neighb_off, s.neighb_r, s.neighb_id = [a.ctypes.data_as(_p) for a in keep]
+        s.rcorr = self.rcorr
+        return s, keep
+
+
+def rearr_block_array(blocks, struct=RearrBlockStruct):
+    arr = (struct * max(1, len(blocks)))()
+    keep = []
+    for i, b in enumerate(blocks):
+        arr[i], k = b.as_struct(struct)
         keep.append(k)
     return arr, keep
