@@ -211,6 +211,82 @@ def reference_arm(args, rank, world):
     return 0
 
 
+def reference_workload_arm(args, rank):
+    """--impl reference for the one-GPU workloads: the reference's own CPU code for that workload's
+    path (oracle/_ref, else the oracle port) on a bounded sample of the workload, all host cores where
+    the reference is parallel; metric and unit of our line for that workload."""
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "softx-d-16-00083_b200"))
+    import oracle as orc
+    from xns_b200 import synth
+    cores = os.cpu_count() or 1
+    try:
+        R, kind = orc.Reference(threads=cores), "reference"
+    except FileNotFoundError:
+        R, kind = orc.Oracle(), "port"
+    w = args.workload
+    if w == "debye":
+        els = synth.fcc_sphere(n=5000, a=4.078, sigma=0.05, seed=0)
+        q = synth.q_mesh(0.1, 10.0, 1024)
+        m = 1500
+        sub = [els[0][:m]]
+        units = m * (m - 1) // 2
+        step = lambda: R.int_debye(sub, q, 0, sl=[7.63])  # noqa: E731
+        metric, unit = "atom-pairs/s", "pairs/s"
+        sample = "calcIntDebye on the first %d atoms of the 5000-atom sphere, 1024 q, %d threads" % (m, cores)
+    elif w == "2d":
+        els = synth.fcc_crystallite(cells=args.cells2d, a=3.61, subst=0.05, seed=0)
+        n = sum(len(e) for e in els)
+        q = synth.q_mesh(0.05, 8.0, args.mesh2d)
+        ff = synth.ff_on_mesh(synth.ff_coefficients(2, seed=3), q)
+        rows, nfi = cores, 64
+        units = n * rows * nfi
+        step = lambda: R.int_2d(els, q[:rows], nfi, [0, 0, 0], [0, 0, 0], [1, 1, 1], 5, 0.01, 1,  # noqa: E731
+                                ff=ff[:, :rows])
+        metric, unit = "(atom, q-point) terms/s", "terms/s"
+        sample = "calcInt2D on %d q rows x %d phi, all %d atoms, %d threads" % (rows, nfi, n, cores)
+    elif w == "batch":
+        structs, ns, _ = synth.sphere_ensemble(count=args.batch_count, seed=0)
+        small = [s for s, n in zip(structs, ns) if n < 6000][:4]
+        q = synth.q_mesh(0.1, 25.0, 4096)
+
+        def step():
+            for st in small:
+                nh = synth.hist_size(st, 0.001)
+                R.pdf_and_debye(st, nh, 0.001, 2, 2, 0.0, q, 0, sl=[7.63])
+        units = len(small)
+        metric, unit = "patterns/s", "patterns/s"
+        sample = ("calcPDFandDebye (Debye_hist) on the %d smallest-index spheres under 6000 atoms of the ensemble "
+                  "(%s atoms), 4096 q, %d threads" % (len(small), ",".join(str(sum(len(e) for e in st)) for st in small),
+                                                      cores))
+    elif w == "build":
+        m = 20000
+        blk = synth.atom_file_block(m)
+        units = m * (m - 1) // 2
+        step = (lambda: R.calc_atoms([blk], 2)) if kind == "reference" else (lambda: R.build_atoms([blk], 2, 1))
+        metric, unit, cores = "site pairs/s (structure build)", "pairs/s", 1
+        sample = "block::calcAtoms on an atom-list block of %d sites (single-threaded in the reference)" % m
+    else:
+        raise ValueError(w)
+    for _ in range(args.warmup):
+        step()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = (time.perf_counter() - t) / args.steps
+    value = units / dt
+    line = {"metric": metric, "value": value, "unit": unit, "impl": "reference", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": w, "sample": sample},
+            "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
 # ---- our arm --------------------------------------------------------------------------------------
 def ours(args, rank, world, local_rank):
     import ctypes as C
@@ -754,6 +830,8 @@ def main():
     if args.workload == "build" and args.impl == "ours":
         return build_workload(args)
     if args.impl == "reference":
+        if args.workload != "histogram":
+            return reference_workload_arm(args, rank)
         return reference_arm(args, rank, world)
     if world > 1:
         import datetime
