@@ -145,6 +145,15 @@ int xns_calc_hist_shard(xns_ctx *ctx, const double *const *xyz_el, const uint32_
                         double bin, uint32_t shard, uint32_t nshard, uint64_t *hist);
 int xns_hist_shard_device(xns_ctx *ctx, const double *xyz_dev, const uint32_t *n_el, uint32_t nel, uint32_t nhist,
                           double bin, uint32_t shard, uint32_t nshard, uint64_t *hist_dev);
+/* One shard of calcIntDebye / calcIntPartialDebye (CalcFunctions.cpp:547-756): the intensity of the
+ * tile pairs w with w % nshard == shard, the self term (sum of N_e w_e^2) on shard 0 only, normalised
+ * and polarised as the whole.  The outputs of shards 0..nshard-1 add up to xns_calc_int_debye's /
+ * xns_calc_int_partial_debye's (up to FP64 summation order): an all-reduce of nq (or (1 + parts) nq)
+ * doubles across ranks, the reference's MPI_Reduce of Itemp (CalcFunctions.cpp:613, :729).
+ * n_el_block: as xns_calc_int_partial_debye, or NULL with nblocks = 1. */
+int xns_calc_int_debye_shard(xns_ctx *ctx, const double *const *xyz_el, const uint32_t *n_el, uint32_t nel, uint32_t nblocks,
+                             const uint32_t *n_el_block, const double *q, uint32_t nq, int source, const double *const *ff,
+                             const double *sl, int polar, double lambda, uint32_t shard, uint32_t nshard, double *I);
 /* The rest of calcPDFandDebye (CalcFunctions.cpp:912-968) on a device histogram, e.g. the sum of the
  * shards: PDF (pdf_dev, (1+P)*nhist) and / or I(q) (I_dev, nq) as xns_pdf_and_debye_device gives them. */
 int xns_pdf_and_debye_from_hist_device(xns_ctx *ctx, const uint64_t *hist_dev, const uint32_t *n_el, uint32_t nel,

@@ -74,8 +74,11 @@ struct AtomPairSrc {
 }  // namespace
 
 // Debye on device coordinates.  out (device): [total | parts] ((1+nparts)*nq when nblocks > 1).
+// shard / nshard: only the tile pairs w with w % nshard == shard, and the self term on shard 0 only, so
+// that the outputs of shards 0..nshard-1 add up to the whole (the epilogue is affine in the sums).
 static int debye_device(xns_ctx *ctx, const DevCoords &dc, uint32_t nblocks, const uint32_t *n_el_block, const double *q,
-                        uint32_t nq, const double *d_w, int polar, double lambda, double *d_out) {
+                        uint32_t nq, const double *d_w, int polar, double lambda, double *d_out, uint32_t shard = 0,
+                        uint32_t nshard = 1) {
   const uint32_t nel = (uint32_t)dc.n_el.size();
   const uint32_t P = xns_npairs(nel);
   const uint32_t nparts = nblocks * (nblocks + 1) / 2;
@@ -119,21 +122,24 @@ static int debye_device(xns_ctx *ctx, const DevCoords &dc, uint32_t nblocks, con
   p.nq = nq;
   p.ncls = nparts * P;
   p.ntiles = ntiles;
+  p.shard = shard;
+  p.nshard = nshard;
   if (!uniform && (st = sinc_upload_q(ctx, q, nq, &p.q))) return st;
   AtomPairSrc src{dc.x, dc.y, dc.z, d_sp, (int)sched.size()};
   int grid = 0;
   if ((st = xns_stage_begin(ctx, STAGE_DEBYE))) return st;
   if ((st = run_sinc(ctx, p, src, sizeof(double) * 3 * (DB_TI + DB_TJ), uniform, &grid))) return st;
   if ((st = sinc_epilogue(ctx, grid, p.ncls, nel, nblocks, n_el_block, q, nq, uniform, q0, dq, d_w, dc.ntot, polar, lambda,
-                          d_out)))
+                          d_out, nullptr, true, shard == 0)))
     return st;
   return xns_stage_end(ctx, STAGE_DEBYE);
 }
 
 static int debye_host(xns_ctx *ctx, const double *const *xyz_el, const uint32_t *n_el, uint32_t nel, uint32_t nblocks,
                       const uint32_t *n_el_block, const double *q, uint32_t nq, int source, const double *const *ff,
-                      const double *sl, int polar, double lambda, double *I) {
+                      const double *sl, int polar, double lambda, double *I, uint32_t shard = 0, uint32_t nshard = 1) {
   if (!ctx) return XNS_ERR_ARG;
+  if (nshard == 0 || shard >= nshard) return xns_fail(ctx, XNS_ERR_ARG, "Debye: shard >= nshard");
   if (!q || !I || nq == 0) return xns_fail(ctx, XNS_ERR_ARG, "Debye: null q / I or nq == 0");
   int st;
   DevCoords dc;
@@ -151,7 +157,8 @@ static int debye_host(xns_ctx *ctx, const double *const *xyz_el, const uint32_t 
     n_el_block = neb_single.data();
   }
   if ((st = xns_timer_start(ctx))) return st;
-  if ((st = debye_device(ctx, dc, nblocks, n_el_block, q, nq, d_w, polar, lambda, (double *)d_out))) return st;
+  if ((st = debye_device(ctx, dc, nblocks, n_el_block, q, nq, d_w, polar, lambda, (double *)d_out, shard, nshard)))
+    return st;
   if ((st = xns_timer_stop(ctx))) return st;
   XNS_CUDA(ctx, cudaMemcpyAsync(I, d_out, sizeof(double) * nout, cudaMemcpyDeviceToHost, ctx->stream));
   XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -172,4 +179,15 @@ extern "C" int xns_calc_int_partial_debye(xns_ctx *ctx, const double *const *xyz
   if (nblocks == 0 || !n_el_block) return xns_fail(ctx, XNS_ERR_ARG, "partial Debye: nblocks == 0 or null n_el_block");
   return debye_host(ctx, xyz_el, n_el, nel, nblocks, nblocks == 1 ? nullptr : n_el_block, q, nq, source, ff, sl, polar,
                     lambda, I);
+}
+
+extern "C" int xns_calc_int_debye_shard(xns_ctx *ctx, const double *const *xyz_el, const uint32_t *n_el, uint32_t nel,
+                                        uint32_t nblocks, const uint32_t *n_el_block, const double *q, uint32_t nq,
+                                        int source, const double *const *ff, const double *sl, int polar, double lambda,
+                                        uint32_t shard, uint32_t nshard, double *I) {
+  if (!ctx) return XNS_ERR_ARG;
+  if (nblocks == 0 || (nblocks > 1 && !n_el_block))
+    return xns_fail(ctx, XNS_ERR_ARG, "Debye shard: nblocks == 0 or null n_el_block");
+  return debye_host(ctx, xyz_el, n_el, nel, nblocks, nblocks == 1 ? nullptr : n_el_block, q, nq, source, ff, sl, polar,
+                    lambda, I, shard, nshard);
 }

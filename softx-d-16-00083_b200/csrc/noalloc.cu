@@ -184,7 +184,7 @@ extern "C" int xns_int_1d_hist_noalloc(const uint64_t *hist_dev, const uint32_t 
   }
   if (cudaGetLastError() != cudaSuccess) return XNS_ERR_CUDA;
   sinc_epilogue_kernel<<<(nq + 127) / 128, 128, 0, s>>>(partial, (int)grid, P, nel, 1, 1, tab, tab + P, w, tab + 2 * P, q0, dq,
-                                                        uniform ? nullptr : dqm, nq, ntot, polar, lambda, 1, I_dev);
+                                                        uniform ? nullptr : dqm, nq, ntot, polar, lambda, 1, 1, I_dev);
   if (cudaGetLastError() != cudaSuccess) return XNS_ERR_CUDA;
   return XNS_OK;
 }

@@ -9,7 +9,7 @@ __global__ void sinc_epilogue_kernel(const double *__restrict__ partial, int gri
                                      const uint32_t *__restrict__ pair_b, const double *__restrict__ w,
                                      const uint32_t *__restrict__ n_el_block, double q0, double dq,
                                      const double *__restrict__ qmesh, uint32_t nq, uint32_t ntot, int polar, double lambda,
-                                     int over_q, double *__restrict__ out) {
+                                     int over_q, int self_term, double *__restrict__ out) {
   const uint32_t iq = blockIdx.x * blockDim.x + threadIdx.x;
   if (iq >= nq) return;
   const uint32_t P = nel * (nel + 1) / 2;
@@ -31,7 +31,7 @@ __global__ void sinc_epilogue_kernel(const double *__restrict__ partial, int gri
         if (over_q) S = (q != 0.0) ? S / q : 0.0;  // sin(0)/(0 + 1e-8) = 0 in the reference
         I += S * w[(size_t)pair_a[t] * nq + iq] * w[(size_t)pair_b[t] * nq + iq] * 2.;
       }
-      if (u == v)
+      if (u == v && self_term)
         for (uint32_t e = 0; e < nel; e++) {
           double we = w[(size_t)e * nq + iq];
           I += n_el_block[e * nblocks + u] * (we * we);
@@ -58,7 +58,7 @@ int sinc_upload_q(xns_ctx *ctx, const double *q, uint32_t nq, const double **d_q
 
 int sinc_epilogue(xns_ctx *ctx, int grid, uint32_t ncls, uint32_t nel, uint32_t nblocks, const uint32_t *n_el_block,
                   const double *q, uint32_t nq, bool uniform, double q0, double dq, const double *d_w, uint32_t ntot,
-                  int polar, double lambda, double *d_out, const double *partial, bool over_q) {
+                  int polar, double lambda, double *d_out, const double *partial, bool over_q, bool self_term) {
   const uint32_t P = xns_npairs(nel);
   const size_t nu32 = 2 * (size_t)P + (size_t)nel * nblocks;
   void *aux, *h;
@@ -82,7 +82,8 @@ int sinc_epilogue(xns_ctx *ctx, int grid, uint32_t ncls, uint32_t nel, uint32_t 
   if (!partial) partial = (const double *)ctx->slot_ptr[SLOT_PARTIAL];
   sinc_epilogue_kernel<<<(nq + 127) / 128, 128, 0, ctx->stream>>>(partial, grid, ncls,
                                                                   nel, nparts, nblocks, d_pa, d_pa + P, d_w, d_pa + 2 * P,
-                                                                  q0, dq, d_q, nq, ntot, polar, lambda, over_q, d_out);
+                                                                  q0, dq, d_q, nq, ntot, polar, lambda, over_q, self_term,
+                                                                  d_out);
   XNS_LAUNCHED(ctx);
   return XNS_OK;
 }

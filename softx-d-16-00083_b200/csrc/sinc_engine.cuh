@@ -73,6 +73,7 @@ struct SincParams {
   uint32_t ncls;
   unsigned long long ntiles;
   double *partial;    // [gridDim.x][ncls][nq] FP64, zeroed
+  uint32_t shard = 0, nshard = 1;  // this launch sums the tiles w with w % nshard == shard
 };
 
 // Shared memory: [M][SE_THREADS] FP64 totals (one column per thread), then SE_TILE records, then the
@@ -98,7 +99,8 @@ __global__ void __launch_bounds__(SE_THREADS, 3) sinc_tiles_kernel(SincParams p,
   }
 
   int cur = -1;
-  for (unsigned long long w = blockIdx.x; w < p.ntiles; w += gridDim.x) {
+  for (unsigned long long w = p.shard + (unsigned long long)p.nshard * blockIdx.x; w < p.ntiles;
+       w += (unsigned long long)p.nshard * gridDim.x) {
     const int c = (int)src.cls(w);
     if (c != cur) {  // flush the previous class's FP64 totals to this CTA's slice
       if (cur >= 0 && active) {
@@ -190,7 +192,7 @@ __global__ void sinc_epilogue_kernel(const double *__restrict__ partial, int gri
                                      const uint32_t *__restrict__ pair_b, const double *__restrict__ w,
                                      const uint32_t *__restrict__ n_el_block, double q0, double dq,
                                      const double *__restrict__ qmesh, uint32_t nq, uint32_t ntot, int polar, double lambda,
-                                     int over_q, double *__restrict__ out);
+                                     int over_q, int self_term, double *__restrict__ out);
 
 // Launches sinc_tiles_kernel with the persistent grid and zeroed partial sums; returns the status
 // and the grid size used.
@@ -201,7 +203,8 @@ int launch_sinc(xns_ctx *ctx, const SincParams &p, const Src &src, int lanes, si
   XNS_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   XNS_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, SE_THREADS, smem));
-  unsigned long long grid = std::min<unsigned long long>(p.ntiles, (unsigned long long)ctx->num_sms * std::max(per_sm, 1));
+  const unsigned long long mine = p.nshard > 1 ? (p.ntiles + p.nshard - 1) / p.nshard : p.ntiles;
+  unsigned long long grid = std::min<unsigned long long>(mine, (unsigned long long)ctx->num_sms * std::max(per_sm, 1));
   if (grid == 0) grid = 1;
   SincParams pp = p;
   void *d;
@@ -235,7 +238,8 @@ int run_sinc(xns_ctx *ctx, SincParams p, const Src &src, size_t stage_bytes, boo
 // need the 1/q (the engine's), otherwise they are already sum w sin(q r)/(q r + 1e-8).
 int sinc_epilogue(xns_ctx *ctx, int grid, uint32_t ncls, uint32_t nel, uint32_t nblocks, const uint32_t *n_el_block,
                   const double *q, uint32_t nq, bool uniform, double q0, double dq, const double *d_w, uint32_t ntot,
-                  int polar, double lambda, double *d_out, const double *partial = nullptr, bool over_q = true);
+                  int polar, double lambda, double *d_out, const double *partial = nullptr, bool over_q = true,
+                  bool self_term = true);
 // The q mesh as a device array (valid until the next call on the context).
 int sinc_upload_q(xns_ctx *ctx, const double *q, uint32_t nq, const double **d_q);
 

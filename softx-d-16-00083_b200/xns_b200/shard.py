@@ -1,5 +1,9 @@
 """One structure over several GPUs (one process per GPU, torch.distributed for the plumbing).
 
+Debye double sum (int_debye): each rank sums its tile pairs (xns_calc_int_debye_shard, the self term
+on rank 0 only) and an all-reduce of the nq FP64 values gives every rank the whole I(q).
+
+Histogram path:
 Each rank counts its shard of the pair-distance histogram (xns_hist_shard_device: every N-th run of the
 whole structure's plan), an all-reduce sums the shards (NCCL over NVLink / NVSwitch on GPUs, gloo on
 CPU), and every rank derives the PDF and I(q) from the sum (xns_pdf_and_debye_from_hist_device).  The
@@ -17,6 +21,8 @@ _p = C.c_void_p
 lib.xns_hist_shard_device.argtypes = [_p, _p, _p, C.c_uint32, C.c_uint32, C.c_double, C.c_uint32, C.c_uint32, _p]
 lib.xns_calc_hist_shard.argtypes = [_p, C.POINTER(_p), _p, C.c_uint32, C.c_uint32, C.c_double, C.c_uint32, C.c_uint32,
                                     _p]
+lib.xns_calc_int_debye_shard.argtypes = [_p, C.POINTER(_p), _p, C.c_uint32, C.c_uint32, _p, _p, C.c_uint32, C.c_int,
+                                         C.POINTER(_p), _p, C.c_int, C.c_double, C.c_uint32, C.c_uint32, _p]
 lib.xns_pdf_and_debye_from_hist_device.argtypes = [_p, _p, _p, C.c_uint32, C.c_uint32, C.c_double, C.c_int, C.c_int,
                                                    C.c_double, _p, C.c_uint32, C.c_int, C.POINTER(_p), _p, C.c_int,
                                                    C.c_double, _p, _p]
@@ -68,3 +74,42 @@ def pdf_and_debye(ctx, xyz_dev, n_el, nhist, bin, scenario, pdftype, p0, q, sour
         ctx.handle, _p(hist_dev.data_ptr()), n_el.ctypes.data_as(_p), nel, nhist, bin, scenario, pdftype, p0,
         q.ctypes.data_as(_p), len(q), source, ffp, None if sl is None else sl.ctypes.data_as(_p), int(polar), lam,
         _p(I_dev.data_ptr()) if I_dev is not None else None, _p(pdf_dev.data_ptr()) if pdf_dev is not None else None))
+
+
+def int_debye_shard(ctx, elements, q, source, sl=None, ff=None, polar=False, lam=0.0, shard=0, nshard=1,
+                    n_el_block=None):
+    """This shard's share of calcIntDebye (or of calcIntPartialDebye with n_el_block, element-major
+    e * nblocks + b): nq doubles (or (1 + parts) x nq)."""
+    arrs = [np.ascontiguousarray(e, dtype=np.float64).reshape(-1, 3) for e in elements]
+    nel = len(arrs)
+    n_el = np.array([len(a) for a in arrs], dtype=np.uint32)
+    table = (_p * nel)(*[a.ctypes.data_as(_p) if len(a) else None for a in arrs])
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    nb = 1 if n_el_block is None else len(n_el_block) // nel
+    neb = None if n_el_block is None else np.ascontiguousarray(n_el_block, dtype=np.uint32)
+    parts = nb * (nb + 1) // 2
+    out = np.zeros((1 + parts if nb > 1 else 1) * len(q))
+    slp = None if sl is None else np.ascontiguousarray(sl, dtype=np.float64)
+    ffp, rows = None, None
+    if ff is not None:
+        rows = [np.ascontiguousarray(r, dtype=np.float64) for r in ff]
+        ffp = (_p * nel)(*[r.ctypes.data_as(_p) for r in rows])
+    _check(ctx, lib.xns_calc_int_debye_shard(ctx.handle, table, n_el.ctypes.data_as(_p), nel, nb,
+                                             None if neb is None else neb.ctypes.data_as(_p), q.ctypes.data_as(_p),
+                                             len(q), source, ffp, None if slp is None else slp.ctypes.data_as(_p),
+                                             int(polar), lam, shard, nshard, out.ctypes.data_as(_p)))
+    return out
+
+
+def int_debye(ctx, elements, q, source, sl=None, ff=None, polar=False, lam=0.0, rank=0, world=1, group=None,
+              n_el_block=None):
+    """calcIntDebye for one structure split over the ranks of group; every rank returns the whole I(q)."""
+    import torch
+    part = int_debye_shard(ctx, elements, q, source, sl, ff, polar, lam, rank, world, n_el_block)
+    if world == 1:
+        return part
+    import torch.distributed as dist
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" else torch.device("cpu")
+    t = torch.from_numpy(part).to(dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return t.cpu().numpy()

@@ -57,3 +57,28 @@ def test_one_rank_pipeline_matches_calc_pdf_and_debye(gpu_ctx):
     # the transform's cross-CTA FP64 sums are order-dependent: equal to the last few bits
     assert np.allclose(I.cpu().numpy(), I_ref, rtol=1e-12, atol=0)
     assert np.allclose(pdf.cpu().numpy(), pdf_ref, rtol=1e-12, atol=1e-300)
+
+
+@pytest.mark.parametrize("nshard", [2, 5])
+def test_debye_shards_sum_to_intensity(gpu_ctx, nshard):
+    els = synth.fcc_sphere(n=1500, a=4.078, sigma=0.05, seed=2)
+    q = synth.q_mesh(0.1, 10.0, 256)
+    full = gpu_ctx.calc_int_debye(els, q, xns_b200.NEUTRON, sl=[7.63])
+    parts = [shard.int_debye_shard(gpu_ctx, els, q, xns_b200.NEUTRON, sl=[7.63], shard=s, nshard=nshard)
+             for s in range(nshard)]
+    assert np.allclose(np.sum(parts, axis=0), full, rtol=1e-12, atol=0)
+    assert all(np.abs(p).max() > 0 for p in parts)
+
+
+def test_partial_debye_shards_sum(gpu_ctx):
+    rng = np.random.default_rng(6)
+    els = [rng.uniform(0, 15, (300, 3)), rng.uniform(0, 15, (200, 3))]
+    n_el_block = np.array([[100, 200], [150, 50]])  # (element, block)
+    q = synth.q_mesh(0.5, 8.0, 128)
+    full = gpu_ctx.calc_int_partial_debye(els, n_el_block, q, xns_b200.NEUTRON, sl=[3.63, 9.58])
+    parts = [shard.int_debye_shard(gpu_ctx, els, q, xns_b200.NEUTRON, sl=[3.63, 9.58], shard=s, nshard=3,
+                                   n_el_block=n_el_block.ravel()) for s in range(3)]
+    tot = np.sum(parts, axis=0)
+    # the cross-block parts cross zero: compare against the total intensity's scale at each q
+    scale = np.tile(np.abs(full[:len(q)]), len(full) // len(q))
+    assert np.max(np.abs(tot - full) / scale) < 1e-12
