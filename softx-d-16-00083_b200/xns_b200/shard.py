@@ -113,3 +113,35 @@ def int_debye(ctx, elements, q, source, sl=None, ff=None, polar=False, lam=0.0, 
     t = torch.from_numpy(part).to(dev)
     dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
     return t.cpu().numpy()
+
+
+def q_rows(nq, rank, world):
+    """The q rows [lo, hi) of rank in a balanced split of nq rows."""
+    return nq * rank // world, nq * (rank + 1) // world
+
+
+def int_2d(ctx, elements, q, nfi, euler_min, euler_max, euler_n, convention, lam, source, ff=None, sl=None,
+           polar=False, rank=0, world=1, group=None):
+    """calcInt2D (CalcFunctions.cpp:969-1091) for one structure split over the ranks by q rows (each row
+    of the reference's polar mesh is independent of the others, as its OpenMP loop over q,
+    :1023-1046, uses): every rank evaluates its rows and an all-gather assembles (I2D, I) on every
+    rank."""
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    lo, hi = q_rows(len(q), rank, world)
+    ffr = None if ff is None else [np.asarray(r)[lo:hi] for r in ff]
+    I2D, I = (ctx.calc_int_2d(elements, q[lo:hi], nfi, euler_min, euler_max, euler_n, convention, lam, source, ff=ffr,
+                              sl=sl, polar=polar) if hi > lo else (np.zeros((0, nfi)), np.zeros(0)))
+    if world == 1:
+        return I2D, I
+    import torch
+    import torch.distributed as dist
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" else torch.device("cpu")
+    rows = max(q_rows(len(q), r, world)[1] - q_rows(len(q), r, world)[0] for r in range(world))
+    mine = torch.zeros((rows, nfi + 1), dtype=torch.float64, device=dev)  # padded to the largest share
+    mine[:hi - lo, :nfi] = torch.from_numpy(I2D)
+    mine[:hi - lo, nfi] = torch.from_numpy(I)
+    parts = [torch.empty_like(mine) for _ in range(world)]
+    dist.all_gather(parts, mine, group=group)
+    full = torch.cat([parts[r][:q_rows(len(q), r, world)[1] - q_rows(len(q), r, world)[0]] for r in range(world)])
+    full = full.cpu().numpy()
+    return np.ascontiguousarray(full[:, :nfi]), np.ascontiguousarray(full[:, nfi])

@@ -82,3 +82,22 @@ def test_partial_debye_shards_sum(gpu_ctx):
     # the cross-block parts cross zero: compare against the total intensity's scale at each q
     scale = np.tile(np.abs(full[:len(q)]), len(full) // len(q))
     assert np.max(np.abs(tot - full) / scale) < 1e-12
+
+
+def test_2d_q_row_shards_assemble_the_pattern(gpu_ctx):
+    rng = np.random.default_rng(9)
+    els = [rng.uniform(-10, 10, (400, 3)), rng.uniform(-10, 10, (100, 3))]
+    q = synth.q_mesh(0.2, 6.0, 37)
+    args = (6, [0.1, 0.2, 0.0], [0.5, 0.9, 0.3], [2, 1, 2], 5, 1.54, xns_b200.NEUTRON)
+    I2D, I = gpu_ctx.calc_int_2d(els, q, *args, sl=[3.0, 5.0])
+    rows2d, rows1d = [], []
+    for r in range(4):
+        lo, hi = shard.q_rows(len(q), r, 4)
+        a, b = gpu_ctx.calc_int_2d(els, q[lo:hi], *args, sl=[3.0, 5.0])
+        rows2d.append(a)
+        rows1d.append(b)
+    assert np.allclose(np.concatenate(rows2d), I2D, rtol=1e-12, atol=0)
+    assert np.allclose(np.concatenate(rows1d), I, rtol=1e-12, atol=0)
+    # the one-rank driver returns the whole pattern
+    a, b = shard.int_2d(gpu_ctx, els, q, *args, sl=[3.0, 5.0])
+    assert np.allclose(a, I2D, rtol=1e-12, atol=0) and np.allclose(b, I, rtol=1e-12, atol=0)

