@@ -67,6 +67,21 @@ def build_lib(verbose_ptxas=False):
     return so
 
 
+# reference functions the relinked program takes from host/interpose.cpp (demangled name prefixes)
+INTERPOSED = ("block::calcAtoms(", "RearrangementInt(", "printI(", "printPartialI(", "printI2(", "printPDF(",
+              "printPartialPDF(", "printAtoms(")
+
+
+def _weaken(obj, out, prefixes):
+    """A copy of obj (built here from the reference's sources) in which the global functions whose
+    demangled names start with prefixes are weak, so that a strong definition linked beside it wins."""
+    lines = subprocess.check_output(["nm", "--defined-only", obj], text=True).splitlines()
+    mangled = [l.split()[-1] for l in lines if len(l.split()) == 3 and l.split()[1] == "T"]
+    demangled = subprocess.check_output(["c++filt"], input="\n".join(mangled), text=True).splitlines()
+    weak = [m for m, d in zip(mangled, demangled) if d.startswith(prefixes)]
+    _run(["objcopy"] + ["--weaken-symbol=" + m for m in weak] + [obj, out])
+
+
 def build_shim(ref):
     """The drop-in: calc_functions_b200.cpp exports the reference's four CPU calc-function
     signatures (main.cpp:344-347) on top of libxns_b200.so.  It is compiled against the reference's
@@ -92,9 +107,25 @@ def build_shim(ref):
         if _newer(o, [s]):
             _run([cxx, "-O3", "-std=c++11", "-w"] + defs + ["-I" + ref, "-c", s, "-o", o])
         objs.append(o)
+    # the functions either side of the calc functions (builder, rearrangement correction, writers) are
+    # not behind a macro: weaken them in copies of the reference's objects and link host/interpose.cpp's
+    # definitions in their place
+    ip_src = os.path.join(PKG, "host", "interpose.cpp")
+    ip_o = os.path.join(BUILD, "interpose.o")
+    if _newer(ip_o, [ip_src, os.path.join(INCLUDE, "xns_b200.h")]):
+        _run([cxx, "-O2", "-std=c++11", "-I" + ref, "-I" + INCLUDE, "-c", ip_src, "-o", ip_o])
+    linked = []
+    for o in objs:
+        if o.endswith("ref_CalcFunctions.o") or o.endswith("ref_IO.o"):
+            w = o.replace(".o", "_weak.o")
+            if _newer(w, [o]):
+                _weaken(o, w, INTERPOSED)
+            linked.append(w)
+        else:
+            linked.append(o)
     exe = os.path.join(LIB, "XaNSoNS_B200")
-    if _newer(exe, objs + [shim_so]):
-        _run([cxx, "-o", exe] + objs + ["-L" + LIB, "-lxns_calc_shim", "-lxns_b200", "-Wl,-rpath,$ORIGIN"])
+    if _newer(exe, linked + [ip_o, shim_so]):
+        _run([cxx, "-o", exe] + linked + [ip_o, "-L" + LIB, "-lxns_calc_shim", "-lxns_b200", "-Wl,-rpath,$ORIGIN"])
     # test program for the drop-in structure builder (tests/shim/build_atoms_check.cpp)
     chk_src = os.path.join(ROOT, "tests", "shim", "build_atoms_check.cpp")
     chk = os.path.join(LIB, "xns_build_atoms_check")

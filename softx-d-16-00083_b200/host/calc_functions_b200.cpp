@@ -62,6 +62,9 @@ float seconds_since(chrono::steady_clock::time_point t1) {
 
 }  // namespace
 
+// The shim's context, for the other drop-in objects of the relinked program (interpose.cpp).
+xns_ctx *xns_shim_context() { return context(); }
+
 // calcIntDebye, CalcFunctions.cpp:547
 void calcIntDebye(double **I, const config *cfg, const unsigned int *NatomEl, const vector<vect3d<double> > *ra,
                   vector<double *> FF, vector<double> SL, const double *q, unsigned int Ntot, int NumOMPthreads) {
@@ -144,16 +147,22 @@ void calcInt2D(double ***I2D, double **I, const config *cfg, const unsigned int 
   cout << "2D pattern calculation time: " << seconds_since(t1) << " s" << endl;
 }
 
-// block::calcAtoms (CalcFunctions.cpp:251-392) of every block on the GPU, for CalcAndPrintAtoms
-// (:397), whose loop `for (iB...) Block[iB].calcAtoms(*ra);` this call replaces: the atoms are appended
-// to ra[] per element in the reference's order, and each block's NatomElAll and N are set as
-// calcAtoms sets them.  The random draws are Philox4x32-10 keyed by the XNS_SEED environment variable;
-// without it the seed comes from the clock, as the reference's generator does (CalcFunctions.cpp:259).
-void calcAtomsB200(block *Block, unsigned int Nblocks, vector<vect3d<double> > *ra, unsigned int Nel) {
+namespace {
+
+// the random seed of this run: XNS_SEED, else the clock (as the reference's generator, CalcFunctions.cpp:259)
+uint64_t run_seed() {
+  static uint64_t seed = 0;
+  static bool set = false;
+  if (!set) {
+    const char *s = getenv("XNS_SEED");
+    seed = s ? strtoull(s, nullptr, 10) : (uint64_t)chrono::system_clock::now().time_since_epoch().count();
+    set = true;
+  }
+  return seed;
+}
+
+void build_blocks(block *Block, unsigned int Nblocks, vector<vect3d<double> > *ra, unsigned int Nel, uint64_t seed) {
   static_assert(sizeof(vect3d<double>) == 3 * sizeof(double), "vect3d<double> must be three packed doubles");
-  const char *s = getenv("XNS_SEED");
-  const uint64_t seed = s ? strtoull(s, nullptr, 10)
-                          : (uint64_t)chrono::system_clock::now().time_since_epoch().count();
   vector<xns_block> xb(Nblocks);
   vector<vector<double> > store(Nblocks);  // pSymm, rSymm, rCopy and cf of each block as flat rows
   for (unsigned int iB = 0; iB < Nblocks; iB++) {
@@ -208,4 +217,24 @@ void calcAtomsB200(block *Block, unsigned int Nblocks, vector<vect3d<double> > *
       Block[iB].N += n_all[o];
     }
   }
+}
+
+}  // namespace
+
+// block::calcAtoms (CalcFunctions.cpp:251-392) of every block on the GPU, for CalcAndPrintAtoms
+// (:397), whose loop `for (iB...) Block[iB].calcAtoms(*ra);` this call replaces: the atoms are appended
+// to ra[] per element in the reference's order, and each block's NatomElAll and N are set as
+// calcAtoms sets them.  The random draws are Philox4x32-10 keyed by the XNS_SEED environment variable;
+// without it the seed comes from the clock, as the reference's generator does (CalcFunctions.cpp:259).
+void calcAtomsB200(block *Block, unsigned int Nblocks, vector<vect3d<double> > *ra, unsigned int Nel) {
+  build_blocks(Block, Nblocks, ra, Nel, run_seed());
+}
+
+// One block, for the relinked program's block::calcAtoms (interpose.cpp): each block of a run gets its
+// own key (the run's seed advanced by a Weyl step per block), so equal blocks draw differently.
+void xns_shim_build_block(block *b, vector<vect3d<double> > *ra) {
+  static uint64_t calls = 0;
+  unsigned int nel = 0;
+  for (unsigned int k = 0; k < b->Nid; k++) nel = max(nel, b->id[k] + 1);
+  build_blocks(b, 1, ra, nel, run_seed() + 0x9E3779B97F4A7C15ull * ++calls);
 }

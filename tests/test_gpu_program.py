@@ -1,7 +1,8 @@
 """GPU end to end: the reference program built from its sources (oracle/_ref/XaNSoNS_OMP) and the same
-program relinked against the drop-in calc functions (softx-d-16-00083_b200/lib/XaNSoNS_B200: the
-reference's main.cpp, ReadXML.cpp and IO.cpp unchanged) run the same XML decks; their output files
-must agree -- PDF files byte for byte, intensity files within the relative tolerance."""
+program relinked against the drop-in (softx-d-16-00083_b200/lib/XaNSoNS_B200: the reference's main.cpp,
+ReadXML.cpp, IO.cpp and CalcFunctions.cpp sources, its calc functions, structure builder, rearrangement
+correction and writers replaced by the GPU library's) run the same XML decks; their output files
+must agree -- PDF and atom files byte for byte, intensity files within the relative tolerance."""
 import os
 import subprocess
 
@@ -21,7 +22,7 @@ need_exes = pytest.mark.skipif(not (os.path.exists(REF_EXE) and os.path.exists(O
                                reason="reference program or relinked program not built")
 
 
-def write_deck(d, name, scenario, elements, names, calc_extra, calc_children):
+def write_deck(d, name, scenario, elements, names, calc_extra, calc_children, block_extra=""):
     with open(os.path.join(d, "atoms.txt"), "w") as f:
         for nm, xyz in zip(names, elements):
             for x, y, z in xyz:
@@ -31,7 +32,7 @@ def write_deck(d, name, scenario, elements, names, calc_extra, calc_children):
     with open(os.path.join(d, name + ".xml"), "w") as f:
         f.write('<?xml version="1.0"?>\n<Main>\n  <Calculation name="%s" source="neutron" scenario="%s" '
                 'FFfilename="sl.txt" %s>\n%s\n  </Calculation>\n  <Block>\n    <Atoms filename="atoms.txt"/>\n'
-                '  </Block>\n</Main>\n' % (name, scenario, calc_extra, calc_children))
+                '%s  </Block>\n</Main>\n' % (name, scenario, calc_extra, calc_children, block_extra))
 
 
 def run_both(tmp_path, name):
@@ -43,7 +44,8 @@ def run_both(tmp_path, name):
         r = subprocess.run([exe, name + ".xml"] + (["4"] if tag == "ref" else []), cwd=d, capture_output=True, text=True,
                            timeout=600)
         assert r.returncode == 0, r.stdout + r.stderr
-        outs[tag] = {f: (d / f).read_text() for f in os.listdir(d) if f.endswith(".txt") and f not in ("atoms.txt", "sl.txt")}
+        outs[tag] = {f: (d / f).read_text() for f in os.listdir(d)
+                     if (f.endswith(".txt") or f.endswith(".xyz")) and f not in ("atoms.txt", "sl.txt", "neigh.txt")}
     assert sorted(outs["ref"]) == sorted(outs["ours"]) and outs["ref"]
     return outs
 
@@ -97,4 +99,34 @@ def test_program_2d(tmp_path):
             floor = 1e-2 * np.median(np.abs(a))
             assert np.max(np.abs(a - b) / np.maximum(np.abs(a), floor)) < 1e-5, f
         else:
+            assert np.max(np.abs(a[:, 1] - b[:, 1]) / np.abs(a[:, 1])) < 1e-5, f
+
+
+@need_exes
+def test_program_debye_rearrangement_and_atoms(tmp_path):
+    """a molecule with a Rearrangement file (RearrangementInt after the Debye sum) and PrintAtoms
+    (the builder's atoms written by printAtoms): intensities within 1e-5, the atom file byte for byte"""
+    from test_rearrangement import molecule_block
+    mb = molecule_block(n=60, seed=4, coeff=1, rcorr=0.4)
+    names = ["Na", "Cl"]
+    ne = [int(v) for v in mb.natom_el]
+    els = [mb.r_atom[:ne[0]], mb.r_atom[ne[0]:]]
+    d = make_dirs(tmp_path)
+    with open(os.path.join(d, "neigh.txt"), "w") as f:
+        for i in range(len(mb.r_atom)):
+            lo, hi = int(mb.neighb_off[i]), int(mb.neighb_off[i + 1])
+            f.write("%d %d\n" % (i, hi - lo))
+            for k in range(lo, hi):
+                x, y, z = mb.neighb_r[k]
+                f.write("%s %.17g %.17g %.17g\n" % (names[int(mb.neighb_id[k])], x, y, z))
+    write_deck(d, "mol", "Debye", els, names, 'PrintAtoms="yes"', '    <q min="0.1" max="12" N="400"/>',
+               '    <Rearrangement filename="neigh.txt" Rcorr="0.4"/>\n')
+    outs = run_both(tmp_path, "mol")
+    assert any(f.endswith(".xyz") for f in outs["ref"])
+    for f, text in outs["ref"].items():
+        if f.endswith(".xyz"):
+            assert text == outs["ours"][f], f
+        else:
+            a, b = table(text), table(outs["ours"][f])
+            assert np.array_equal(a[:, 0], b[:, 0])
             assert np.max(np.abs(a[:, 1] - b[:, 1]) / np.abs(a[:, 1])) < 1e-5, f
