@@ -231,7 +231,7 @@ struct MergeArgs {
   const float *lx, *ly, *lz;  // offsets of each site from its tile's box corner
   double ct[3 * MAX_T];       // translations e0 cx + e1 cy + e2 cz in the reference's loop order
   uint32_t S, ntile, T;
-  unsigned long long npairs;  // tile pairs ti <= tj
+  unsigned long long npairs;  // (I tile, pair of J tiles) pairs: nJ (nJ + 1), nJ = ceil(ntile / 2)
   unsigned long long *hits;
   uint32_t cap;
   uint32_t *nhit, *outdeg, *indeg;
@@ -250,54 +250,84 @@ __device__ __forceinline__ bool exact_hit(const MergeArgs &a, D3 d0, int t) {
   return sqr3(add3(d0, D3{a.ct[3 * t], a.ct[3 * t + 1], a.ct[3 * t + 2]})) < 0.25;
 }
 
+// The tile-pair constants of one J half (tile tj, when it exists) for one translation c: whether the
+// boxes come within 0.5 A, the frame shift delta = oI - oJ + c and the FP32 threshold (-1 when dead).
+struct HalfBox {
+  bool live;
+  float dx, dy, dz, thr;
+};
+__device__ __forceinline__ HalfBox half_box(const double *bi, const double *box, unsigned long long tj, uint32_t ntile,
+                                            const double *c) {
+  HalfBox r{false, 0.f, 0.f, 0.f, -1.f};
+  if (tj >= ntile) return r;
+  const double *bj = box + 6 * tj;
+  double g2 = 0, esum = 0, del[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const double dlo = bi[k] - bj[3 + k] + c[k], dhi = bi[3 + k] - bj[k] + c[k];  // d = ri - rj + c in [dlo, dhi]
+    const double g = fmax(0.0, fmax(dlo, -dhi));
+    g2 += g * g;
+    del[k] = bi[k] - bj[k] + c[k];
+    esum += 0x1.0p-23 * (2.0 * (bi[3 + k] - bi[k]) + 2.0 * (bj[3 + k] - bj[k]) + 2.0 * fabs(del[k]) + 1.0) + 1e-9;
+  }
+  if (!(g2 < 0.25 * (1.0 + 1e-9) + 1e-9)) return r;
+  r.live = true;
+  r.dx = (float)del[0], r.dy = (float)del[1], r.dz = (float)del[2];
+  r.thr = __double2float_ru((0.5 + esum) * (0.5 + esum) * (1.0 + 0x1.0p-20));
+  return r;
+}
+
+// d~^2 - thr for a pair of J rows, evaluated as one FMA chain: its rounding stays within 2^-21 thr,
+// inside the 2^-20 thr of slack in thr, so every pair under the FP32 bound comes out negative
+__device__ __forceinline__ xns_f2::f2 merge_excess(xns_f2::f2 xd, xns_f2::f2 yd, xns_f2::f2 zd, xns_f2::f2 nthr,
+                                                   xns_f2::f2 xj, xns_f2::f2 yj, xns_f2::f2 zj) {
+  using namespace xns_f2;
+  const f2 dx = sub(xd, xj), dy = sub(yd, yj), dz = sub(zd, zj);
+  return fma(dz, dz, fma(dy, dy, fma(dx, dx, nthr)));
+}
+
+// A CTA takes an I tile (MT sites, one per thread) against a J tile of 2 MT sites (two consecutive
+// tiles, each in its own frame): tile pair p of the triangle ti <= 2 tj2 + 1 decodes as
+// tj2 (tj2 + 1) <= p < (tj2 + 1)(tj2 + 2), ti = p - tj2 (tj2 + 1).
 __global__ void __launch_bounds__(128) merge_kernel(const __grid_constant__ MergeArgs a) {
   using namespace xns_f2;
-  __shared__ f2 jx2[MT / 2], jy2[MT / 2], jz2[MT / 2];
-  __shared__ float sdel[MAX_T][4];  // delta x y z and thr per live translation
+  __shared__ f2 jx2[MT], jy2[MT], jz2[MT];  // the J tile's 2 MT sites as MT pairs
+  __shared__ float sdel[MAX_T][2][4];       // per live translation and J half: delta x y z, thr (< 0: dead)
   __shared__ uint8_t alive[MAX_T];
   __shared__ int nalive;
   for (unsigned long long p = blockIdx.x; p < a.npairs; p += gridDim.x) {
-    unsigned long long tj = (unsigned long long)((sqrt(8.0 * (double)p + 1.0) - 1.0) * 0.5);
-    while (tj * (tj + 1) / 2 > p) tj--;
-    while ((tj + 1) * (tj + 2) / 2 <= p) tj++;
-    const unsigned long long ti = p - tj * (tj + 1) / 2;
+    unsigned long long tj2 = (unsigned long long)((sqrt(4.0 * (double)p + 1.0) - 1.0) * 0.5);
+    while (tj2 * (tj2 + 1) > p) tj2--;
+    while ((tj2 + 1) * (tj2 + 2) <= p) tj2++;
+    const unsigned long long ti = p - tj2 * (tj2 + 1);
+    if (ti >= a.ntile) continue;  // uniform across the CTA: an odd tile count leaves no I tile here
     __syncthreads();
     if (threadIdx.x == 0) nalive = 0;
     __syncthreads();
     // a translation can only give a hit when the boxes come closer than 0.5 A (with slack for rounding);
-    // live translations are kept in loop order, so the first one that hits a pair is found first
-    const double *bi = a.box + 6 * ti, *bj = a.box + 6 * tj;
+    // live translations (live for either half) are kept in loop order, so the first one that hits a
+    // pair is found first
+    const double *bi = a.box + 6 * ti;
     if (threadIdx.x < 32) {
       for (uint32_t t0 = 0; t0 < a.T; t0 += 32) {
         const uint32_t t = t0 + threadIdx.x;
-        bool live = false;
-        double del[3], esum = 0;
-        if (t < a.T) {
-          double g2 = 0;
-          for (int k = 0; k < 3; k++) {
-            const double c = a.ct[3 * t + k];
-            const double dlo = bi[k] - bj[3 + k] + c, dhi = bi[3 + k] - bj[k] + c;  // d = ri - rj + c in [dlo, dhi]
-            const double g = fmax(0.0, fmax(dlo, -dhi));
-            g2 += g * g;
-            del[k] = bi[k] - bj[k] + c;
-            esum += 0x1.0p-23 * (2.0 * (bi[3 + k] - bi[k]) + 2.0 * (bj[3 + k] - bj[k]) + 2.0 * fabs(del[k]) + 1.0) + 1e-9;
-          }
-          live = g2 < 0.25 * (1.0 + 1e-9) + 1e-9;
-        }
+        const HalfBox h0 = t < a.T ? half_box(bi, a.box, 2 * tj2, a.ntile, a.ct + 3 * t) : HalfBox{false, 0.f, 0.f, 0.f, -1.f};
+        const HalfBox h1 = t < a.T ? half_box(bi, a.box, 2 * tj2 + 1, a.ntile, a.ct + 3 * t) : HalfBox{false, 0.f, 0.f, 0.f, -1.f};
+        const bool live = h0.live || h1.live;
         const uint32_t m = __ballot_sync(0xffffffffu, live);
         if (live) {
           const int slot = nalive + __popc(m & ((1u << threadIdx.x) - 1));
           alive[slot] = (uint8_t)t;
-          for (int k = 0; k < 3; k++) sdel[slot][k] = (float)del[k];
-          sdel[slot][3] = __double2float_ru((0.5 + esum) * (0.5 + esum) * (1.0 + 0x1.0p-20));
+          sdel[slot][0][0] = h0.dx, sdel[slot][0][1] = h0.dy, sdel[slot][0][2] = h0.dz, sdel[slot][0][3] = h0.thr;
+          sdel[slot][1][0] = h1.dx, sdel[slot][1][1] = h1.dy, sdel[slot][1][2] = h1.dz, sdel[slot][1][3] = h1.thr;
         }
         __syncwarp();
         if (threadIdx.x == 0) nalive += __popc(m);
         __syncwarp();
       }
     }
-    if (threadIdx.x < MT / 2) {
-      const size_t j = tj * MT + 2 * threadIdx.x;
+    {
+      const size_t j = tj2 * 2 * MT + 2 * threadIdx.x;
       // rows past the end sit far away and never pass the FP32 test
       const float x0 = j < a.S ? a.lx[j] : 1e30f, y0 = j < a.S ? a.ly[j] : 1e30f, z0 = j < a.S ? a.lz[j] : 1e30f;
       const float x1 = j + 1 < a.S ? a.lx[j + 1] : 1e30f, y1 = j + 1 < a.S ? a.ly[j + 1] : 1e30f,
@@ -310,35 +340,35 @@ __global__ void __launch_bounds__(128) merge_kernel(const __grid_constant__ Merg
     const uint32_t i = (uint32_t)(ti * MT) + threadIdx.x;
     if (i >= a.S) continue;
     const float xi = a.lx[i], yi = a.ly[i], zi = a.lz[i];
+    // the first half holds only sites below every i of the I tile when the I tile is the second tile
+    const int h0 = ti == 2 * tj2 + 1 ? 1 : 0;
     for (int s = 0; s < na; s++) {
-      const f2 xd = splat(xi + sdel[s][0]), yd = splat(yi + sdel[s][1]), zd = splat(zi + sdel[s][2]);
-      const f2 nthr = splat(-sdel[s][3]);
-      // d~^2 - thr, evaluated as one FMA chain: its rounding stays within 2^-21 thr, inside the 2^-20 thr
-      // of slack in thr, so every pair under the FP32 bound comes out negative
-      auto excess = [&](int k) {
-        const f2 dx = sub(xd, jx2[k]), dy = sub(yd, jy2[k]), dz = sub(zd, jz2[k]);
-        return fma(dz, dz, fma(dy, dy, fma(dx, dx, nthr)));
-      };
-      for (int k0 = 0; k0 < MT / 2; k0 += 4) {
-        unsigned long long any = 0;  // sign bits of four pairs of J rows
+      for (int h = h0; h < 2; h++) {
+        const float thr = sdel[s][h][3];
+        if (thr < 0.f) continue;
+        const f2 xd = splat(xi + sdel[s][h][0]), yd = splat(yi + sdel[s][h][1]), zd = splat(zi + sdel[s][h][2]);
+        const f2 nthr = splat(-thr);
+        for (int k0 = h * (MT / 2); k0 < (h + 1) * (MT / 2); k0 += 4) {
+          unsigned long long any = 0;  // sign bits of four pairs of J rows
 #pragma unroll
-        for (int u = 0; u < 4; u++) any |= excess(k0 + u);
-        if (!(any & 0x8000000080000000ull)) continue;
-        for (int u = 0; u < 4; u++) {
-          const unsigned long long e2 = excess(k0 + u);
-          for (int h = 0; h < 2; h++) {
-            const uint32_t j = (uint32_t)(tj * MT) + 2 * (k0 + u) + h;
-            if (!((e2 >> (32 * h + 31)) & 1) || j <= i || j >= a.S) continue;
-            const D3 d0 = sub3(D3{a.px[i], a.py[i], a.pz[i]}, D3{a.px[j], a.py[j], a.pz[j]});
-            // record the pair once: at the first live translation that hits it
-            if (!exact_hit(a, d0, alive[s])) continue;
-            bool earlier = false;
-            for (int e = 0; e < s && !earlier; e++) earlier = exact_hit(a, d0, alive[e]);
-            if (earlier) continue;
-            const uint32_t pos = atomicAdd(a.nhit, 1u);
-            if (pos < a.cap) a.hits[pos] = ((unsigned long long)i << 32) | j;
-            atomicAdd(a.outdeg + i, 1u);
-            atomicAdd(a.indeg + j, 1u);
+          for (int u = 0; u < 4; u++) any |= merge_excess(xd, yd, zd, nthr, jx2[k0 + u], jy2[k0 + u], jz2[k0 + u]);
+          if (!(any & 0x8000000080000000ull)) continue;
+          for (int u = 0; u < 4; u++) {
+            const unsigned long long e2 = merge_excess(xd, yd, zd, nthr, jx2[k0 + u], jy2[k0 + u], jz2[k0 + u]);
+            for (int hh = 0; hh < 2; hh++) {
+              const uint32_t j = (uint32_t)(tj2 * 2 * MT) + 2 * (k0 + u) + hh;
+              if (!((e2 >> (32 * hh + 31)) & 1) || j <= i || j >= a.S) continue;
+              const D3 d0 = sub3(D3{a.px[i], a.py[i], a.pz[i]}, D3{a.px[j], a.py[j], a.pz[j]});
+              // record the pair once: at the first live translation that hits it
+              if (!exact_hit(a, d0, alive[s])) continue;
+              bool earlier = false;
+              for (int e = 0; e < s && !earlier; e++) earlier = exact_hit(a, d0, alive[e]);
+              if (earlier) continue;
+              const uint32_t pos = atomicAdd(a.nhit, 1u);
+              if (pos < a.cap) a.hits[pos] = ((unsigned long long)i << 32) | j;
+              atomicAdd(a.outdeg + i, 1u);
+              atomicAdd(a.indeg + j, 1u);
+            }
           }
         }
       }
@@ -721,7 +751,8 @@ int plan_block(xns_ctx *ctx, Arena &ar, const xns_block &bk, uint32_t blk, uint6
   uint32_t *outdeg = deg, *indeg = deg + S;
   nhit = deg + 2 * (size_t)S;
   ma.px = px, ma.py = py, ma.pz = pz, ma.box = box, ma.S = S, ma.ntile = ntile, ma.T = (uint32_t)T;
-  ma.npairs = (unsigned long long)ntile * (ntile + 1) / 2;
+  const unsigned long long nj2 = (ntile + 1) / 2;
+  ma.npairs = nj2 * (nj2 + 1);
   ma.outdeg = outdeg, ma.indeg = indeg, ma.nhit = nhit;
   uint32_t cap = std::max<uint32_t>(S, 1u << 16), h_nhit = 0;
   for (int attempt = 0; attempt < 2; attempt++) {

@@ -90,6 +90,8 @@ def draw_free_cases():
     pts = rng.uniform(0, 30, (3000, 3))
     pts[1500:1600] = pts[:100] + rng.normal(0, 0.1, (100, 3))
     cases["atom_file"] = ([Block(pts, [2000, 1000], [1, 0], occ=np.ones(3000))], 2)
+    # every site vacant (occupancy 0: a draw of exactly 0 is the only way in, probability 2^-53)
+    cases["all_vacant"] = ([rocksalt((3, 3, 3), occ=[0.0, 0.0])], 2)
     return cases
 
 

@@ -158,3 +158,19 @@ def test_drop_in_builder_matches_reference_program_objects():
     assert r.returncode == 0, r.stdout + r.stderr
     lines = r.stdout.strip().splitlines()
     assert len(lines) == 2 and all(l.endswith("identical") for l in lines)
+
+
+def test_empty_inputs(gpu_ctx):
+    """no blocks, a block without sites next to a real one, a fully vacant block"""
+    _, n_el, n_all = gpu_ctx.build_atoms([], 3, 1)
+    assert list(n_el) == [0, 0, 0] and len(n_all) == 0
+    assert [len(x) for x in gpu_ctx.copy_atoms(n_el)] == [0, 0, 0]
+    empty = Block(np.zeros((0, 3)), [0], [1])
+    b = rocksalt((2, 2, 2))
+    xg, ng, _, _ = _build(gpu_ctx, [empty, b], 2, 4)
+    xo, no = oracle().build_atoms([empty, b], 2, seed=4)
+    assert np.array_equal(ng, no) and list(ng) == [0, 32, 32]
+    for a, c in zip(xg, xo):
+        assert np.array_equal(a, c)
+    xg, ng, _, _ = _build(gpu_ctx, [rocksalt((3, 3, 3), occ=[0.0, 0.0])], 2, 4)
+    assert [len(x) for x in xg] == [0, 0] and list(ng) == [0, 0]
