@@ -325,7 +325,7 @@ __global__ void pair_key_kernel(KeyParams p, uint32_t *__restrict__ kcnt) {
   for (unsigned long long w0 = blockIdx.x * (unsigned long long)blockDim.x + (threadIdx.x & ~31u); w0 < p.ntp;
        w0 += stride) {
     const unsigned long long w = w0 + lane;
-    const bool act = w < p.ntp && w % p.nshard == p.shard;
+    const bool act = w < p.ntp && (p.nshard == 1 || w % p.nshard == p.shard);
     const unsigned act_mask = __ballot_sync(0xffffffffu, act);
     if (act) {
       TilePair tp;
@@ -343,7 +343,7 @@ __global__ void pair_scatter_kernel(KeyParams p, const uint32_t *__restrict__ ko
   for (unsigned long long w0 = blockIdx.x * (unsigned long long)blockDim.x + (threadIdx.x & ~31u); w0 < p.ntp;
        w0 += stride) {
     const unsigned long long w = w0 + lane;
-    const bool act = w < p.ntp && w % p.nshard == p.shard;
+    const bool act = w < p.ntp && (p.nshard == 1 || w % p.nshard == p.shard);
     const unsigned act_mask = __ballot_sync(0xffffffffu, act);
     if (act) {
       TilePair tp;
