@@ -73,6 +73,13 @@ double xns_last_stage_ms(const xns_ctx *ctx, int stage);
 int xns_calc_hist(xns_ctx *ctx, const double *const *xyz_el, const uint32_t *n_el, uint32_t nel, uint32_t nhist, double bin,
                   uint64_t *hist);
 
+/* xns_calc_hist in passes: the tile pairs of the spatial plan are enumerated and taken at most
+ * max_tile_pairs at a time (16 bytes of device memory each; 0 = 2^28, the default of every histogram
+ * entry point), each pass adding into one histogram, so that structures of any size fit the device;
+ * the result equals xns_calc_hist's. */
+int xns_calc_hist_passes(xns_ctx *ctx, const double *const *xyz_el, const uint32_t *n_el, uint32_t nel, uint32_t nhist,
+                         double bin, uint64_t max_tile_pairs, uint64_t *hist);
+
 /* Histogram -> I(q).  Replaces calcInt1DHist (CalcFunctions.cpp:810-911) and calcInt1DHistCuda
  * (CalcFunctionsCUDA.cu:988-1045).  ff: nel pointers to nq doubles (X-ray) or NULL; sl: nel doubles
  * (neutron) or NULL.  I: nq doubles, already divided by ntot and polarisation-corrected if polar. */

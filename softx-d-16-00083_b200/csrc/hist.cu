@@ -297,7 +297,8 @@ __device__ __forceinline__ void tile_pair_range(const Tile &A, const Tile &B, do
 struct KeyParams {
   const SegPair *sp;
   int nsp;
-  unsigned long long ntp;
+  unsigned long long ntp;   // tile pairs of this pass: w = wbeg + [0, ntp)
+  unsigned long long wbeg;
   const Tile *tiles;
   double inv_bin;
   uint32_t nhist, nbuckets, nkeys;  // key = class * nbuckets + bucket; nkeys - 1 = the wide key
@@ -324,8 +325,8 @@ __global__ void pair_key_kernel(KeyParams p, uint32_t *__restrict__ kcnt) {
   const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
   for (unsigned long long w0 = blockIdx.x * (unsigned long long)blockDim.x + (threadIdx.x & ~31u); w0 < p.ntp;
        w0 += stride) {
-    const unsigned long long w = w0 + lane;
-    const bool act = w < p.ntp && (p.nshard == 1 || w % p.nshard == p.shard);
+    const unsigned long long w = p.wbeg + w0 + lane;
+    const bool act = w0 + lane < p.ntp && (p.nshard == 1 || w % p.nshard == p.shard);
     const unsigned act_mask = __ballot_sync(0xffffffffu, act);
     if (act) {
       TilePair tp;
@@ -342,8 +343,8 @@ __global__ void pair_scatter_kernel(KeyParams p, const uint32_t *__restrict__ ko
   const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
   for (unsigned long long w0 = blockIdx.x * (unsigned long long)blockDim.x + (threadIdx.x & ~31u); w0 < p.ntp;
        w0 += stride) {
-    const unsigned long long w = w0 + lane;
-    const bool act = w < p.ntp && (p.nshard == 1 || w % p.nshard == p.shard);
+    const unsigned long long w = p.wbeg + w0 + lane;
+    const bool act = w0 + lane < p.ntp && (p.nshard == 1 || w % p.nshard == p.shard);
     const unsigned act_mask = __ballot_sync(0xffffffffu, act);
     if (act) {
       TilePair tp;
@@ -969,7 +970,7 @@ int xns_hist_plan(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, u
   if ((st = xns_scratch(ctx, SLOT_HCELL, sizeof(uint32_t) * (4 * (size_t)ncells + 8), &vcell))) return st;
   uint32_t *d_cnt = (uint32_t *)vcell, *d_coff = d_cnt + ncells, *d_toff = d_coff + ncells, *d_cur = d_toff + ncells,
            *d_tot = d_cur + ncells;
-  const bool ordered = tune.nshard > 1;
+  const bool ordered = tune.nshard > 1 || tune.ordered;
   if ((st = xns_scratch(ctx, SLOT_HSORT, (sizeof(double) * 3 + sizeof(uint32_t) * (ordered ? 2 : 1)) * (size_t)ntot,
                         &vsort)))
     return st;
@@ -1029,8 +1030,12 @@ int xns_hist_plan(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, u
       }
   }
   std::vector<SegPair> sched;
-  const unsigned long long ntp = xns_build_schedule(sa, sb, cls, same, 1, 1, &sched);
-  if (ntp >= (1ull << 32)) return xns_fail(ctx, XNS_ERR_ARG, "histogram: too many tile pairs");
+  const unsigned long long ntp_all = xns_build_schedule(sa, sb, cls, same, 1, 1, &sched);
+  L->ntp_total = ntp_all;
+  // this pass: tile pairs [w_begin, w_begin + ntp) of the enumeration
+  unsigned long long ntp = ntp_all > tune.w_begin ? ntp_all - tune.w_begin : 0;
+  if (tune.max_pairs) ntp = std::min(ntp, tune.max_pairs);
+  if (ntp >= (1ull << 32)) return xns_fail(ctx, XNS_ERR_ARG, "histogram: too many tile pairs for one pass");
   if (ntp == 0) return XNS_OK;
   SegPair *d_sp;
   if ((st = xns_upload_schedule(ctx, sched, &d_sp))) return st;
@@ -1038,6 +1043,7 @@ int xns_hist_plan(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, u
   kp.sp = d_sp;
   kp.nsp = (int)sched.size();
   kp.ntp = ntp;
+  kp.wbeg = tune.w_begin;
   kp.tiles = d_tiles;
   kp.inv_bin = 1.0 / bin;
   kp.nhist = nhist;
@@ -1119,7 +1125,7 @@ int xns_hist_plan(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, u
 }
 
 int xns_hist_enqueue(xns_ctx *ctx, const HistLaunch &L) {
-  XNS_CUDA(ctx, cudaMemsetAsync(L.hist, 0, sizeof(unsigned long long) * L.hist_words, ctx->stream));
+  if (L.zero_hist) XNS_CUDA(ctx, cudaMemsetAsync(L.hist, 0, sizeof(unsigned long long) * L.hist_words, ctx->stream));
   XNS_CUDA(ctx, cudaMemsetAsync(L.flags, 0, 2 * sizeof(unsigned int), ctx->stream));
   HistParams hp;
   memcpy(&hp, L.params, sizeof(hp));
@@ -1148,18 +1154,35 @@ int xns_hist_check(xns_ctx *ctx, const HistLaunch &L) {
   return XNS_OK;
 }
 
-int xns_hist_set(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, unsigned long long *d_hist) {
-  HistLaunch L;
+// The histogram of a set in passes of at most t.max_pairs tile pairs, all adding into d_hist.
+static int hist_passes(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, HistTuning t,
+                       unsigned long long *d_hist) {
+  if (!t.max_pairs) t.max_pairs = XNS_HIST_PASS_PAIRS;
   int st;
-  if ((st = xns_hist_plan(ctx, hs, nhist, bin, d_hist, HistTuning(), &L))) return st;
-  if ((st = xns_stage_begin(ctx, STAGE_HIST))) return st;
-  if ((st = xns_hist_enqueue(ctx, L))) return st;
-  if ((st = xns_stage_end(ctx, STAGE_HIST))) return st;
-  return xns_hist_check(ctx, L);
+  for (unsigned long long pass = 0;; pass++) {
+    t.w_begin = pass * t.max_pairs;
+    HistLaunch L;
+    if ((st = xns_hist_plan(ctx, hs, nhist, bin, d_hist, t, &L))) return st;
+    if (pass == 0 && !t.ordered && L.ntp_total > t.max_pairs) {
+      // several passes must form the same tiles: plan again with the cells in input order
+      t.ordered = true;
+      if ((st = xns_hist_plan(ctx, hs, nhist, bin, d_hist, t, &L))) return st;
+    }
+    L.zero_hist = pass == 0;
+    if (pass == 0 && (st = xns_stage_begin(ctx, STAGE_HIST))) return st;
+    if ((st = xns_hist_enqueue(ctx, L))) return st;
+    if ((st = xns_hist_check(ctx, L))) return st;
+    if (t.w_begin + t.max_pairs >= L.ntp_total) break;
+  }
+  return xns_stage_end(ctx, STAGE_HIST);
+}
+
+int xns_hist_set(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, unsigned long long *d_hist) {
+  return hist_passes(ctx, hs, nhist, bin, HistTuning(), d_hist);
 }
 
 int xns_hist_device_shard(xns_ctx *ctx, const DevCoords &dc, uint32_t nhist, double bin, uint32_t shard, uint32_t nshard,
-                          unsigned long long *d_hist) {
+                          unsigned long long *d_hist, unsigned long long max_pairs) {
   HistSet hs;
   hs.x = dc.x;
   hs.y = dc.y;
@@ -1170,13 +1193,8 @@ int xns_hist_device_shard(xns_ctx *ctx, const DevCoords &dc, uint32_t nhist, dou
   HistTuning t;
   t.shard = shard;
   t.nshard = nshard;
-  HistLaunch L;
-  int st;
-  if ((st = xns_hist_plan(ctx, hs, nhist, bin, d_hist, t, &L))) return st;
-  if ((st = xns_stage_begin(ctx, STAGE_HIST))) return st;
-  if ((st = xns_hist_enqueue(ctx, L))) return st;
-  if ((st = xns_stage_end(ctx, STAGE_HIST))) return st;
-  return xns_hist_check(ctx, L);
+  t.max_pairs = max_pairs;
+  return hist_passes(ctx, hs, nhist, bin, t, d_hist);
 }
 
 extern "C" int xns_hist_shard_device(xns_ctx *ctx, const double *xyz_dev, const uint32_t *n_el, uint32_t nel, uint32_t nhist,
@@ -1232,6 +1250,24 @@ extern "C" int xns_calc_hist(xns_ctx *ctx, const double *const *xyz_el, const ui
   if ((st = xns_scratch(ctx, SLOT_HIST, bytes, &d_hist))) return st;
   if ((st = xns_timer_start(ctx))) return st;
   if ((st = xns_hist_device(ctx, dc, nhist, bin, (unsigned long long *)d_hist))) return st;
+  if ((st = xns_timer_stop(ctx))) return st;
+  XNS_CUDA(ctx, cudaMemcpyAsync(hist, d_hist, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return XNS_OK;
+}
+
+extern "C" int xns_calc_hist_passes(xns_ctx *ctx, const double *const *xyz_el, const uint32_t *n_el, uint32_t nel,
+                                    uint32_t nhist, double bin, uint64_t max_tile_pairs, uint64_t *hist) {
+  if (!ctx) return XNS_ERR_ARG;
+  if (!hist) return xns_fail(ctx, XNS_ERR_ARG, "hist passes: null output");
+  int st;
+  DevCoords dc;
+  if ((st = xns_upload_coords(ctx, xyz_el, n_el, nel, &dc))) return st;
+  void *d_hist;
+  size_t bytes = sizeof(unsigned long long) * (size_t)xns_npairs(nel) * nhist;
+  if ((st = xns_scratch(ctx, SLOT_HIST, bytes, &d_hist))) return st;
+  if ((st = xns_timer_start(ctx))) return st;
+  if ((st = xns_hist_device_shard(ctx, dc, nhist, bin, 0, 1, (unsigned long long *)d_hist, max_tile_pairs))) return st;
   if ((st = xns_timer_stop(ctx))) return st;
   XNS_CUDA(ctx, cudaMemcpyAsync(hist, d_hist, bytes, cudaMemcpyDeviceToHost, ctx->stream));
   XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

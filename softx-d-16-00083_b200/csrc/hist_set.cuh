@@ -20,10 +20,14 @@ struct HistSet {
 // shard / nshard: this plan counts only its share of the tile pairs (every nshard-th run of the
 // size-sorted run list and every nshard-th wide tile pair); the shares of shards 0..nshard-1 add up to
 // the whole histogram exactly.
+// w_begin / max_pairs: this plan takes the tile pairs [w_begin, w_begin + max_pairs) of the structure's
+// enumeration (0: all of them, fewer than 2^32); the passes of a large structure add into one histogram.
 struct HistTuning {
   uint32_t cell_target = 56;
   uint32_t win = 45 * 1024 + 512;
   uint32_t shard = 0, nshard = 1;
+  unsigned long long w_begin = 0, max_pairs = 0;
+  bool ordered = false;  // atoms of each cell in input order (same tiles in every pass or shard)
 };
 
 // Everything the counting kernels need, built by xns_hist_plan; the buffers it points to live in the
@@ -35,6 +39,8 @@ struct HistLaunch {
   unsigned int *flags = nullptr;          // [0] pairs beyond nhist, [1] run queue
   uint32_t classes = 0, nranges = 0, window_grid = 0, wide = 0;
   size_t window_smem = 0;
+  unsigned long long ntp_total = 0;       // tile pairs of the whole structure (all passes)
+  bool zero_hist = true;                  // the counting launches clear the histogram first
 };
 
 // d_hist receives classes x nhist u64 counts; structure s owns classes [sum_{s'<s} P(nel_s'),
@@ -46,6 +52,9 @@ int xns_hist_plan(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, u
                   const HistTuning &tune, HistLaunch *L);
 int xns_hist_enqueue(xns_ctx *ctx, const HistLaunch &L);
 int xns_hist_check(xns_ctx *ctx, const HistLaunch &L);
-// One shard of a structure's histogram on device coordinates (plan, count, check).
+// Tile pairs per pass of the one-structure histogram entry points (16 bytes of device memory each).
+constexpr unsigned long long XNS_HIST_PASS_PAIRS = 1ull << 28;
+// One shard of a structure's histogram on device coordinates (plan, count, check), in passes of at most
+// max_pairs tile pairs (0: XNS_HIST_PASS_PAIRS).
 int xns_hist_device_shard(xns_ctx *ctx, const DevCoords &dc, uint32_t nhist, double bin, uint32_t shard, uint32_t nshard,
-                          unsigned long long *d_hist);
+                          unsigned long long *d_hist, unsigned long long max_pairs = 0);

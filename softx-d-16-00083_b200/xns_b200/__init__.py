@@ -91,6 +91,7 @@ lib.xns_binning_correction.argtypes = [_p, _p, _p, _u32, _dbl, _p, _u32, _dbl, _
 lib.xns_build_atoms.argtypes = [_p, _p, _u32, _u32, C.c_uint64, _p, _p, C.POINTER(_p)]
 lib.xns_copy_atoms.argtypes = [_p, _PP]
 lib.xns_rearrangement_int.argtypes = [_p, _p, _p, _u32, _p, _u32, _u32, _int, _PP, _p, _int, _int, _dbl, _u32]
+lib.xns_calc_hist_passes.argtypes = [_p, _PP, _p, _u32, _u32, _dbl, C.c_uint64, _p]
 lib.xns_write_i.argtypes = [C.c_char_p, _p, _p, _u32]
 lib.xns_write_i2.argtypes = [C.c_char_p, _p, _u32, _u32]
 lib.xns_write_pdf.argtypes = [C.c_char_p, _p, _u32, _dbl, _int]
@@ -332,6 +333,14 @@ class Context:
         el = _Elements(elements)
         out = np.zeros(el.nel * (el.nel + 1) // 2 * nhist, dtype=np.uint64)
         self._check(lib.xns_calc_hist(self._h, el.table, _ptr(el.n_el), el.nel, nhist, bin, _ptr(out)))
+        return out
+
+    def calc_hist_passes(self, elements, nhist, bin, max_tile_pairs):
+        """calc_hist taking the spatial plan's tile pairs at most max_tile_pairs per pass."""
+        el = _Elements(elements)
+        out = np.zeros(el.nel * (el.nel + 1) // 2 * nhist, dtype=np.uint64)
+        self._check(lib.xns_calc_hist_passes(self._h, el.table, _ptr(el.n_el), el.nel, nhist, bin, max_tile_pairs,
+                                             _ptr(out)))
         return out
 
     def calc_int_1d_hist(self, hist, n_el, nhist, bin, q, source, ff=None, sl=None, polar=False, lam=0.0):

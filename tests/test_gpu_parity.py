@@ -161,3 +161,14 @@ def test_2d_golden(gpu_ctx, name):
                                  float(g["lam"]), int(g["source"]), ff=g.get("ff"), sl=g.get("sl"), polar=bool(g["polar"]))
     assert rel_err_floor(I2D, g["I2D"], FLOOR_2D) < TOL_2D
     assert rel_err(I, g["I"]) < TOL_2D
+
+
+@pytest.mark.parametrize("max_pairs", [1000, 12345, 1 << 20])
+def test_hist_in_passes(gpu_ctx, oracle, max_pairs):
+    """the tile pairs taken a few at a time (as for structures whose tile-pair list would not fit the
+    device): the passes add up to the one-pass histogram, bit for bit"""
+    els = synth.rocksalt_cube(cells=7, seed=12)
+    nh = synth.hist_size(els, 0.001)
+    one = gpu_ctx.calc_hist(els, nh, 0.001)
+    assert np.array_equal(gpu_ctx.calc_hist_passes(els, nh, 0.001, max_pairs), one)
+    assert np.array_equal(one, oracle.hist(els, nh, 0.001))
