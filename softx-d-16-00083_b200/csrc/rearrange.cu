@@ -183,7 +183,6 @@ extern "C" int xns_rearrangement_int(xns_ctx *ctx, double *I0, const double *q, 
     for (uint32_t k = 0; k < nn; k++)
       if (B.neighb_id[k] >= nel) return xns_fail(ctx, XNS_ERR_ARG, "rearrangement_int: neighbour element id >= nel");
   }
-  int st;
   double *d_w;
   XNS_RTRY(xns_upload_weights(ctx, nel, nq, source, ff, sl, &d_w));
   Scratch sc(ctx);
@@ -260,6 +259,5 @@ extern "C" int xns_rearrangement_int(xns_ctx *ctx, double *I0, const double *q, 
   XNS_RTRY(xns_timer_stop(ctx));
   XNS_CUDA(ctx, cudaMemcpyAsync(I0, d_I0, n0 * sizeof(double), cudaMemcpyDeviceToHost, s));
   XNS_CUDA(ctx, cudaStreamSynchronize(s));
-  (void)st;
   return XNS_OK;
 }
