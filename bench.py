@@ -792,6 +792,11 @@ def build_workload(args):
         line["cpu_baseline"] = {"value": m * (m - 1) // 2 / dt, "unit": "pairs/s", "cores": 1, "kind": kind,
                                 "sample": "block::calcAtoms on an atom-list block of %d sites of the same generator, "
                                           "%.2f s (the reference's builder is single-threaded)" % (m, dt)}
+        # the crystal case through the reference's builder as well
+        for name, b, nel in (("rock-salt 30^3 cells, 10% vacancies, sigma 0.07 A", synth.rocksalt_block(30), 2),):
+            t = time.perf_counter()
+            (R.calc_atoms([b], nel) if kind == "reference" else R.build_atoms([b], nel, 1))
+            extra[name]["reference_ms"] = (time.perf_counter() - t) * 1e3
     print(json.dumps(line))
     ctx.close()
     return 0
