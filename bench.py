@@ -445,6 +445,26 @@ def ours(args, rank, world, local_rank):
     if world == 1 and not args.no_cpu_baseline:
         v, kind, cores, sample, _ = cpu_reference_sample()
         line["cpu_baseline"] = {"value": v, "unit": "pairs/s", "cores": cores, "kind": kind, "sample": sample}
+        # the full-size pattern against FP64: I(q) against the reference's calcInt1DHist of the same
+        # histogram, the rPDF against the oracle's PDF of it (bit for bit), every pair counted once
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as orc
+        step_device()
+        torch.cuda.synchronize()
+        h = d_hist.cpu().numpy().view(np.uint64)
+        I_ours, pdf_ours = d_I.cpu().numpy(), d_pdf.cpu().numpy()
+        try:
+            R, rk = orc.Reference(threads=cores), "reference calcInt1DHist"
+        except FileNotFoundError:
+            R, rk = orc.Oracle(), "oracle port of calcInt1DHist"
+        I_ref = R.int_1d_hist(h, n_el, nh, BIN, q, 0, sl=SL)
+        rel = np.abs(I_ours - I_ref) / np.abs(I_ref)
+        pdf_ref = orc.Oracle().pdf(h, n_el, nh, BIN, 2, p0, SL)
+        line["max_rel_err_vs_reference"] = {
+            "iq": float(rel.max()), "iq_q_at_max": float(q[int(rel.argmax())]), "iq_checker": rk,
+            "iq_points_above_1e-5": int((rel > 1e-5).sum()), "iq_points": int(len(q)),
+            "rpdf_identical_to_oracle": bool(np.array_equal(pdf_ours, pdf_ref)),
+            "histogram_counts_every_pair_once": bool(int(h.sum()) == pairs)}
     print(json.dumps(line))
     ctx.close()
     return 0
@@ -700,6 +720,19 @@ def twod_workload(args):
         line["cpu_baseline"] = {"value": n * rows * nfi_s / dt, "unit": "(atom, q-point) terms/s", "cores": cores,
                                 "kind": kind, "sample": "calcInt2D on %d q rows x %d phi, all %d atoms, %.2f s"
                                                         % (rows, nfi_s, n, dt)}
+        # sampled points of the full-size plane against the FP64 sum over all atoms (the oracle's restatement of
+        # the reference's amplitude sum at q_z = 0): 64 columns of two rows
+        Ip = ctx.calc_amp_plane(els, -8.0, dq, nq, -8.0, dq, nq, xns_b200.XRAY, coef=coef).reshape(nq, nq)
+        O = orc.Oracle()
+        errs = []
+        for iy in (nq // 3, nq // 2 + 7):
+            cols = slice(nq // 4, nq // 4 + 64)
+            ref = O.amp_plane(els, -8.0 + (nq // 4) * dq, dq, 64, -8.0 + iy * dq, dq, 1, xns_b200.XRAY, coef=coef).ravel()
+            got = Ip[iy, cols]
+            floor = 1e-2 * float(np.median(np.abs(ref)))
+            errs.append(float(np.max(np.abs(got - ref) / np.maximum(np.abs(ref), floor))))
+        line["max_rel_err_vs_fp64"] = {"plane_sampled_points": 128, "max": max(errs),
+                                       "note": "relative, denominator floored at 1 % of the sampled median"}
     print(json.dumps(line))
     ctx.close()
     return 0
