@@ -1130,11 +1130,11 @@ int xns_hist_enqueue(xns_ctx *ctx, const HistLaunch &L) {
   HistParams hp;
   memcpy(&hp, L.params, sizeof(hp));
   if (L.nranges) {
-    static bool attr = false;
-    if (!attr) {
+    static bool attr[XNS_MAX_DEVICES] = {};  // the attribute is per device; set once on each
+    if (ctx->device < 0 || ctx->device >= XNS_MAX_DEVICES || !attr[ctx->device]) {
       const int max_smem = (int)(sizeof(uint32_t) * (WIN_MAX + 32) + (size_t)WARP_STAGE * HW_WARPS);
       XNS_CUDA(ctx, cudaFuncSetAttribute(hist_window_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
-      attr = true;
+      if (ctx->device >= 0 && ctx->device < XNS_MAX_DEVICES) attr[ctx->device] = true;
     }
     hist_window_kernel<<<L.window_grid, HW_THREADS, L.window_smem, ctx->stream>>>(hp);
     XNS_LAUNCHED(ctx);

@@ -369,10 +369,10 @@ __global__ void max_count_kernel(const unsigned long long *__restrict__ hist, ui
 // given number of CTAs.
 template <class E>
 int launch_digit_gemm(xns_ctx *ctx, const XArgs &g, unsigned grid) {
-  static bool attr_set = false;
-  if (!attr_set) {
+  static bool attr_set[XNS_MAX_DEVICES] = {};  // the attribute is per device; set once on each
+  if (ctx->device < 0 || ctx->device >= XNS_MAX_DEVICES || !attr_set[ctx->device]) {
     XNS_CUDA(ctx, cudaFuncSetAttribute(sinc_exact_kernel<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, E::SMEM));
-    attr_set = true;
+    if (ctx->device >= 0 && ctx->device < XNS_MAX_DEVICES) attr_set[ctx->device] = true;
   }
   const unsigned long long units = (unsigned long long)g.NT * g.MT * g.KT;
   if (!grid) grid = (unsigned)std::min<unsigned long long>((unsigned long long)ctx->num_sms, units);

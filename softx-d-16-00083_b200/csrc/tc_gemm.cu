@@ -241,10 +241,10 @@ int xns_tc_pack_counts(xns_ctx *ctx, const unsigned long long *d_hist, uint32_t 
 }
 
 int xns_tc_sinc_gemm(xns_ctx *ctx, const GemmArgs &g, int grid) {
-  static bool attr_set = false;
-  if (!attr_set) {
+  static bool attr_set[XNS_MAX_DEVICES] = {};  // the attribute is per device; set once on each
+  if (ctx->device < 0 || ctx->device >= XNS_MAX_DEVICES || !attr_set[ctx->device]) {
     XNS_CUDA(ctx, cudaFuncSetAttribute(sinc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-    attr_set = true;
+    if (ctx->device >= 0 && ctx->device < XNS_MAX_DEVICES) attr_set[ctx->device] = true;
   }
   if (g.BN < 16 || g.BN > BN_MAX || g.BN % 16) return xns_fail(ctx, XNS_ERR_ARG, "sinc GEMM: column tile not in 16..256");
   const unsigned long long units = (unsigned long long)g.NT * g.MT * g.KT;

@@ -9,6 +9,7 @@
 #include "xns_b200.h"
 
 #define XNS_PI 3.1415926535897932384626433832795028841971693993  // typedefs.h:73
+#define XNS_MAX_DEVICES 64  // devices tracked by the once-per-device kernel attribute settings
 
 // Scratch slots: each is a grow-only device buffer owned by the context.
 enum ScratchSlot {
