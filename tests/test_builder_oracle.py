@@ -185,3 +185,45 @@ def test_molecule_rotation_and_displacement_match_reference_in_distribution():
     bo, br = xo[1] - xo[0], xr[1] - xr[0]
     assert ks_2samp(bo[:, 2], br[:, 2]).pvalue > 1e-4
     assert ks_2samp(np.arctan2(bo[:, 1], bo[:, 0]), np.arctan2(br[:, 1], br[:, 0])).pvalue > 1e-4
+
+
+def random_draw_free_block(seed):
+    """A random block whose build draws nothing that matters: occupancies 0 or 1 (a site's draw decides
+    nothing then), no displacements, no molecule rotation; triclinic cell, random symmetry operations
+    (orthogonal rotations with random translations, so some sites land on others), 1-4 cells per axis
+    (up to 125 merge translations), 1-3 copies with random rotations, random cut-offs."""
+    rng = np.random.default_rng(seed)
+    e = np.diag(rng.uniform(2.5, 6.0, 3)) + np.triu(rng.uniform(-1.0, 1.0, (3, 3)), 1)
+    natom = int(rng.integers(1, 7))
+    nid = int(rng.integers(1, min(natom, 3) + 1))
+    cuts = np.sort(rng.choice(np.arange(1, natom), nid - 1, replace=False)) if nid > 1 else np.array([], int)
+    natom_el = np.diff(np.concatenate([[0], cuts, [natom]]))
+    ids = rng.choice(4, nid, replace=False)
+    frac = rng.uniform(0, 1, (natom, 3))
+    if natom > 1:  # a site planted near another, possibly across a cell boundary
+        frac[-1] = (frac[0] + rng.normal(0, 0.03, 3)) % 1.0
+    symm = [(np.eye(3), np.zeros(3))]
+    for _ in range(int(rng.integers(0, 4))):
+        qm, _r = np.linalg.qr(rng.normal(size=(3, 3)))
+        symm.append((qm, rng.choice([0.0, 0.5], 3)))
+    ncell = tuple(int(c) for c in rng.integers(1, 5, 3))
+    occ = rng.choice([0.0, 1.0], natom, p=[0.2, 0.8])
+    ncopy = int(rng.integers(1, 4))
+    r_copy = rng.uniform(-30, 30, (ncopy, 3))
+    cf = [np.linalg.qr(rng.normal(size=(3, 3)))[0] for _ in range(ncopy)]
+    kw = dict(r_copy=r_copy, cf=cf)
+    if rng.random() < 0.5:
+        kw["rcut"] = float(rng.uniform(3, 15))
+    if rng.random() < 0.3:
+        kw["rcut_copies"] = float(rng.uniform(10, 50))
+    return Block.crystal(e, frac, natom_el, ids, ncell, symm=symm, occ=occ, centered=bool(rng.random() < 0.5), **kw)
+
+
+@needs_reference
+@pytest.mark.parametrize("seed", range(40))
+def test_random_draw_free_blocks_match_reference(seed):
+    b = random_draw_free_block(seed)
+    xo, nao = oracle().build_atoms([b], 4, seed=seed)
+    xr, nar = reference().calc_atoms([b], 4)
+    assert np.array_equal(nao, nar)
+    assert same(xo, xr)

@@ -9,7 +9,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from test_builder_oracle import FCC, draw_free_cases, oracle, rocksalt
+from test_builder_oracle import FCC, draw_free_cases, oracle, random_draw_free_block, rocksalt
 from xns_b200.structure import Block
 
 pytestmark = pytest.mark.gpu
@@ -174,3 +174,13 @@ def test_empty_inputs(gpu_ctx):
         assert np.array_equal(a, c)
     xg, ng, _, _ = _build(gpu_ctx, [rocksalt((3, 3, 3), occ=[0.0, 0.0])], 2, 4)
     assert [len(x) for x in xg] == [0, 0] and list(ng) == [0, 0]
+
+
+@pytest.mark.parametrize("seed", range(40))
+def test_random_draw_free_blocks_bit_exact(gpu_ctx, seed):
+    b = random_draw_free_block(seed)
+    xg, ng, _, _ = _build(gpu_ctx, [b], 4, seed)
+    xo, no = oracle().build_atoms([b], 4, seed=seed)
+    assert np.array_equal(ng, no)
+    for a, c in zip(xg, xo):
+        assert np.array_equal(a, c)
