@@ -79,3 +79,56 @@ def test_gpu_matches_oracle(gpu_ctx, name):
     # the GPU adds the terms in an order set by atomics, and the correction cancels terms some 1e4 times
     # its result: FP64 rounding leaves a few 1e-12 of relative difference
     assert np.allclose(g[fin], o[fin], rtol=1e-10, atol=0)
+
+
+def random_case(seed):
+    """random blocks (1-3 elements, 5-80 sites, 0-4 neighbours per site from a shifted copy and the
+    block itself, random Rcorr and coeff), neutron or X-ray, polar or not, partial or not"""
+    rng = np.random.default_rng(100 + seed)
+    nel = int(rng.integers(1, 4))
+    nb = int(rng.integers(1, 4))
+    blocks = []
+    for b in range(nb):
+        n = int(rng.integers(5, 81))
+        r = rng.uniform(-6, 6, (n, 3))
+        k = int(rng.integers(1, nel + 1))
+        cuts = np.sort(rng.choice(np.arange(1, n), k - 1, replace=False)) if k > 1 else np.array([], int)
+        ne = np.diff(np.concatenate([[0], cuts, [n]]))
+        ids = rng.choice(nel, k, replace=False)
+        shift = rng.uniform(-12, 12, 3)
+        neigh = []
+        for i in range(n):
+            m = int(rng.integers(0, 5))
+            js = rng.choice(n, m)
+            neigh.append([tuple(r[j] + (shift if rng.random() < 0.5 else 0.0) + rng.normal(0, 0.3, 3)) +
+                          (int(rng.integers(0, nel)),) for j in js])
+        blocks.append(RearrBlock(r, ne, ids, neigh, float(rng.uniform(0, 1.5)), int(rng.integers(1, 30)),
+                                 bool(rng.random() < 0.8)))
+    nq = 150
+    q = np.linspace(0.05, 15.0, nq)
+    partial = bool(rng.random() < 0.5)
+    n0 = nq * (1 + nb * (nb + 1) // 2) if partial else nq
+    source = int(rng.integers(0, 2))
+    return dict(I0=1.0 + rng.random(n0), q=q, blocks=blocks, nel=nel, source=source,
+                ff=2.0 + rng.random((nel, nq)) if source == 1 else None,
+                sl=rng.uniform(-4, 10, nel) if source == 0 else None, partial=partial,
+                polar=bool(rng.random() < 0.5), lam=float(rng.uniform(0.5, 2.0)), ntot=int(rng.integers(100, 20000)))
+
+
+@needs_reference
+@pytest.mark.parametrize("seed", range(12))
+def test_random_cases_oracle_matches_reference(seed):
+    c = random_case(seed)
+    assert np.array_equal(_run(Oracle(), c), _run(Reference(), c), equal_nan=True)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", range(12))
+def test_random_cases_gpu_matches_oracle(gpu_ctx, seed):
+    c = random_case(seed)
+    g, o = _run(gpu_ctx, c), _run(Oracle(), c)
+    fin = np.isfinite(o)
+    assert np.array_equal(fin, np.isfinite(g))
+    # relative to the correction's scale at each q as well as to I0 itself: the correction can cancel
+    scale = np.maximum(np.abs(o[fin]), 1e-3 * np.max(np.abs(o[fin])))
+    assert np.max(np.abs(g[fin] - o[fin]) / scale) < 1e-10
