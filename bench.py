@@ -245,7 +245,7 @@ def reference_workload_arm(args, rank):
         units = n * rows * nfi
         step = lambda: R.int_2d(els, q[:rows], nfi, [0, 0, 0], [0, 0, 0], [1, 1, 1], 5, 0.01, 1,  # noqa: E731
                                 ff=ff[:, :rows])
-        metric, unit = "(atom, q-point) terms/s", "terms/s"
+        metric, unit = "terms/s", "(atom, q-point) terms/s"
         sample = "calcInt2D on %d q rows x %d phi, all %d atoms, %d threads" % (rows, nfi, n, cores)
     elif w == "batch":
         structs, ns, _ = synth.sphere_ensemble(count=args.batch_count, seed=0)
