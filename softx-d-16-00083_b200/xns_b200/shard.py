@@ -69,7 +69,9 @@ def pdf_and_debye(ctx, xyz_dev, n_el, nhist, bin, scenario, pdftype, p0, q, sour
                                           rank, world, _p(hist_dev.data_ptr())))
     if world > 1:
         reduce_histogram(hist_dev, group)
-        hist_dev.device.type == "cuda" and __import__("torch").cuda.current_stream(hist_dev.device).synchronize()
+        if hist_dev.device.type == "cuda":  # the library's stream may differ from torch's: let the sum land
+            import torch
+            torch.cuda.current_stream(hist_dev.device).synchronize()
     _check(ctx, lib.xns_pdf_and_debye_from_hist_device(
         ctx.handle, _p(hist_dev.data_ptr()), n_el.ctypes.data_as(_p), nel, nhist, bin, scenario, pdftype, p0,
         q.ctypes.data_as(_p), len(q), source, ffp, None if sl is None else sl.ctypes.data_as(_p), int(polar), lam,
