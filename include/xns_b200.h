@@ -69,7 +69,8 @@ double xns_last_stage_ms(const xns_ctx *ctx, int stage);
 
 /* Pair-distance histogram.  Replaces calcHist (CalcFunctions.cpp:757-809) and calcHistCuda
  * (CalcFunctionsCUDA.cu:855-920).  hist: P*nhist counts, bit-identical to the reference's FP64
- * (unsigned int)(|ri-rj|/bin).  XNS_ERR_RANGE if some distance maps to a bin >= nhist. */
+ * (unsigned int)(|ri-rj|/bin).  XNS_ERR_RANGE if some distance maps to a bin >= nhist.  Structures of
+ * any size: beyond 2^28 tile pairs (about 2e6 atoms) the count runs in passes (xns_calc_hist_passes). */
 int xns_calc_hist(xns_ctx *ctx, const double *const *xyz_el, const uint32_t *n_el, uint32_t nel, uint32_t nhist, double bin,
                   uint64_t *hist);
 
