@@ -320,41 +320,48 @@ __device__ __forceinline__ uint32_t pair_key(const KeyParams &p, unsigned long l
 
 // Consecutive tile pairs (a tile against its neighbours' tiles) mostly share a distance bucket, so the
 // lanes of a warp group by key (match.any) and one lane per key does the warp's atomic.
-__global__ void pair_key_kernel(KeyParams p, uint32_t *__restrict__ kcnt) {
+// The key pass decodes every tile pair once, counts its key and keeps the tile pair and key (tmp, tkey:
+// indexed by the pass-local w; key ~0u for a tile pair of another shard); the scatter pass only moves them.
+__global__ void pair_key_kernel(KeyParams p, uint32_t *__restrict__ kcnt, TilePair *__restrict__ tmp,
+                                uint32_t *__restrict__ tkey) {
   const uint32_t lane = threadIdx.x & 31;
   const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
   for (unsigned long long w0 = blockIdx.x * (unsigned long long)blockDim.x + (threadIdx.x & ~31u); w0 < p.ntp;
        w0 += stride) {
-    const unsigned long long w = p.wbeg + w0 + lane;
-    const bool act = w0 + lane < p.ntp && (p.nshard == 1 || w % p.nshard == p.shard);
+    const unsigned long long wl = w0 + lane, w = p.wbeg + wl;
+    const bool act = wl < p.ntp && (p.nshard == 1 || w % p.nshard == p.shard);
     const unsigned act_mask = __ballot_sync(0xffffffffu, act);
     if (act) {
       TilePair tp;
       const uint32_t key = pair_key(p, w, &tp);
       const unsigned same = __match_any_sync(act_mask, key);
       if (lane == (uint32_t)(__ffs(same) - 1)) atomicAdd(kcnt + key, (uint32_t)__popc(same));
+      tmp[wl] = tp;
+      tkey[wl] = key;
+    } else if (wl < p.ntp) {
+      tkey[wl] = 0xffffffffu;
     }
   }
 }
 
 __global__ void pair_scatter_kernel(KeyParams p, const uint32_t *__restrict__ koff, uint32_t *__restrict__ kcur,
+                                    const TilePair *__restrict__ tmp, const uint32_t *__restrict__ tkey,
                                     TilePair *__restrict__ list) {
   const uint32_t lane = threadIdx.x & 31;
   const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
   for (unsigned long long w0 = blockIdx.x * (unsigned long long)blockDim.x + (threadIdx.x & ~31u); w0 < p.ntp;
        w0 += stride) {
-    const unsigned long long w = p.wbeg + w0 + lane;
-    const bool act = w0 + lane < p.ntp && (p.nshard == 1 || w % p.nshard == p.shard);
+    const unsigned long long wl = w0 + lane;
+    const uint32_t key = wl < p.ntp ? tkey[wl] : 0xffffffffu;
+    const bool act = key != 0xffffffffu;
     const unsigned act_mask = __ballot_sync(0xffffffffu, act);
     if (act) {
-      TilePair tp;
-      const uint32_t key = pair_key(p, w, &tp);
       const unsigned same = __match_any_sync(act_mask, key);
       const uint32_t leader = (uint32_t)(__ffs(same) - 1);
       uint32_t at = 0;
       if (lane == leader) at = atomicAdd(kcur + key, (uint32_t)__popc(same));
       at = __shfl_sync(same, at, leader) + (uint32_t)__popc(same & ((1u << lane) - 1u));
-      list[koff[key] + at] = tp;
+      list[koff[key] + at] = tmp[wl];
     }
   }
 }
@@ -1062,11 +1069,15 @@ int xns_hist_plan(xns_ctx *ctx, const HistSet &hs, uint32_t nhist, double bin, u
   XNS_CUDA(ctx, cudaMemsetAsync(d_kcnt, 0, sizeof(uint32_t) * kp.nkeys, ctx->stream));
   XNS_CUDA(ctx, cudaMemsetAsync(d_kcur, 0, sizeof(uint32_t) * kp.nkeys, ctx->stream));
   const int kgrid = ctx->num_sms * 8;
-  pair_key_kernel<<<kgrid, 256, 0, ctx->stream>>>(kp, d_kcnt);
+  void *vt;
+  if ((st = xns_scratch(ctx, SLOT_HTMP, (sizeof(TilePair) + sizeof(uint32_t)) * ntp, &vt))) return st;
+  TilePair *d_tmp = (TilePair *)vt;
+  uint32_t *d_tkey = (uint32_t *)(d_tmp + ntp);
+  pair_key_kernel<<<kgrid, 256, 0, ctx->stream>>>(kp, d_kcnt, d_tmp, d_tkey);
   XNS_LAUNCHED(ctx);
   scan_kernel<<<1, SCAN_THREADS, 0, ctx->stream>>>(d_kcnt, kp.nkeys, d_koff, nullptr, d_ktot);
   XNS_LAUNCHED(ctx);
-  pair_scatter_kernel<<<kgrid, 256, 0, ctx->stream>>>(kp, d_koff, d_kcur, d_list);
+  pair_scatter_kernel<<<kgrid, 256, 0, ctx->stream>>>(kp, d_koff, d_kcur, d_tmp, d_tkey, d_list);
   XNS_LAUNCHED(ctx);
   // cut the sorted list into runs of one class: about 4 runs per SM over the whole list, so that the
   // queue balances uneven classes; a CTA's u32 window counts at most 64*64*entries pairs per bin, so a

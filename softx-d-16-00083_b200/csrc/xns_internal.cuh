@@ -28,6 +28,7 @@ enum ScratchSlot {
   SLOT_HCELL,           // histogram plan: per-cell counts, offsets, cursors
   SLOT_HTILE,           // histogram plan: tiles (atom ranges with bounding boxes)
   SLOT_HLIST,           // histogram plan: tile pairs sorted by (element pair, distance bucket)
+  SLOT_HTMP,            // histogram plan: tile pairs and keys in enumeration order (before the sort)
   SLOT_HKEY,            // histogram plan: bucket counts / offsets and small tables
   SLOT_TC_A,            // split-BF16 sinc matrix (hi and lo planes, tensor-core tile order)
   SLOT_TC_B,            // split-BF16 histogram columns (hi and lo planes)
