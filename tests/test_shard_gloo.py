@@ -134,3 +134,41 @@ def test_two_rank_2d_gather(tmp_path):
     want = np.concatenate([np.arange(21, dtype=np.float64), -np.arange(7, dtype=np.float64)])
     for r in range(WORLD):
         assert np.array_equal(np.load(os.path.join(tmp_path, "g%d.npy" % r)), want)
+
+
+def _debye_main(rank, port, out_dir):
+    """two gloo ranks run xns_b200.shard.int_debye with each rank's shard of the sum given directly"""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(WORLD))
+    sys.path.insert(0, os.path.join(ROOT, "softx-d-16-00083_b200"))
+    import datetime
+
+    import torch.distributed as tdist
+
+    from xns_b200 import shard
+    tdist.init_process_group("gloo", rank=rank, world_size=WORLD, timeout=datetime.timedelta(seconds=60))
+    try:
+        # stands in for the library: shard s holds (s + 1) / 3 of a pattern, so the two sum to it
+        def fake_shard(ctx, elements, q, source, sl, ff, polar, lam, s_, n, neb):
+            return (s_ + 1) / 3.0 * np.linspace(1.0, 2.0, len(q))
+        shard.int_debye_shard = fake_shard
+        I = shard.int_debye(None, [], np.arange(5, dtype=np.float64), 0, rank=rank, world=WORLD)
+        np.save(os.path.join(out_dir, "d%d.npy" % rank), I)
+    finally:
+        tdist.destroy_process_group()
+
+
+def test_two_rank_debye_all_reduce(tmp_path):
+    import torch.multiprocessing as mp
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=_debye_main, args=(r, port, str(tmp_path))) for r in range(WORLD)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        if p.is_alive():
+            p.kill()
+            pytest.fail("a rank did not finish")
+        assert p.exitcode == 0
+    for r in range(WORLD):
+        assert np.allclose(np.load(os.path.join(tmp_path, "d%d.npy" % r)), np.linspace(1.0, 2.0, 5), rtol=0, atol=1e-15)
