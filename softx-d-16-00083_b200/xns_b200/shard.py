@@ -4,8 +4,8 @@ Debye double sum (int_debye): each rank sums its tile pairs (xns_calc_int_debye_
 on rank 0 only) and an all-reduce of the nq FP64 values gives every rank the whole I(q).
 
 Histogram path:
-Each rank counts its shard of the pair-distance histogram (xns_hist_shard_device: every N-th run of the
-whole structure's plan), an all-reduce sums the shards (NCCL over NVLink / NVSwitch on GPUs, gloo on
+Each rank counts its shard of the pair-distance histogram (xns_hist_shard_device: the tile pairs w of
+the whole structure's plan with w mod N = rank), an all-reduce sums the shards (NCCL over NVLink / NVSwitch on GPUs, gloo on
 CPU), and every rank derives the PDF and I(q) from the sum (xns_pdf_and_debye_from_hist_device).  The
 counts are integers, so the sum is the one-GPU histogram bit for bit, as the reference's MPI_Reduce of
 its per-rank rij_hist is (CalcFunctions.cpp:804-807).  The exchange is P x nhist u64 (1.2 MB for the
@@ -106,10 +106,10 @@ def int_debye_shard(ctx, elements, q, source, sl=None, ff=None, polar=False, lam
 def int_debye(ctx, elements, q, source, sl=None, ff=None, polar=False, lam=0.0, rank=0, world=1, group=None,
               n_el_block=None):
     """calcIntDebye for one structure split over the ranks of group; every rank returns the whole I(q)."""
-    import torch
     part = int_debye_shard(ctx, elements, q, source, sl, ff, polar, lam, rank, world, n_el_block)
     if world == 1:
         return part
+    import torch
     import torch.distributed as dist
     dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" else torch.device("cpu")
     t = torch.from_numpy(part).to(dev)
