@@ -231,7 +231,7 @@ int xns_calc_amp_plane(xns_ctx *ctx, const double *const *xyz_el, const uint32_t
  * calcHist (:757-809, bit-exact) and the I(q) of calcInt1DHist (:810-911, exact transform, within 1e-5
  * of FP64).
  *
- * Inputs, for nstruct structures:
+ * Inputs, for nstruct structures (1..65535):
  *   nel[s]      elements of structure s; G = sum nel elements in all;
  *   n_el[g]     atoms of element g (structure-major, then element order), g < G;
  *   xyz         all atoms as packed x y z doubles in that order (sum n_el triples);

@@ -104,6 +104,8 @@ int batch_build(xns_batch *b, uint32_t nstruct, const uint32_t *nel, const uint3
   xns_ctx *ctx = b->ctx;
   if (!nel || !n_el || !xyz || !q || nstruct == 0 || nq == 0 || nhist == 0 || !(bin > 0))
     return xns_fail(ctx, XNS_ERR_ARG, "batch: null pointer or zero size");
+  // the transform's grid has one row of CTAs per structure
+  if (nstruct > 65535) return xns_fail(ctx, XNS_ERR_ARG, "batch: at most 65535 structures per batch");
   b->nstruct = nstruct;
   b->nq = nq;
   b->nhist = nhist;

@@ -87,24 +87,28 @@ __global__ void __launch_bounds__(SUM_Q) sum_entries_kernel(const Entry *__restr
                                                             double *__restrict__ I) {
   __shared__ Entry se[256];
   const uint32_t iq = blockIdx.x * SUM_Q + threadIdx.x;
-  const unsigned long long lo = (unsigned long long)blockIdx.y * SUM_CHUNK, hi = min(n, lo + SUM_CHUNK);
   const double qv = iq < nq ? q[iq] : 0.0;
   double acc = 0;
-  for (unsigned long long c = lo; c < hi; c += 256) {
-    __syncthreads();
-    for (uint32_t k = threadIdx.x; k < 256 && c + k < hi; k += SUM_Q) se[k] = e[c + k];
-    __syncthreads();
-    if (iq < nq) {
-      const uint32_t m = (uint32_t)(hi - c < 256 ? hi - c : 256);
-      for (uint32_t k = 0; k < m; k++) {
-        const double qr = se[k].r * qv;
-        const double wt = __dmul_rn(__dmul_rn(coeff, w[(size_t)se[k].a * nq + iq]), w[(size_t)se[k].b * nq + iq]);
-        const double t = __ddiv_rn(__dmul_rn(wt, sin(qr)), __dadd_rn(qr, 0.00000001));
-        acc = se[k].sign > 0 ? __dadd_rn(acc, t) : __dsub_rn(acc, t);
+  // chunks blockIdx.y, blockIdx.y + gridDim.y, ...: the grid's y extent is capped at 65535
+  for (unsigned long long lo = (unsigned long long)blockIdx.y * SUM_CHUNK; lo < n;
+       lo += (unsigned long long)gridDim.y * SUM_CHUNK) {
+    const unsigned long long hi = min(n, lo + SUM_CHUNK);
+    for (unsigned long long c = lo; c < hi; c += 256) {
+      __syncthreads();
+      for (uint32_t k = threadIdx.x; k < 256 && c + k < hi; k += SUM_Q) se[k] = e[c + k];
+      __syncthreads();
+      if (iq < nq) {
+        const uint32_t m = (uint32_t)(hi - c < 256 ? hi - c : 256);
+        for (uint32_t k = 0; k < m; k++) {
+          const double qr = se[k].r * qv;
+          const double wt = __dmul_rn(__dmul_rn(coeff, w[(size_t)se[k].a * nq + iq]), w[(size_t)se[k].b * nq + iq]);
+          const double t = __ddiv_rn(__dmul_rn(wt, sin(qr)), __dadd_rn(qr, 0.00000001));
+          acc = se[k].sign > 0 ? __dadd_rn(acc, t) : __dsub_rn(acc, t);
+        }
       }
     }
   }
-  if (iq < nq && hi > lo) atomicAdd(I + iq, acc);
+  if (iq < nq && (unsigned long long)blockIdx.y * SUM_CHUNK < n) atomicAdd(I + iq, acc);
 }
 
 // PolarFactor1D (CalcFunctions.cpp:460-468) for one q
@@ -249,7 +253,7 @@ extern "C" int xns_rearrangement_int(xns_ctx *ctx, double *I0, const double *q, 
     XNS_LAUNCHED(ctx);
     neighbour_entries_kernel<<<tb, 128, 0, s>>>(rb, d_cnt + 1, d_e + cnt[0], cnt[1]);
     XNS_LAUNCHED(ctx);
-    const dim3 g((nq + SUM_Q - 1) / SUM_Q, (unsigned)((ne + SUM_CHUNK - 1) / SUM_CHUNK));
+    const dim3 g((nq + SUM_Q - 1) / SUM_Q, (unsigned)std::min<unsigned long long>((ne + SUM_CHUNK - 1) / SUM_CHUNK, 65535));
     sum_entries_kernel<<<g, SUM_Q, 0, s>>>(d_e, ne, d_q, nq, d_w, (double)B.coeff, slot);
     XNS_LAUNCHED(ctx);
   }

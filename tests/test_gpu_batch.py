@@ -88,3 +88,12 @@ def test_batch_range_error(gpu_ctx):
     with pytest.raises(xns_b200.XnsError) as e:
         gpu_ctx.calc_batch_debye_hist(structs, 100, 0.001, synth.q_mesh(0.1, 5.0, 64), 0, sl=sls)
     assert e.value.status == 4
+
+
+def test_batch_too_many_structures(gpu_ctx):
+    """The transform's grid has one row of CTAs per structure: 65536 structures are refused up front."""
+    import xns_b200
+    structs = [[np.zeros((1, 3))]] * 65536
+    with pytest.raises(xns_b200.XnsError) as e:
+        gpu_ctx.calc_batch_debye_hist(structs, 16, 0.01, synth.q_mesh(0.1, 5.0, 8), 0, sl=[[1.0]] * 65536)
+    assert e.value.status == 1
