@@ -97,30 +97,109 @@ def job_rate(world, units_per_rank, ms_max):
 
 # ---- clocks -----------------------------------------------------------------------------------------
 class Clocks:
+    """SM clock and throttle reasons during a timed region: NVML polled every 10 ms from a thread (the
+    CUDA device found by its PCI address), else nvidia-smi -lms 200 in a child process."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event reason bits (nvml.h nvmlClocksEventReason*)
+    REASON_BITS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+                   ("sw_power_cap", 0x4))
+    PERIOD_S = 0.01
 
-    def __init__(self, device):
+    def __init__(self, device, pci_bus_id=None):
         self.device = device
+        self.pci_bus_id = pci_bus_id
         self.proc = None
         self.path = None
+        self.nvml = None
+        self.thread = None
+        self.out = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        bus = self.pci_bus_id
+        if bus is None:
+            try:
+                import torch
+                if not torch.cuda.is_initialized():  # never the first CUDA call of a process (workers may fork)
+                    raise RuntimeError("CUDA not initialised")
+                pr = torch.cuda.get_device_properties(self.device)
+                bus = "%08X:%02X:%02X.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            except Exception:
+                bus = None
+        h = None
+        if bus is not None:
+            try:
+                h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            except Exception:
+                h = None
+        if h is None:
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.device)
+        return pynvml, h
+
+    def _poll(self, nv, h, stop, rows):
+        reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while True:
+            try:
+                rows.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), int(reasons(h))))
+            except Exception:
+                pass
+            if stop.wait(self.PERIOD_S):
+                return
 
     def start(self):
+        """Starts both samplers; stop() reports NVML's when it took samples, else nvidia-smi's."""
+        try:
+            import threading
+            nv, h = self._nvml_handle()
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.nvml = (nv, h, threading.Event(), [])
+            self.thread = threading.Thread(target=self._poll, args=self.nvml, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.nvml = None
+            self.thread = None
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
+            self.out = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
                                           "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            if self.out is not None:
+                self.out.close()
+            if self.path is not None:
+                os.unlink(self.path)
 
     def stop(self):
+        if self.nvml is not None:
+            self.nvml[2].set()
+            self.thread.join()
+        smi = self._stop_smi()
+        if self.nvml is not None:
+            nv, h, stop, rows = self.nvml
+            try:
+                nv.nvmlShutdown()
+            except Exception:
+                pass
+            if rows:
+                reasons = sorted({n for _, r in rows for n, bit in self.REASON_BITS if r & bit})
+                return {"sm_mhz": float(np.median([c for c, _ in rows])), "sm_max_mhz": self.max_mhz,
+                        "reasons": reasons, "samples": len(rows), "source": "nvml, 10 ms",
+                        "nvidia_smi": smi}
+        return smi
+
+    def _stop_smi(self):
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
         self.proc.wait()
+        self.out.close()
         rows = []
         for line in open(self.path):
             f = [x.strip() for x in line.split(",")]
@@ -134,7 +213,7 @@ class Clocks:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "source": "nvidia-smi, 200 ms"}
 
 
 # ---- CPU baseline ---------------------------------------------------------------------------------
