@@ -10,7 +10,7 @@ weights, FP32 accumulation, trained on the GPU by the library's own forward and 
 predicts them from the bin's neighbourhood in the coarse histogram.
 
 Training data come from the GPU: coarse histograms for the inputs, histograms 32x finer for the exact
-per-bin moments, and the exact Debye double sum (xns_calc_int_debye: no binning at all) as the judge.
+per-bin moments, and the exact Debye double sum (xns_calc_int_debye: no binning at all) as the arbiter.
 The integer histograms are never altered.  fit() holds structures out and records the largest relative
 error of the corrected I(q) against the double sum; predict() uses the network only where that
 validated error is within the tolerance, and otherwise returns the exact double sum for every structure.
@@ -120,7 +120,7 @@ class LearnedCorrector:
         p = np.clip(wts, 0, None)
         pick = rng.choice(len(p), size=min(samples, int((p > 0).sum()) * 4), p=p / p.sum())
         losses = [self.net.train(X[pick], Y[pick], batch=batch, epochs=1, lr=lr) for _ in range(epochs)]
-        # the judge: the exact double sum on the held-out structures
+        # the arbiter: the exact double sum on the held-out structures
         held = [structures[i] for i in va]
         I_x = exact_pass(self.ctx, held, [sls[i] for i in va], self.q)
         I_l = self.corrected(I_c[va], [hs[i] for i in va], s0[va])

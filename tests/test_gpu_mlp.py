@@ -1,6 +1,6 @@
 """The learned correction's perceptron: hand-written GPU forward / backward kernels against the FP64
 numpy oracle (oracle/mlp_oracle.py), training, and what the trained network gains over the coarse
-histogram alone -- with the exact Debye double sum as the judge and the fallback."""
+histogram alone -- with the exact Debye double sum as the arbiter and the fallback."""
 import numpy as np
 import pytest
 
