@@ -65,14 +65,18 @@ def npairs(els):
     return n * (n - 1) // 2
 
 
-def config_block(els, nh, extra=None, cells=CELLS):
-    c = {"workload": "DebyePDF rock-salt nanocube %d^3 cells a=%.2f A, %d atoms, hist bin %.3f A (%d bins x 3 pairs), "
-                     "rPDF, I(q) %d q in [%.1f,%.1f)" % (cells, A, sum(len(e) for e in els), BIN, nh, NQ, QMIN, QMAX),
-         "atoms": int(sum(len(e) for e in els)), "pairs_per_step": int(npairs(els)), "nhist": int(nh), "nq": NQ,
-         "l2": "flushed (512 MB write) before every timed step"}
-    if extra:
-        c.update(extra)
-    return c
+def config_block(els, nh, cells=CELLS):
+    """The workload's description, the same dict in both arms (seed 0)."""
+    return {"workload": "DebyePDF rock-salt nanocube %d^3 cells a=%.2f A, %d atoms, hist bin %.3f A (%d bins x 3 pairs), "
+                        "rPDF, I(q) %d q in [%.1f,%.1f)" % (cells, A, sum(len(e) for e in els), BIN, nh, NQ, QMIN, QMAX),
+            "atoms": int(sum(len(e) for e in els)), "pairs_per_step": int(npairs(els)), "nhist": int(nh), "nq": NQ,
+            "seed": 0, "l2": "flushed (512 MB write) before every timed step"}
+
+
+def hist_sha256(h):
+    """SHA-256 of u64 counts (little-endian): both arms print it for the full-size histogram."""
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(h, dtype="<u8").tobytes()).hexdigest()
 
 
 # ---- ranks ------------------------------------------------------------------------------------------
@@ -217,22 +221,21 @@ class Clocks:
 
 
 # ---- CPU baseline ---------------------------------------------------------------------------------
-def cpu_reference_sample(target_s=12.0):
-    """Times the reference's calcPDFandDebye (DebyePDF, rPDF, the same bin and q mesh) on a cube of the
-    same lattice, grown until one pass takes about target_s.  Returns (pairs/s, kind, cores, sample)."""
+def cpu_reference_sample(target_s=12.0, max_cells=CELLS):
+    """Times the reference's calcPDFandDebye (DebyePDF, rPDF, the same bin and q mesh) on the seed-0
+    cube, grown from 6^3 cells until one pass takes about target_s (the full 30^3 cells where the host
+    is fast enough).  Returns (pairs/s, kind, cores, sample, (cells, seconds))."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
     cores = os.cpu_count() or 1
     try:
         R = orc.Reference(threads=cores)
-        kind = "reference"
+        kind, O = "reference", None
     except FileNotFoundError:
-        R = None
-        kind = "port"
-    O = orc.Oracle()
+        R, kind, O = None, "port", orc.Oracle()
 
     def run(cells):
-        els, nh, q, p0 = workload(1000, cells)
+        els, nh, q, p0 = workload(0, cells)
         t = time.perf_counter()
         if R is not None:
             R.pdf_and_debye(els, nh, BIN, 4, 2, p0, q, 0, sl=SL)
@@ -242,15 +245,15 @@ def cpu_reference_sample(target_s=12.0):
             O.int_1d_hist(h, [len(e) for e in els], nh, BIN, q, 0, sl=SL)
         return time.perf_counter() - t, els
 
-    cells = 6
+    cells = min(6, max_cells)
     dt, els = run(cells)
-    while dt < target_s / 4 and cells < CELLS:
+    while dt < target_s / 4 and cells < max_cells:
         # pairs grow as cells^6, the transform as cells: step the size by the measured time
         grow = min(max((target_s / max(dt, 1e-3)) ** (1 / 6), 1.15), 1.8)
-        cells = min(CELLS, max(cells + 1, int(cells * grow)))
+        cells = min(max_cells, max(cells + 1, int(cells * grow)))
         dt, els = run(cells)
     pairs = npairs(els)
-    sample = ("one calcPDFandDebye pass (histogram + rPDF + I(q), %d q) on a %d^3-cell cube of the same lattice, %d atoms, "
+    sample = ("one calcPDFandDebye pass (histogram + rPDF + I(q), %d q) on the seed-0 cube of %d^3 cells, %d atoms, "
               "%.3g pairs, %.2f s" % (NQ, cells, sum(len(e) for e in els), pairs, dt))
     return pairs / dt, kind, cores, sample, (cells, dt)
 
@@ -259,10 +262,10 @@ def cpu_reference_sample(target_s=12.0):
 def reference_arm(args, rank, world):
     if rank != 0:
         return 0
-    v, kind, cores, sample, (cells, dt0) = cpu_reference_sample()
+    v, kind, cores, sample, (cells, dt0) = cpu_reference_sample(max_cells=args.cells)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
-    els, nh, q, p0 = workload(1000, cells)
+    els, nh, q, p0 = workload(0, cells)
     if kind == "reference":
         R = orc.Reference(threads=cores)
         step = lambda: R.pdf_and_debye(els, nh, BIN, 4, 2, p0, q, 0, sl=SL)  # noqa: E731
@@ -280,12 +283,20 @@ def reference_arm(args, rank, world):
         step()
     dt = (time.perf_counter() - t) / args.steps
     value = npairs(els) / dt
+    full, nh_full = workload(0, args.cells)[:2]
+    sample = sample if cells == args.cells else sample + " (a bounded sample of the full cube)"
     line = {"metric": METRIC, "value": value, "unit": "pairs/s", "impl": "reference", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": config_block(*workload(0)[:2], extra={"sample": sample, "reference_cells": cells}),
+            "config": config_block(full, nh_full, args.cells),
             "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    # the reference's histogram of the full cube (calcHist, untimed), hashed: our line prints the hash of
+    # ours for the same cube
+    R = orc.Reference(threads=cores) if kind == "reference" else orc.Oracle()
+    line["histogram_sha256"] = hist_sha256(R.hist(full, nh_full, BIN))
+    line["histogram_sha256_of"] = ("calcHist of the reference on the full %d-atom cube" % sum(len(e) for e in full)
+                                   if kind == "reference" else "the oracle port's histogram of the full cube")
     print(json.dumps(line))
     return 0
 
@@ -508,7 +519,7 @@ def ours(args, rank, world, local_rank):
                      "tensor-core transform with exact sums (I(q)); f64 (PDF)",
             "data": "synthetic (seeded)",
             "patterns_per_s": units / (ms_step * 1e-3),
-            "config": config_block(els, nh, {"parallelism": par}, args.cells),
+            "config": config_block(els, nh, args.cells), "parallelism": par,
             "stages_ms": {"histogram": hist_avg, "pdf": pdf_ms / args.steps, "iq": iq_ms / args.steps},
             "roofline": {"kernel": "hist_window_kernel", "bound": "smem_atomic", "achieved": inc, "peak": atom_peak.value,
                          "unit": "1e9 shared-memory increments/s", "frac": inc / atom_peak.value if atom_peak.value else None,
@@ -521,6 +532,21 @@ def ours(args, rank, world, local_rank):
             "e2e": {"value": job_rate(units, pairs, e2e_ms), "unit": "pairs/s", "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches), "clocks": clk}
+    # the full-size histogram, hashed (the reference arm prints the hash of the reference's calcHist for the
+    # same cube; tests/golden holds the one the reference's own code produced)
+    step_device()
+    torch.cuda.synchronize()
+    h_last = d_hist.cpu().numpy().view(np.uint64)
+    line["histogram_sha256"] = hist_sha256(h_last)
+    gpath = os.path.join(ROOT, "tests", "golden", "histhash__rocksalt30_seed0_b0.001.npz")
+    if args.cells == CELLS and rank == 0 and not args.shard and os.path.exists(gpath):
+        with np.load(gpath) as g:
+            line["histogram_matches_reference"] = {"equal": line["histogram_sha256"] == str(g["sha256"]),
+                                                   "reference_sha256": str(g["sha256"]),
+                                                   "source": "tests/golden/histhash__rocksalt30_seed0_b0.001.npz "
+                                                             "(calcHist of the reference, tests/golden/make_golden.py)"}
+    if world == 1 and not args.no_extra:
+        line.update(extra_rows(args))
     if world == 1 and not args.no_cpu_baseline:
         v, kind, cores, sample, _ = cpu_reference_sample()
         line["cpu_baseline"] = {"value": v, "unit": "pairs/s", "cores": cores, "kind": kind, "sample": sample}
@@ -587,90 +613,108 @@ def _fma_peaks(ctx):
     return p64.value, p32.value
 
 
-def debye_workload(args):
-    """Exact Debye double sum, fcc sphere a = 4.078 A cropped to 5000 atoms, Gaussian
-    displacement 0.05 A, neutron b = 7.63 fm, 1024 q in [0.1, 10).  Metric atom-pairs/s per pattern;
-    roofline: FP32 pipe at 4 flops per (pair, q) term."""
+def _ctx0():
     import torch
     import xns_b200
-    from xns_b200 import synth
     torch.cuda.set_device(0)
     ctx = xns_b200.Context(0)
     ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    return ctx
+
+
+DEBYE_GOLDEN = os.path.join(ROOT, "tests", "golden", "debye__fcc5000_neutron.npz")
+
+
+def debye_measure(ctx, steps, warmup):
+    """Exact Debye double sum (calcIntDebye), fcc sphere a = 4.078 A cropped to 5000 atoms, Gaussian
+    displacement 0.05 A, neutron b = 7.63 fm, 1024 q in [0.1, 10).  `value` = atom pairs / call time of
+    the host-buffer C-ABI call (coordinates in, I(q) out); roofline: the FP32 pipe at 4 flops per
+    (pair, q) term over the kernel-only stage time.  The error is against the reference's own
+    calcIntDebye of the same input (tests/golden, made by tests/golden/make_golden.py)."""
+    import xns_b200
+    from xns_b200 import synth
     els = synth.fcc_sphere(n=5000, a=4.078, sigma=0.05, seed=0)
     q = synth.q_mesh(0.1, 10.0, 1024)
     n = 5000
     pairs = n * (n - 1) // 2
-    ms, kms, launches, clk = _measure(ctx, lambda: ctx.calc_int_debye(els, q, xns_b200.NEUTRON, sl=[7.63]), args.steps,
-                                      args.warmup, 3)
+    ms, kms, launches, clk = _measure(ctx, lambda: ctx.calc_int_debye(els, q, xns_b200.NEUTRON, sl=[7.63]), steps,
+                                      warmup, 3)
     p64, p32 = _fma_peaks(ctx)
     achieved = 4.0 * pairs * len(q) / (kms * 1e-3) / 1e12
-    line = {"metric": "atom-pairs/s", "value": pairs / (kms * 1e-3), "unit": "pairs/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": kms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 terms, f64 reductions", "data": "synthetic (seeded)", "patterns_per_s": 1e3 / kms,
+    line = {"metric": "atom-pairs/s", "value": pairs / (ms * 1e-3), "unit": "pairs/s", "n_gpus": 1, "steps": steps,
+            "warmup": warmup, "ms_per_step": ms, "kernel_ms": kms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 terms (f64 seeds), f64 reductions", "data": "synthetic (seeded)",
+            "patterns_per_s": 1e3 / ms,
             "config": {"workload": "exact Debye, fcc sphere 5000 atoms a=4.078 A sigma=0.05 A, neutron, 1024 q in [0.1,10)",
                        "pairs_per_step": pairs, "nq": len(q), "l2": "flushed (512 MB write) before every timed step"},
             "roofline": {"kernel": "sinc_tiles_kernel<AtomPairSrc>", "bound": "fp32", "achieved": achieved, "peak": p32,
                          "unit": "TFLOP/s", "frac": achieved / p32, "traffic": None, "flops_per_term": 4,
+                         "time": "kernel-only stage (sinc kernel, +1e-8 kernel, epilogue)",
                          "peak_source": "measured in-process (FFMA loop, xns_measure_fma_peak)"},
             "e2e": {"value": pairs / (ms * 1e-3), "unit": "pairs/s", "ms_per_step": ms, "h2d_bytes_per_step": n * 24 + 8 * 1024,
                     "d2h_bytes_per_step": 8 * 1024},
             "gpu_launches": int(launches), "clocks": clk}
+    if os.path.exists(DEBYE_GOLDEN):
+        with np.load(DEBYE_GOLDEN) as g:
+            gx, Iref = g["xyz"], g["I"]
+        if np.array_equal(gx, np.concatenate(els)):
+            I = ctx.calc_int_debye(els, q, xns_b200.NEUTRON, sl=[7.63])
+            rel = np.abs(I - Iref) / np.abs(Iref)
+            line["max_rel_err_vs_reference"] = {
+                "atoms": n, "max": float(rel.max()), "q_at_max": float(q[int(rel.argmax())]),
+                "I_at_max_over_max_I": float(abs(Iref[int(rel.argmax())]) / np.abs(Iref).max()),
+                "points_above_1e-5": int((rel > 1e-5).sum()), "points": len(q),
+                "reference": "calcIntDebye of the reference on the same 5000 atoms (tests/golden/debye__fcc5000_neutron.npz)"}
+    return line
+
+
+def debye_workload(args):
+    ctx = _ctx0()
+    line = debye_measure(ctx, args.steps, args.warmup)
     if not args.no_cpu_baseline:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as orc
+        from xns_b200 import synth
         cores = os.cpu_count() or 1
         try:
             R, kind = orc.Reference(threads=cores), "reference"
         except FileNotFoundError:
             R, kind = orc.Oracle(), "port"
+        els = synth.fcc_sphere(n=5000, a=4.078, sigma=0.05, seed=0)
+        q = synth.q_mesh(0.1, 10.0, 1024)
         m = 1500
         while True:
             sub = [els[0][:m]]
             t = time.perf_counter()
-            Iref = R.int_debye(sub, q, 0, sl=[7.63])
+            R.int_debye(sub, q, 0, sl=[7.63])
             dt = time.perf_counter() - t
-            if dt > 3.0 or m >= n:
+            if dt > 3.0 or m >= 5000:
                 break
-            m = min(n, int(m * min(2.0, max(1.2, (8.0 / max(dt, 1e-3)) ** 0.5))))
-        sp = m * (m - 1) // 2
-        line["cpu_baseline"] = {"value": sp / dt, "unit": "pairs/s", "cores": cores, "kind": kind,
+            m = min(5000, int(m * min(2.0, max(1.2, (8.0 / max(dt, 1e-3)) ** 0.5))))
+        line["cpu_baseline"] = {"value": m * (m - 1) // 2 / dt, "unit": "pairs/s", "cores": cores, "kind": kind,
                                 "sample": "calcIntDebye on the first %d atoms of the sphere, 1024 q, %.2f s" % (m, dt)}
-        # accuracy of the whole pattern against the reference's FP64 sum
-        if m < n:
-            sub = els
-            Iref = R.int_debye(sub, q, 0, sl=[7.63])
-        I = ctx.calc_int_debye(sub, q, xns_b200.NEUTRON, sl=[7.63])
-        rel = np.abs(I - Iref) / np.abs(Iref)
-        line["max_rel_err_vs_reference"] = {"atoms": n, "max": float(rel.max()), "q_at_max": float(q[int(rel.argmax())]),
-                                            "I_at_max_over_max_I": float(abs(Iref[int(rel.argmax())]) / np.abs(Iref).max()),
-                                            "points_above_1e-5": int((rel > 1e-5).sum()), "points": len(q)}
     print(json.dumps(line))
     ctx.close()
     return 0
 
 
-def batch_workload(args):
-    """An ensemble of fcc spheres (a = 4.078 A), atom counts log-uniform in [1e3, 2e5], each
-    with its own Gaussian displacement sigma in [0.02, 0.1] A; 0.001 A bins, 4096 q in [0.1, 25),
-    neutron b = 7.63 fm.  Metric: patterns (I(q) of one structure) per second of the batched pass
-    (one plan, one persistent histogram launch, one exact tensor-core transform), next to the plain
-    path (one Debye_hist call per structure)."""
-    import torch
+def batch_measure(ctx, steps, warmup, count=256, errors=True):
+    """An ensemble of fcc spheres (a = 4.078 A), atom counts log-uniform in [1e3, 2e5], each with its own
+    Gaussian displacement sigma in [0.02, 0.1] A; 0.001 A bins, 4096 q in [0.1, 25), neutron b = 7.63 fm.
+    Metric: patterns (I(q) of one structure) per second of the batched pass (one plan, one persistent
+    histogram launch, one exact tensor-core transform), next to the plain path (one Debye_hist call
+    per structure)."""
     import xns_b200
     from xns_b200 import synth
-    torch.cuda.set_device(0)
-    ctx = xns_b200.Context(0)
-    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
-    structs, ns, sig = synth.sphere_ensemble(count=args.batch_count, seed=0)
+    structs, ns, sig = synth.sphere_ensemble(count=count, seed=0)
     bin = 0.001
     nh = max(synth.hist_size(s, bin) for s in structs)
     q = synth.q_mesh(0.1, 25.0, 4096)
     sl = [[7.63]] * len(structs)
     pairs = int(sum(int(n) * (int(n) - 1) // 2 for n in ns))
-    steps, warmup = args.steps, args.warmup
     chosen = lambda: ctx.calc_batch_debye_hist(structs, nh, bin, q, xns_b200.NEUTRON, sl=sl)  # noqa: E731
     ms_c, kms_c, launches_c, clk = _measure(ctx, chosen, steps, warmup, 0)
+
     def plain():  # the common bin count keeps the transform's sinc planes cached between structures
         for s in structs:
             ctx.calc_pdf_and_debye(s, nh, bin, xns_b200.DEBYE_HIST, 0, 0.0, q, xns_b200.NEUTRON, sl=[7.63])
@@ -689,7 +733,7 @@ def batch_workload(args):
     # extended-precision (x87 80-bit) sum on 128 q points that include the deepest minima -- at those
     # minima the sequential FP64 sum itself is off by up to ~1e-5 for 2e5-atom particles
     errs = {}
-    if not args.no_cpu_baseline:
+    if errors:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as orc
         O = orc.Oracle()
@@ -726,62 +770,89 @@ def batch_workload(args):
             "e2e": {"value": len(structs) / (ms_c * 1e-3), "unit": "patterns/s", "ms_per_step": ms_c,
                     "h2d_bytes_per_step": int(ns.sum()) * 24 + 8 * len(q), "d2h_bytes_per_step": 8 * len(q) * len(structs)},
             "gpu_launches": int(launches_c), "clocks": clk}
-    print(json.dumps(line))
+    return line
+
+
+def batch_workload(args):
+    ctx = _ctx0()
+    print(json.dumps(batch_measure(ctx, args.steps, args.warmup, args.batch_count, not args.no_cpu_baseline)))
     ctx.close()
     return 0
 
 
-def twod_workload(args):
+def plane_measure(ctx, steps, warmup, cells2d=63, mesh2d=1024, polar=True, errors=True):
     """2D intensity of a 1,000,188-atom fcc crystallite (a = 3.61 A, 63^3 cells, 5 % second
     species, seeded random orientation), X-ray form factors from seeded 4-Gaussian coefficients, one
     orientation, on two meshes:
       * the Cartesian q plane normal to the beam, 1024 x 1024 points over [-8, 8)^2 A^-1 (the
         configuration's mesh): xns_calc_amp_plane, a complex digit product on the tensor cores -- the
-        line's `value`;
+        line's `value` (call time of the host-buffer C-ABI call);
       * the reference's polar mesh of 1024 q in [0.05, 8) x 1024 phi with lambda = 0.01 A (nearly flat):
         xns_calc_int_2d, the drop-in path (FP64 phase, FP32 sincos) -- reported beside it.
     Metric (atom, mesh point) terms per second."""
-    import torch
     import xns_b200
     from xns_b200 import synth
-    torch.cuda.set_device(0)
-    ctx = xns_b200.Context(0)
-    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
-    els = synth.fcc_crystallite(cells=args.cells2d, a=3.61, subst=0.05, seed=0)
+    els = synth.fcc_crystallite(cells=cells2d, a=3.61, subst=0.05, seed=0)
     n = sum(len(e) for e in els)
-    nq = nfi = args.mesh2d
+    nq = nfi = mesh2d
     coef = synth.ff_coefficients(2, seed=3)
     dq = 16.0 / nq
     plane = lambda: ctx.calc_amp_plane(els, -8.0, dq, nq, -8.0, dq, nq, xns_b200.XRAY, coef=coef)  # noqa: E731
-    ms, kms, launches, clk = _measure(ctx, plane, args.steps, args.warmup, 4)
+    ms, kms, launches, clk = _measure(ctx, plane, steps, warmup, 4)
     q = synth.q_mesh(0.05, 8.0, nq)
     ff = synth.ff_on_mesh(coef, q)
-    polar = lambda: ctx.calc_int_2d(els, q, nfi, [0, 0, 0], [0, 0, 0], [1, 1, 1], 5, 0.01, xns_b200.XRAY, ff=ff)  # noqa
-    ms_p, kms_p, _, _ = _measure(ctx, polar, 1, 1, 4)
     terms = n * nq * nfi
     p64, p32 = _fma_peaks(ctx)
     peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
         os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"bf16_tflops": 1590.0}
     bf16 = float(peaks["bf16_tflops"])
-    line = {"metric": "terms/s", "value": terms / (kms * 1e-3), "unit": "(atom, q-point) terms/s", "n_gpus": 1,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": kms, "higher_is_better": True,
+    line = {"metric": "terms/s", "value": terms / (ms * 1e-3), "unit": "(atom, q-point) terms/s", "n_gpus": 1,
+            "steps": steps, "warmup": warmup, "ms_per_step": ms, "kernel_ms": kms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f64 sines, 4 integer digits per value on the bf16 tensor cores, exact sums, f64 totals",
-            "data": "synthetic (seeded)", "patterns_per_s": 1e3 / kms,
+            "data": "synthetic (seeded)", "patterns_per_s": 1e3 / ms,
             "config": {"workload": "2D Cartesian q plane %dx%d over [-8,8)^2, fcc crystallite %d atoms, X-ray" % (nq, nfi, n),
                        "atoms": n, "terms_per_step": terms},
             "roofline": {"kernel": "sinc_exact_kernel<PlaneScheme> (digit GEMM)", "bound": "tensor",
                          "achieved": 8.0 * terms / (kms * 1e-3) / 1e12, "peak": bf16, "unit": "TFLOP/s",
                          "frac": 8.0 * terms / (kms * 1e-3) / 1e12 / bf16, "traffic": None,
+                         "time": "kernel-only stage",
                          "flops_per_term": "8 (one complex multiply-add), counted once: the 10 digit products "
                                            "per term are not credited",
                          "peak_source": "MEASURED_PEAKS.json bf16_tflops (cuBLAS bf16, burst)"},
-            "polar_mesh": {"ms_per_step": kms_p, "terms_per_s": terms / (kms_p * 1e-3),
-                           "roofline_fp64_frac": 10.0 * terms / (kms_p * 1e-3) / 1e12 / p64,
-                           "path": "xns_calc_int_2d (drop-in), 1024 q x 1024 phi, lambda 0.01 A"},
             "e2e": {"value": terms / (ms * 1e-3), "unit": "(atom, q-point) terms/s", "ms_per_step": ms,
                     "h2d_bytes_per_step": n * 24, "d2h_bytes_per_step": nq * nfi * 8},
             "gpu_launches": int(launches), "clocks": clk}
+    if polar:
+        pol = lambda: ctx.calc_int_2d(els, q, nfi, [0, 0, 0], [0, 0, 0], [1, 1, 1], 5, 0.01, xns_b200.XRAY, ff=ff)  # noqa
+        ms_p, kms_p, _, _ = _measure(ctx, pol, 1, 1, 4)
+        line["polar_mesh"] = {"ms_per_step": ms_p, "terms_per_s": terms / (ms_p * 1e-3),
+                              "roofline_fp64_frac": 10.0 * terms / (kms_p * 1e-3) / 1e12 / p64,
+                              "path": "xns_calc_int_2d (drop-in), 1024 q x 1024 phi, lambda 0.01 A"}
+    if errors:
+        # sampled points of the full-size plane against the FP64 sum over all atoms (the oracle's restatement of
+        # the reference's amplitude sum at q_z = 0): 64 columns of two rows
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as orc
+        Ip = ctx.calc_amp_plane(els, -8.0, dq, nq, -8.0, dq, nq, xns_b200.XRAY, coef=coef).reshape(nq, nq)
+        O = orc.Oracle()
+        errs = []
+        for iy in (nq // 3, nq // 2 + 7):
+            cols = slice(nq // 4, nq // 4 + 64)
+            ref = O.amp_plane(els, -8.0 + (nq // 4) * dq, dq, 64, -8.0 + iy * dq, dq, 1, xns_b200.XRAY, coef=coef).ravel()
+            got = Ip[iy, cols]
+            floor = 1e-2 * float(np.median(np.abs(ref)))
+            errs.append(float(np.max(np.abs(got - ref) / np.maximum(np.abs(ref), floor))))
+        line["max_rel_err_vs_fp64"] = {"plane_sampled_points": 128, "max": max(errs),
+                                       "note": "relative, denominator floored at 1 % of the sampled median"}
+    return line, (els, q, ff, n, nfi)
+
+
+def twod_workload(args):
+    import xns_b200
+    ctx = _ctx0()
+    line, (els, q, ff, n, nfi) = plane_measure(ctx, args.steps, args.warmup, args.cells2d, args.mesh2d, True,
+                                               not args.no_cpu_baseline)
     if not args.no_cpu_baseline:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as orc
@@ -799,22 +870,28 @@ def twod_workload(args):
         line["cpu_baseline"] = {"value": n * rows * nfi_s / dt, "unit": "(atom, q-point) terms/s", "cores": cores,
                                 "kind": kind, "sample": "calcInt2D on %d q rows x %d phi, all %d atoms, %.2f s"
                                                         % (rows, nfi_s, n, dt)}
-        # sampled points of the full-size plane against the FP64 sum over all atoms (the oracle's restatement of
-        # the reference's amplitude sum at q_z = 0): 64 columns of two rows
-        Ip = ctx.calc_amp_plane(els, -8.0, dq, nq, -8.0, dq, nq, xns_b200.XRAY, coef=coef).reshape(nq, nq)
-        O = orc.Oracle()
-        errs = []
-        for iy in (nq // 3, nq // 2 + 7):
-            cols = slice(nq // 4, nq // 4 + 64)
-            ref = O.amp_plane(els, -8.0 + (nq // 4) * dq, dq, 64, -8.0 + iy * dq, dq, 1, xns_b200.XRAY, coef=coef).ravel()
-            got = Ip[iy, cols]
-            floor = 1e-2 * float(np.median(np.abs(ref)))
-            errs.append(float(np.max(np.abs(got - ref) / np.maximum(np.abs(ref), floor))))
-        line["max_rel_err_vs_fp64"] = {"plane_sampled_points": 128, "max": max(errs),
-                                       "note": "relative, denominator floored at 1 % of the sampled median"}
     print(json.dumps(line))
     ctx.close()
     return 0
+
+
+def extra_rows(args):
+    """The other configurations of the hot path, measured in the default run's process on the same GPU
+    (each with its own clock record): the exact Debye sum (5000-atom sphere), the Cartesian 2D plane
+    (1e6 atoms, 1024^2) and the batched ensemble against the plain per-structure path (256 spheres)."""
+    ctx = _ctx0()
+    out = {}
+    keep = ("metric", "value", "unit", "ms_per_step", "kernel_ms", "steps", "warmup", "config", "roofline", "e2e",
+            "clocks", "gpu_launches", "max_rel_err_vs_reference", "max_rel_err_vs_fp64", "patterns_per_s", "plain",
+            "speedup_vs_plain", "pairs_per_s", "graph_replay_ms", "autotune", "dtype")
+    d = debye_measure(ctx, 20, 5)
+    out["debye_sphere5000"] = {k: v for k, v in d.items() if k in keep}
+    p, _ = plane_measure(ctx, 5, 3, polar=False, errors=True)
+    out["plane2d_crystallite1e6"] = {k: v for k, v in p.items() if k in keep}
+    b = batch_measure(ctx, 3, 3, errors=False)
+    out["batch_spheres256"] = {k: v for k, v in b.items() if k in keep}
+    ctx.close()
+    return out
 
 
 def build_workload(args):
@@ -921,6 +998,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="histogram workload: skip the other configurations' keys (Debye, 2D plane, batch)")
     ap.add_argument("--cells", type=int, default=CELLS,
                     help="cube edge in unit cells (default 30, the benchmark; smaller only for profiler captures)")
     ap.add_argument("--workload", default="histogram", choices=["histogram", "debye", "2d", "batch", "build"],

@@ -139,12 +139,16 @@ def build_shim(ref):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--shim", action="store_true")
-    ap.add_argument("--ref", default=os.environ.get("REF", "/root/reference"))
+    ap.add_argument("--ref", default=os.environ.get("REF", ""),
+                    help="the reference source tree (default: $REF); --shim needs it")
     ap.add_argument("--ptxas-v", action="store_true")
     a = ap.parse_args()
     print(build_lib(a.ptxas_v))
     if a.shim:
-        print(build_shim(a.ref))
+        if not a.ref:
+            print("--shim: no reference source tree given (--ref or REF): shim not built")
+        else:
+            print(build_shim(a.ref))
 
 
 if __name__ == "__main__":

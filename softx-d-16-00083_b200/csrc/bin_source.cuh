@@ -14,7 +14,7 @@ struct BinSrc {
 
   __device__ uint32_t cls(unsigned long long w) const { return (uint32_t)(w / tiles_per_pair); }
 
-  __device__ int fill(unsigned long long w, PairRec *pr, void *, double dq) const {
+  __device__ int fill(unsigned long long w, PairRec *pr, void *, const SincParams &p, uint32_t cls) const {
     const uint32_t t = (uint32_t)(w / tiles_per_pair);
     const uint32_t b0 = (uint32_t)(w % tiles_per_pair) * SE_TILE;
     const unsigned long long *h = hist + (size_t)t * nhist;
@@ -23,7 +23,7 @@ struct BinSrc {
       PairRec rec = null_rec();
       if (k < nhist) {
         unsigned long long n = h[k];
-        if (n) rec = make_rec(((double)k + 0.5) * bin, (double)n, dq);
+        if (n) rec = make_rec(p, cls, ((double)k + 0.5) * bin, (double)n);
       }
       pr[e] = rec;
     }

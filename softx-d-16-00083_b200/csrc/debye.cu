@@ -33,7 +33,7 @@ struct AtomPairSrc {
   }
 
   // stage: 3 * (DB_TI + DB_TJ) doubles
-  __device__ int fill(unsigned long long w, PairRec *pr, void *stage, double dq) const {
+  __device__ int fill(unsigned long long w, PairRec *pr, void *stage, const SincParams &p, uint32_t cls) const {
     double *sxi = (double *)stage, *syi = sxi + DB_TI, *szi = syi + DB_TI;
     double *sxj = szi + DB_TI, *syj = sxj + DB_TJ, *szj = syj + DB_TJ;
     int s;
@@ -62,7 +62,7 @@ struct AtomPairSrc {
         double dx = sxi[ii] - sxj[jj], dy = syi[ii] - syj[jj], dz = szi[ii] - szj[jj];
         double r = sqrt(dx * dx + dy * dy + dz * dz);
         // coincident atoms: sin(q*0)/(q*0 + 1e-8) = 0 in the reference
-        if (r > 0) rec = make_rec(r, 1.0, dq);
+        if (r > 0) rec = make_rec(p, cls, r, 1.0);
       }
       pr[e] = rec;
     }
@@ -76,9 +76,10 @@ struct AtomPairSrc {
 // Debye on device coordinates.  out (device): [total | parts] ((1+nparts)*nq when nblocks > 1).
 // shard / nshard: only the tile pairs w with w % nshard == shard, and the self term on shard 0 only, so
 // that the outputs of shards 0..nshard-1 add up to the whole (the epilogue is affine in the sums).
+// rmax: an upper bound of the pair distances (the bounding-box diagonal), for the +1e-8 histogram.
 static int debye_device(xns_ctx *ctx, const DevCoords &dc, uint32_t nblocks, const uint32_t *n_el_block, const double *q,
-                        uint32_t nq, const double *d_w, int polar, double lambda, double *d_out, uint32_t shard = 0,
-                        uint32_t nshard = 1) {
+                        uint32_t nq, const double *d_w, int polar, double lambda, double *d_out, double rmax,
+                        uint32_t shard = 0, uint32_t nshard = 1) {
   const uint32_t nel = (uint32_t)dc.n_el.size();
   const uint32_t P = xns_npairs(nel);
   const uint32_t nparts = nblocks * (nblocks + 1) / 2;
@@ -128,9 +129,9 @@ static int debye_device(xns_ctx *ctx, const DevCoords &dc, uint32_t nblocks, con
   AtomPairSrc src{dc.x, dc.y, dc.z, d_sp, (int)sched.size()};
   int grid = 0;
   if ((st = xns_stage_begin(ctx, STAGE_DEBYE))) return st;
-  if ((st = run_sinc(ctx, p, src, sizeof(double) * 3 * (DB_TI + DB_TJ), uniform, &grid))) return st;
+  if ((st = run_sinc(ctx, p, src, sizeof(double) * 3 * (DB_TI + DB_TJ), uniform, rmax, &grid))) return st;
   if ((st = sinc_epilogue(ctx, grid, p.ncls, nel, nblocks, n_el_block, q, nq, uniform, q0, dq, d_w, dc.ntot, polar, lambda,
-                          d_out, nullptr, true, shard == 0)))
+                          d_out, nullptr, true, shard == 0, (const double *)ctx->slot_ptr[SLOT_EPS_T])))
     return st;
   return xns_stage_end(ctx, STAGE_DEBYE);
 }
@@ -156,8 +157,21 @@ static int debye_host(xns_ctx *ctx, const double *const *xyz_el, const uint32_t 
     neb_single.assign(n_el, n_el + nel);
     n_el_block = neb_single.data();
   }
+  // bounding-box diagonal: no pair is farther apart
+  double lo[3] = {HUGE_VAL, HUGE_VAL, HUGE_VAL}, hi[3] = {-HUGE_VAL, -HUGE_VAL, -HUGE_VAL};
+  for (uint32_t e = 0; e < nel; e++)
+    for (uint32_t i = 0; i < n_el[e]; i++)
+      for (int k = 0; k < 3; k++) {
+        const double v = xyz_el[e][3 * (size_t)i + k];
+        if (!(v == v) || v == HUGE_VAL || v == -HUGE_VAL)
+          return xns_fail(ctx, XNS_ERR_ARG, "Debye: non-finite coordinate");
+        lo[k] = v < lo[k] ? v : lo[k];
+        hi[k] = v > hi[k] ? v : hi[k];
+      }
+  const double rmax = sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
+                           (hi[2] - lo[2]) * (hi[2] - lo[2])) * (1 + 1e-12) + 1e-9;
   if ((st = xns_timer_start(ctx))) return st;
-  if ((st = debye_device(ctx, dc, nblocks, n_el_block, q, nq, d_w, polar, lambda, (double *)d_out, shard, nshard)))
+  if ((st = debye_device(ctx, dc, nblocks, n_el_block, q, nq, d_w, polar, lambda, (double *)d_out, rmax, shard, nshard)))
     return st;
   if ((st = xns_timer_stop(ctx))) return st;
   XNS_CUDA(ctx, cudaMemcpyAsync(I, d_out, sizeof(double) * nout, cudaMemcpyDeviceToHost, ctx->stream));

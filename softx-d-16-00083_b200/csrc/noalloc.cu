@@ -64,13 +64,17 @@ __global__ void noalloc_tables_kernel(Tables t, uint32_t *tab, double *w) {
 
 size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 
+// The +1e-8 histogram's bins at most (the array holds P * this many doubles).
+constexpr uint32_t NOALLOC_EPS_NB = 4096;
+
 template <int M, bool DIRECT>
 cudaError_t prepare(int *per_sm) {
-  const size_t smem = sizeof(double) * M * SE_THREADS + sizeof(PairRec) * SE_TILE;
   auto kern = sinc_tiles_kernel<M, DIRECT, BinSrc>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sinc_smem_bytes(M, SE_THREADS, 0));
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kern, SE_THREADS, smem);
+  // the widest layout (one FP64 column per thread): a grid sized by it fits every call
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kern, SE_THREADS, sinc_smem_bytes(M, SE_THREADS, 0));
 }
 
 // First call on a device: look up the device address of the scratch array (with that device
@@ -121,9 +125,14 @@ extern "C" int xns_int_1d_hist_noalloc(const uint64_t *hist_dev, const uint32_t 
   const uint32_t P = nel * (nel + 1) / 2;
   double q0 = 0, dq = 0;
   const bool uniform = xns_uniform_mesh(q, nq, &q0, &dq);
-  // scratch layout: weights [nel][nq] | q mesh [nq] | tables [2P + nel] | per-CTA partial sums [G][P][nq]
+  // scratch layout: weights [nel][nq] | q mesh [nq] | tables [2P + nel] | +1e-8 histogram [P][nb] |
+  // +1e-8 sums [P][nq] | per-CTA partial sums [G][P][nq]
+  uint32_t eps_nb;
+  double eps_bin;
+  eps_layout((double)nhist * bin, NOALLOC_EPS_NB, &eps_nb, &eps_bin);
   const size_t w_off = 0, q_off = align256(w_off + sizeof(double) * nel * nq);
-  const size_t t_off = align256(q_off + sizeof(double) * nq), p_off = align256(t_off + sizeof(uint32_t) * (2 * P + nel));
+  const size_t t_off = align256(q_off + sizeof(double) * nq), h_off = align256(t_off + sizeof(uint32_t) * (2 * P + nel));
+  const size_t e_off = align256(h_off + sizeof(double) * P * eps_nb), p_off = align256(e_off + sizeof(double) * P * nq);
   const size_t per_cta = sizeof(double) * P * nq;
   if (p_off + per_cta > NOALLOC_BYTES) return XNS_ERR_LIMIT;
   const int per_sm = uniform ? ds.per_sm_uniform : ds.per_sm_direct;
@@ -133,6 +142,7 @@ extern "C" int xns_int_1d_hist_noalloc(const uint64_t *hist_dev, const uint32_t 
   grid = std::min<unsigned long long>(grid, (NOALLOC_BYTES - p_off) / per_cta);
   if (grid == 0) grid = 1;
   double *w = (double *)(ds.scratch + w_off), *dqm = (double *)(ds.scratch + q_off), *partial = (double *)(ds.scratch + p_off);
+  double *eps_hist = (double *)(ds.scratch + h_off), *eps_t = (double *)(ds.scratch + e_off);
   uint32_t *tab = (uint32_t *)(ds.scratch + t_off);
 
   Tables t;
@@ -150,7 +160,9 @@ extern "C" int xns_int_1d_hist_noalloc(const uint64_t *hist_dev, const uint32_t 
     t.sl[e] = source == XNS_NEUTRON ? sl[e] : 0.0;
   }
   t.fill_weights = source == XNS_NEUTRON;
-  // what must start at zero: the partial sums (the array keeps the previous call's contents)
+  // what must start at zero: the +1e-8 histogram and sums, the partial sums (the array keeps the
+  // previous call's contents; cudaMemsetAsync allocates nothing)
+  if (cudaMemsetAsync(eps_hist, 0, e_off - h_off + sizeof(double) * P * nq, s) != cudaSuccess) return XNS_ERR_CUDA;
   if (cudaMemsetAsync(partial, 0, per_cta * grid, s) != cudaSuccess) return XNS_ERR_CUDA;
   noalloc_tables_kernel<<<std::max(1u, std::min(64u, (nel * nq + 255) / 256)), 256, 0, s>>>(t, tab, w);
   if (cudaGetLastError() != cudaSuccess) return XNS_ERR_CUDA;
@@ -169,6 +181,9 @@ extern "C" int xns_int_1d_hist_noalloc(const uint64_t *hist_dev, const uint32_t 
   p.ncls = P;
   p.ntiles = ntiles;
   p.partial = partial;
+  p.eps_hist = eps_hist;
+  p.eps_nb = eps_nb;
+  p.eps_inv_bw = 1.0 / eps_bin;
   BinSrc src{(const unsigned long long *)hist_dev, nhist, tpp, bin};
   const int M = uniform ? SE_M_UNIFORM : SE_M_DIRECT;
   const uint32_t chunks = (nq + M - 1) / M;
@@ -176,15 +191,18 @@ extern "C" int xns_int_1d_hist_noalloc(const uint64_t *hist_dev, const uint32_t 
   while (lanes < (int)chunks) lanes <<= 1;
   if (lanes > SE_THREADS) return XNS_ERR_LIMIT;
   if (uniform) {
-    const size_t smem = sizeof(double) * SE_M_UNIFORM * SE_THREADS + sizeof(PairRec) * SE_TILE;
+    const size_t smem = sinc_smem_bytes(SE_M_UNIFORM, lanes, 0);
     sinc_tiles_kernel<SE_M_UNIFORM, false, BinSrc><<<(unsigned)grid, SE_THREADS, smem, s>>>(p, src, lanes);
   } else {
-    const size_t smem = sizeof(double) * SE_M_DIRECT * SE_THREADS + sizeof(PairRec) * SE_TILE;
+    const size_t smem = sinc_smem_bytes(SE_M_DIRECT, lanes, 0);
     sinc_tiles_kernel<SE_M_DIRECT, true, BinSrc><<<(unsigned)grid, SE_THREADS, smem, s>>>(p, src, lanes);
   }
   if (cudaGetLastError() != cudaSuccess) return XNS_ERR_CUDA;
+  dim3 eg((nq + 127) / 128, (eps_nb + EPS_RUN - 1) / EPS_RUN, P);
+  sinc_eps_kernel<<<eg, 128, 0, s>>>(eps_hist, eps_nb, eps_bin, q0, dq, uniform ? nullptr : dqm, nq, eps_t);
+  if (cudaGetLastError() != cudaSuccess) return XNS_ERR_CUDA;
   sinc_epilogue_kernel<<<(nq + 127) / 128, 128, 0, s>>>(partial, (int)grid, P, nel, 1, 1, tab, tab + P, w, tab + 2 * P, q0, dq,
-                                                        uniform ? nullptr : dqm, nq, ntot, polar, lambda, 1, 1, I_dev);
+                                                        uniform ? nullptr : dqm, nq, ntot, polar, lambda, 1, 1, eps_t, I_dev);
   if (cudaGetLastError() != cudaSuccess) return XNS_ERR_CUDA;
   return XNS_OK;
 }

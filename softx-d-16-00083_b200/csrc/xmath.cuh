@@ -43,6 +43,37 @@ __device__ __forceinline__ void xns_sincos(double x, float *s, float *c) {
   sincos_quadrant((float)y, n, s, c);
 }
 
+// sin and cos of x (radians) in FP64: the same quadrant reduction, then the Taylor series in FP64,
+//   sin y = y - y^3/3! + ... - y^11/11!   (truncation < 1e-11 on |y| <= pi/4)
+//   cos y = 1 - y^2/2! + ... - y^10/10!   (truncation < 2e-10)
+// for seeds that must round to FP32 correctly: the FP32 series above leaves one or two FP32 ulps,
+// which at the deep minima of a Debye pattern (a sum that cancels to 1e-5 of its terms) is visible.
+// Runs on the FP64 pipe, beside the FP32 work of the sinc engine.  Valid for |x| < 2^50.
+__device__ __forceinline__ void xns_sincos64(double x, double *s, double *c) {
+  const double MAGIC = 6755399441055744.0;
+  const double TWO_OVER_PI = 0.63661977236758134308;
+  const double PIO2_HI = 1.5707963267948966192;
+  const double PIO2_LO = 6.123233995736766036e-17;
+  const double t = __fma_rn(x, TWO_OVER_PI, MAGIC);
+  const int n = __double2loint(t);
+  const double nd = t - MAGIC;
+  const double y = __fma_rn(-nd, PIO2_LO, __fma_rn(-nd, PIO2_HI, x));
+  const double y2 = y * y;
+  double sp = __fma_rn(y2, -1.0 / 39916800.0, 1.0 / 362880.0);  // -1/11!, 1/9!
+  sp = __fma_rn(y2, sp, -1.0 / 5040.0);                          // -1/7!
+  sp = __fma_rn(y2, sp, 1.0 / 120.0);                            // 1/5!
+  sp = __fma_rn(y2, sp, -1.0 / 6.0);                             // -1/3!
+  sp = __fma_rn(y2 * y, sp, y);
+  double cp = __fma_rn(y2, -1.0 / 3628800.0, 1.0 / 40320.0);    // -1/10!, 1/8!
+  cp = __fma_rn(y2, cp, -1.0 / 720.0);                           // -1/6!
+  cp = __fma_rn(y2, cp, 1.0 / 24.0);                             // 1/4!
+  cp = __fma_rn(y2, cp, -0.5);                                   // -1/2!
+  cp = __fma_rn(y2, cp, 1.0);
+  const double a = (n & 1) ? cp : sp, b = (n & 1) ? sp : cp;
+  *s = (n & 2) ? -a : a;
+  *c = ((n + 1) & 2) ? -b : b;
+}
+
 __device__ __forceinline__ float xns_sin(double x) {
   float s, c;
   xns_sincos(x, &s, &c);

@@ -38,6 +38,8 @@ enum ScratchSlot {
   SLOT_BATCH,           // batched ensemble: coordinates, schedules and per-structure tables
   SLOT_BATCH_HIST,      // batched ensemble: histograms
   SLOT_ATOMS,           // structure builder: the last build's atoms (x y z doubles, element-major)
+  SLOT_EPS_HIST,        // sinc engine: the +1e-8 distance histogram
+  SLOT_EPS_T,           // sinc engine: the +1e-8 sums per class and q
   SLOT_COUNT
 };
 

@@ -1,8 +1,9 @@
 """Python binding of the xns_b200 C ABI (include/xns_b200.h) over ctypes.
 
-The library is the in-tree build softx-d-16-00083_b200/lib/libxns_b200.so; importing this package
-fails loudly if it is missing, and every call raises XnsError on a non-zero status.  There is no CPU
-code path here: each function calls the CUDA library.
+The library is the in-tree build softx-d-16-00083_b200/lib/libxns_b200.so, loaded at the first call
+into it (importing the package alone maps nothing); a missing build raises ImportError there, and every
+call raises XnsError on a non-zero status.  There is no CPU code path here: each function calls the
+CUDA library.
 
 Arrays follow the reference's layout (see the header): coordinates per element as (n_e, 3) float64
 arrays, element pairs a <= b in loop order, histograms element-pair major.
@@ -32,72 +33,91 @@ def _load():
     return C.CDLL(LIB_PATH)
 
 
-lib = _load()
 _p = C.c_void_p
 _u32 = C.c_uint32
 _dbl = C.c_double
 _int = C.c_int
 _PP = C.POINTER(C.c_void_p)
 
-lib.xns_create.argtypes = [_int, C.POINTER(_p)]
-lib.xns_destroy.argtypes = [_p]
-lib.xns_destroy.restype = None
-lib.xns_last_error.argtypes = [_p]
-lib.xns_last_error.restype = C.c_char_p
-lib.xns_status_string.argtypes = [_int]
-lib.xns_status_string.restype = C.c_char_p
-lib.xns_set_stream.argtypes = [_p, _p]
-lib.xns_last_kernel_ms.argtypes = [_p]
-lib.xns_last_kernel_ms.restype = _dbl
-lib.xns_kernel_launches.argtypes = [_p]
-lib.xns_kernel_launches.restype = C.c_uint64
-lib.xns_calc_hist.argtypes = [_p, _PP, _p, _u32, _u32, _dbl, _p]
-lib.xns_calc_int_1d_hist.argtypes = [_p, _p, _p, _u32, _u32, _dbl, _p, _u32, _int, _PP, _p, _int, _dbl, _p]
-lib.xns_calc_pdf.argtypes = [_p, _p, _p, _u32, _u32, _dbl, _int, _dbl, _p, _p]
-lib.xns_calc_pdf_and_debye.argtypes = [_p, _PP, _p, _u32, _u32, _dbl, _int, _int, _dbl, _p, _u32, _int, _PP, _p, _int,
-                                       _dbl, _p, _p, _p]
-lib.xns_calc_int_debye.argtypes = [_p, _PP, _p, _u32, _p, _u32, _int, _PP, _p, _int, _dbl, _p]
-lib.xns_calc_int_partial_debye.argtypes = [_p, _PP, _p, _u32, _u32, _p, _p, _u32, _int, _PP, _p, _int, _dbl, _p]
-lib.xns_calc_int_2d.argtypes = [_p, _PP, _p, _u32, _p, _u32, _u32, _p, _p, _p, _u32, _dbl, _int, _PP, _p, _int, _p, _p]
-lib.xns_hist_transform_bf16x3.argtypes = [_p, _p, _u32, _u32, _dbl, _p, _u32, _p]
-lib.xns_hist_transform_exact.argtypes = [_p, _p, _u32, _u32, _dbl, _p, _u32, _p]
-_BATCH_IN = [_u32, _p, _p, _p, _u32, _dbl, _p, _u32, _int, _PP, _p, _int, _dbl]
-lib.xns_calc_batch_debye_hist.argtypes = [_p] + _BATCH_IN + [_p, _p]
-lib.xns_batch_create.argtypes = [_p] + _BATCH_IN + [_int, C.POINTER(_p)]
-lib.xns_batch_run.argtypes = [_p, _p, _p]
-lib.xns_batch_last_ms.argtypes = [_p]
-lib.xns_batch_last_ms.restype = _dbl
-lib.xns_batch_last_error.argtypes = [_p]
-lib.xns_batch_last_error.restype = C.c_char_p
-lib.xns_batch_tuning.argtypes = [_p, C.POINTER(_u32), C.POINTER(_u32)]
-lib.xns_batch_tuning.restype = _dbl
-lib.xns_batch_destroy.argtypes = [_p]
-lib.xns_batch_destroy.restype = None
-lib.xns_mlp_create.argtypes = [_p, _p, C.c_uint64, C.POINTER(_p)]
-lib.xns_mlp_destroy.argtypes = [_p]
-lib.xns_mlp_destroy.restype = None
-lib.xns_mlp_last_error.argtypes = [_p]
-lib.xns_mlp_last_error.restype = C.c_char_p
-lib.xns_mlp_param_count.argtypes = [_p]
-lib.xns_mlp_param_count.restype = C.c_long
-lib.xns_mlp_get_params.argtypes = [_p, _p]
-lib.xns_mlp_set_params.argtypes = [_p, _p]
-lib.xns_mlp_forward.argtypes = [_p, _p, _int, _p]
-lib.xns_mlp_gradients.argtypes = [_p, _p, _p, _p, _int, _p, C.POINTER(_dbl)]
-lib.xns_mlp_train.argtypes = [_p, _p, _p, _p, _int, _int, _int, C.c_float, C.POINTER(_dbl)]
-lib.xns_calc_amp_plane.argtypes = [_p, _PP, _p, _u32, _dbl, _dbl, _u32, _dbl, _dbl, _u32, _int, _p, _p, _p]
-lib.xns_binning_features.argtypes = [_p, _p, _u32, _p]
-lib.xns_binning_correction.argtypes = [_p, _p, _p, _u32, _dbl, _p, _u32, _dbl, _p]
-lib.xns_build_atoms.argtypes = [_p, _p, _u32, _u32, C.c_uint64, _p, _p, C.POINTER(_p)]
-lib.xns_copy_atoms.argtypes = [_p, _PP]
-lib.xns_rearrangement_int.argtypes = [_p, _p, _p, _u32, _p, _u32, _u32, _int, _PP, _p, _int, _int, _dbl, _u32]
-lib.xns_calc_hist_passes.argtypes = [_p, _PP, _p, _u32, _u32, _dbl, C.c_uint64, _p]
-lib.xns_write_i.argtypes = [C.c_char_p, _p, _p, _u32]
-lib.xns_write_i2.argtypes = [C.c_char_p, _p, _u32, _u32]
-lib.xns_write_pdf.argtypes = [C.c_char_p, _p, _u32, _dbl, _int]
-lib.xns_write_atoms.argtypes = [C.c_char_p, _p, _p, _u32, _PP]
-lib.xns_pdf_and_debye_device.argtypes = [_p, _p, _p, _u32, _u32, _dbl, _int, _int, _dbl, _p, _u32, _int, _PP, _p, _int,
-                                         _dbl, _p, _p, _p]
+
+def _declare(lib):
+    """The C prototypes of the entry points (include/xns_b200.h)."""
+    lib.xns_create.argtypes = [_int, C.POINTER(_p)]
+    lib.xns_destroy.argtypes = [_p]
+    lib.xns_destroy.restype = None
+    lib.xns_last_error.argtypes = [_p]
+    lib.xns_last_error.restype = C.c_char_p
+    lib.xns_status_string.argtypes = [_int]
+    lib.xns_status_string.restype = C.c_char_p
+    lib.xns_set_stream.argtypes = [_p, _p]
+    lib.xns_last_kernel_ms.argtypes = [_p]
+    lib.xns_last_kernel_ms.restype = _dbl
+    lib.xns_kernel_launches.argtypes = [_p]
+    lib.xns_kernel_launches.restype = C.c_uint64
+    lib.xns_calc_hist.argtypes = [_p, _PP, _p, _u32, _u32, _dbl, _p]
+    lib.xns_calc_int_1d_hist.argtypes = [_p, _p, _p, _u32, _u32, _dbl, _p, _u32, _int, _PP, _p, _int, _dbl, _p]
+    lib.xns_calc_pdf.argtypes = [_p, _p, _p, _u32, _u32, _dbl, _int, _dbl, _p, _p]
+    lib.xns_calc_pdf_and_debye.argtypes = [_p, _PP, _p, _u32, _u32, _dbl, _int, _int, _dbl, _p, _u32, _int, _PP, _p, _int,
+                                           _dbl, _p, _p, _p]
+    lib.xns_calc_int_debye.argtypes = [_p, _PP, _p, _u32, _p, _u32, _int, _PP, _p, _int, _dbl, _p]
+    lib.xns_calc_int_partial_debye.argtypes = [_p, _PP, _p, _u32, _u32, _p, _p, _u32, _int, _PP, _p, _int, _dbl, _p]
+    lib.xns_calc_int_2d.argtypes = [_p, _PP, _p, _u32, _p, _u32, _u32, _p, _p, _p, _u32, _dbl, _int, _PP, _p, _int, _p, _p]
+    lib.xns_hist_transform_bf16x3.argtypes = [_p, _p, _u32, _u32, _dbl, _p, _u32, _p]
+    lib.xns_hist_transform_exact.argtypes = [_p, _p, _u32, _u32, _dbl, _p, _u32, _p]
+    _BATCH_IN = [_u32, _p, _p, _p, _u32, _dbl, _p, _u32, _int, _PP, _p, _int, _dbl]
+    lib.xns_calc_batch_debye_hist.argtypes = [_p] + _BATCH_IN + [_p, _p]
+    lib.xns_batch_create.argtypes = [_p] + _BATCH_IN + [_int, C.POINTER(_p)]
+    lib.xns_batch_run.argtypes = [_p, _p, _p]
+    lib.xns_batch_last_ms.argtypes = [_p]
+    lib.xns_batch_last_ms.restype = _dbl
+    lib.xns_batch_last_error.argtypes = [_p]
+    lib.xns_batch_last_error.restype = C.c_char_p
+    lib.xns_batch_tuning.argtypes = [_p, C.POINTER(_u32), C.POINTER(_u32)]
+    lib.xns_batch_tuning.restype = _dbl
+    lib.xns_batch_destroy.argtypes = [_p]
+    lib.xns_batch_destroy.restype = None
+    lib.xns_mlp_create.argtypes = [_p, _p, C.c_uint64, C.POINTER(_p)]
+    lib.xns_mlp_destroy.argtypes = [_p]
+    lib.xns_mlp_destroy.restype = None
+    lib.xns_mlp_last_error.argtypes = [_p]
+    lib.xns_mlp_last_error.restype = C.c_char_p
+    lib.xns_mlp_param_count.argtypes = [_p]
+    lib.xns_mlp_param_count.restype = C.c_long
+    lib.xns_mlp_get_params.argtypes = [_p, _p]
+    lib.xns_mlp_set_params.argtypes = [_p, _p]
+    lib.xns_mlp_forward.argtypes = [_p, _p, _int, _p]
+    lib.xns_mlp_gradients.argtypes = [_p, _p, _p, _p, _int, _p, C.POINTER(_dbl)]
+    lib.xns_mlp_train.argtypes = [_p, _p, _p, _p, _int, _int, _int, C.c_float, C.POINTER(_dbl)]
+    lib.xns_calc_amp_plane.argtypes = [_p, _PP, _p, _u32, _dbl, _dbl, _u32, _dbl, _dbl, _u32, _int, _p, _p, _p]
+    lib.xns_binning_features.argtypes = [_p, _p, _u32, _p]
+    lib.xns_binning_correction.argtypes = [_p, _p, _p, _u32, _dbl, _p, _u32, _dbl, _p]
+    lib.xns_build_atoms.argtypes = [_p, _p, _u32, _u32, C.c_uint64, _p, _p, C.POINTER(_p)]
+    lib.xns_copy_atoms.argtypes = [_p, _PP]
+    lib.xns_rearrangement_int.argtypes = [_p, _p, _p, _u32, _p, _u32, _u32, _int, _PP, _p, _int, _int, _dbl, _u32]
+    lib.xns_calc_hist_passes.argtypes = [_p, _PP, _p, _u32, _u32, _dbl, C.c_uint64, _p]
+    lib.xns_write_i.argtypes = [C.c_char_p, _p, _p, _u32]
+    lib.xns_write_i2.argtypes = [C.c_char_p, _p, _u32, _u32]
+    lib.xns_write_pdf.argtypes = [C.c_char_p, _p, _u32, _dbl, _int]
+    lib.xns_write_atoms.argtypes = [C.c_char_p, _p, _p, _u32, _PP]
+    lib.xns_pdf_and_debye_device.argtypes = [_p, _p, _p, _u32, _u32, _dbl, _int, _int, _dbl, _p, _u32, _int, _PP, _p, _int,
+                                             _dbl, _p, _p, _p]
+
+
+class _Lib:
+    """The CUDA library, loaded and its prototypes declared at the first call through it, so that
+    importing the package (for its structure generators, say) maps no shared library; a missing build
+    raises ImportError at that first call."""
+    _cdll = None
+
+    def __getattr__(self, name):
+        if _Lib._cdll is None:
+            cdll = _load()
+            _declare(cdll)
+            _Lib._cdll = cdll
+        return getattr(_Lib._cdll, name)
+
+
+lib = _Lib()
 
 
 def _ptr(a):

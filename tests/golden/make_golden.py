@@ -2,7 +2,10 @@
 (CalcFunctions.cpp compiled from the reference sources by oracle/Makefile into
 oracle/_ref/libxnsref.so) on small seeded synthetic structures.
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle REF=<reference source tree> && python tests/golden/make_golden.py [case-prefix ...]
+
+With prefixes, only the cases whose names start with one of them are regenerated (the full-size
+cases take about a minute of the reference's CPU code each).
 
 The reference ships no unit tests and no histogram or PDF outputs (its two example patterns need
 inputs that cannot be rebuilt here), so these fixtures are the pinned known answers: the CPU test
@@ -27,9 +30,42 @@ def pack(elements):
     return np.concatenate([np.asarray(e).reshape(-1, 3) for e in elements]), np.array([len(e) for e in elements], np.uint32)
 
 
-def main():
-    R = Reference(threads=4)
+def sha256_u64(a):
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(a, dtype="<u8").tobytes()).hexdigest()
+
+
+def sha256_f64(a):
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(a, dtype="<f8").tobytes()).hexdigest()
+
+
+def full_size_cases(R, out):
+    """The two full-size workloads: the Debye double sum on the 5000-atom fcc sphere (1024 q in
+    [0.1, 10), neutron b = 7.63 fm) with its pattern, and the 1.94e5-atom rock-salt cube's histogram at
+    0.001 A (30^3 cells, seed 0) as a SHA-256 of its u64 counts (plus its size and total, and the
+    hash of the coordinates it was made from, so that a change of the generator shows as such)."""
+    sphere = synth.fcc_sphere(n=5000, a=4.078, sigma=0.05, seed=0)
+    q = synth.q_mesh(0.1, 10.0, 1024)
+    xyz, n = pack(sphere)
+    out["debye/fcc5000_neutron"] = dict(xyz=xyz, n_el=n, q=q, source=0, sl=np.array([7.63]), polar=0, lam=0.0,
+                                        I=R.int_debye(sphere, q, 0, sl=[7.63]))
+    cube = synth.rocksalt_cube(cells=30, a=5.64, vacancy=0.1, sigma=0.07, seed=0)
+    nh = R.hist_size(cube, 0.001)
+    h = R.hist(cube, nh, 0.001)
+    xyz, n = pack(cube)
+    out["histhash/rocksalt30_seed0_b0.001"] = dict(n_el=n, bin=0.001, nhist=nh, total=int(h.sum()),
+                                                   sha256=sha256_u64(h), xyz_sha256=sha256_f64(xyz))
+
+
+def main(prefixes=()):
+    R = Reference(threads=os.cpu_count() or 4)
     out = {}
+    if prefixes:
+        full_size_cases(R, out)
+        out = {k: v for k, v in out.items() if k.startswith(tuple(prefixes))}
+        save(out)
+        return
 
     # 1. histograms: two species rock salt at the reference bin 0.001 and a coarse bin; one-element
     #    fcc sphere; three elements with an empty one and coincident atoms
@@ -97,6 +133,11 @@ def main():
     eul = np.array([0.3, 1.1, -0.7])
     out["rot/all"] = dict(euler=eul, m=np.stack([R.rot_matrix(eul, c) for c in range(12)]))
 
+    full_size_cases(R, out)
+    save(out)
+
+
+def save(out):
     for key, d in out.items():
         path = os.path.join(HERE, key.replace("/", "__") + ".npz")
         np.savez_compressed(path, **{k: np.asarray(v) for k, v in d.items()})
@@ -104,4 +145,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -77,12 +77,21 @@ def test_hist_out_of_range_is_an_error(gpu_ctx):
 
 
 def test_hist_checksum_full_size(gpu_ctx):
-    """Full configuration (rock-salt cube, 30^3 cells, ~1.94e5 atoms): size-independent checks --
-    the total count equals the number of pairs of each element pair, and the histogram of a
-    permuted, shuffled copy is identical."""
+    """Full configuration (rock-salt cube, 30^3 cells, ~1.94e5 atoms, 0.001 A): the counts are the
+    reference's calcHist's bit for bit (SHA-256 of the u64 counts against the hash the reference's own
+    code produced, tests/golden/make_golden.py); and size-independent checks -- the total count
+    equals the number of pairs of each element pair, and the histogram of a permuted, shuffled copy
+    is identical."""
+    import hashlib
+    g = load_golden("histhash__rocksalt30_seed0_b0.001")
     els = synth.rocksalt_cube(cells=30, seed=0)
+    xyz = np.ascontiguousarray(np.concatenate(els), dtype="<f8")
+    assert hashlib.sha256(xyz.tobytes()).hexdigest() == str(g["xyz_sha256"]), "the cube generator changed"
     nh = synth.hist_size(els, 0.001)
+    assert nh == int(g["nhist"])
     h = gpu_ctx.calc_hist(els, nh, 0.001).reshape(3, nh)
+    assert hashlib.sha256(np.ascontiguousarray(h, dtype="<u8").tobytes()).hexdigest() == str(g["sha256"])
+    assert int(h.sum()) == int(g["total"])
     n0, n1 = len(els[0]), len(els[1])
     assert [int(x) for x in h.sum(axis=1)] == [n0 * (n0 - 1) // 2, n0 * n1, n1 * (n1 - 1) // 2]
     rng = np.random.default_rng(9)

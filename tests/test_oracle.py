@@ -28,9 +28,11 @@ def test_hist_bitexact(oracle, name):
 def test_debye(oracle, name):
     g = load_golden(name)
     els = split_elements(g["xyz"], g["n_el"])
-    I = oracle.int_debye(els, g["q"], int(g["source"]), ff=g.get("ff"), sl=g.get("sl"), polar=bool(g["polar"]),
-                         lam=float(g["lam"]))
-    assert rel_err(I, g["I"]) < 1e-12
+    # the full-size pattern (5000 atoms x 1024 q) on every 64th q, so that the CPU suite stays short
+    sub = slice(None, None, 64 if len(g["q"]) > 256 else 1)
+    I = oracle.int_debye(els, g["q"][sub], int(g["source"]), ff=None if g.get("ff") is None else g["ff"][:, sub],
+                         sl=g.get("sl"), polar=bool(g["polar"]), lam=float(g["lam"]))
+    assert rel_err(I, g["I"][sub]) < 1e-12
 
 
 def test_partial_debye(oracle):
