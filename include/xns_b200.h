@@ -56,6 +56,19 @@ const char *xns_last_error(const xns_ctx *ctx);
 const char *xns_status_string(int status);
 /* Run on the caller's stream (a cudaStream_t) instead of the library's own; NULL restores it. */
 int xns_set_stream(xns_ctx *ctx, void *stream);
+/* Caps the device scratch the calc functions keep in the context between calls (their grow-only
+ * buffers) at bytes; 0 removes the cap.  A call that would need more returns XNS_ERR_NOMEM before
+ * queueing any work, and the context stays usable.  If the context already holds more than the new
+ * cap, that scratch is released first (the context's stream is synchronised).  For a service with a
+ * fixed device-memory budget per context; no counterpart in the reference. */
+int xns_set_memory_limit(xns_ctx *ctx, uint64_t bytes);
+/* Failure-path test of the tensor-core pipelines: the next tensor-core transform on this context
+ * (the exact histogram -> I(q) transform or the 2D plane) runs with its copy warp issuing no copies
+ * and every pipeline wait bounded by wait_limit_ns (at most 2 s, the kernels' own bound).  Its waits
+ * run out, the kernel releases its tensor memory and returns, and that call fails with XNS_ERR_CUDA
+ * ("a pipeline wait ran out of time"); the context stays usable and the following calls run
+ * normally.  Affects one call.  No counterpart in the reference. */
+int xns_inject_pipeline_stall(xns_ctx *ctx, uint64_t wait_limit_ns);
 /* Device time of the most recent call's kernels, in milliseconds (CUDA events). */
 double xns_last_kernel_ms(const xns_ctx *ctx);
 /* Number of kernels the library launched since the context was created. */
@@ -174,18 +187,27 @@ int xns_pdf_and_debye_from_hist_device(xns_ctx *ctx, const uint64_t *hist_dev, c
 /* Histogram -> I(q) that allocates no device memory.  No counterpart in the reference: it serves
  * callers that cannot call cudaMalloc -- a plugin whose host framework owns all device memory and
  * hands it buffers, or a service whose memory budget is fixed at start-up.  The caller passes the
- * histogram (hist_dev: P*nhist u64) and the output (I_dev: nq doubles) as device buffers it owns; the
- * result equals xns_calc_int_1d_hist's.  Intermediates live in one file-scope device array of
- * XNS_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until exit.  Limits: at most
- * XNS_NOALLOC_MAX_ELEMENTS elements, XNS_NOALLOC_MAX_Q q points, and (P + nel + 1) * nq * 8 bytes plus
- * one CTA's P * nq * 8 bytes of partial sums within the array; larger sizes return XNS_ERR_LIMIT.
- * Runs on the current device and the given stream (NULL = default stream) and returns without
- * waiting for the GPU.  The first call on a device looks up the array's device address: make it before
- * any stream capture.  Calls share the array: calls that overlap on the GPU (other streams, other host
- * threads) race on it. */
+ * histogram (hist_dev: P*nhist u64) and the output (I_dev: nq doubles) as device buffers it owns.
+ * Intermediates live in one file-scope device array of XNS_NOALLOC_SCRATCH_BYTES that every GPU
+ * loading the library holds until exit.
+ * Accuracy: the result is xns_calc_int_1d_hist's quantity computed another way -- an FP32 sine
+ * recurrence over the bins with FP64 seeds and FP64 sums (the engine of the exact Debye sum) instead
+ * of the integer-digit tensor-core sums -- and agrees with it within 1e-5 relative at every q, the deep
+ * low-q minima of I(q) included (the GPU tests check a 10-cell rock-salt cube at 0.001 A on 4096 q).
+ * Limits: at most XNS_NOALLOC_MAX_ELEMENTS elements; at most XNS_NOALLOC_MAX_Q q points on a uniform
+ * mesh and XNS_NOALLOC_MAX_Q_NONUNIFORM on any other; and the array must hold, each region rounded up
+ * to 256 bytes, the weights and the q mesh ((nel + 1) * nq * 8 bytes), the pair tables ((2P + nel) * 4),
+ * the +1e-8 histogram (P * nb * 8, nb = min(4096, nhist * bin / 0.05 + 2)), its sums (P * nq * 8) and
+ * at least one CTA's partial sums (P * nq * 8).  Larger sizes return XNS_ERR_LIMIT before any work is
+ * queued.  Runs on the current device and the given stream (NULL = default stream); X-ray form factors
+ * and a non-uniform q mesh are copied from the caller's host arrays with cudaMemcpyAsync, which waits
+ * for the copy when that host memory is pageable.  The first call on a device looks up the array's
+ * device address: make it before any stream capture.  Calls share the array: calls that overlap on the
+ * GPU (other streams, other host threads) race on it. */
 #define XNS_NOALLOC_SCRATCH_BYTES (16u << 20)
 #define XNS_NOALLOC_MAX_ELEMENTS 16
 #define XNS_NOALLOC_MAX_Q 8192
+#define XNS_NOALLOC_MAX_Q_NONUNIFORM 2048
 int xns_int_1d_hist_noalloc(const uint64_t *hist_dev, const uint32_t *n_el, uint32_t nel, uint32_t nhist, double bin,
                             const double *q, uint32_t nq, int source, const double *const *ff, const double *sl, int polar,
                             double lambda, double *I_dev, void *stream);

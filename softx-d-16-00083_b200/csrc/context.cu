@@ -21,13 +21,25 @@ int xns_cuda_fail(xns_ctx *ctx, cudaError_t e, const char *what) {
 int xns_scratch(xns_ctx *ctx, ScratchSlot slot, size_t bytes, void **out) {
   if (bytes == 0) bytes = 16;
   if (ctx->slot_size[slot] < bytes) {
+    size_t sz = bytes + bytes / 8;  // headroom so slowly growing calls do not reallocate each time
+    if (ctx->mem_limit) {
+      size_t others = 0;
+      for (int s = 0; s < SLOT_COUNT; s++)
+        if (s != slot) others += ctx->slot_size[s];
+      if (others + bytes > ctx->mem_limit) {
+        char buf[160];
+        snprintf(buf, sizeof(buf), "device scratch of %zu bytes would exceed the context's memory limit of %zu bytes",
+                 others + bytes, ctx->mem_limit);
+        return xns_fail(ctx, XNS_ERR_NOMEM, buf);
+      }
+      sz = std::min(sz, ctx->mem_limit - others);
+    }
     if (ctx->slot_ptr[slot]) {
       cudaError_t e = cudaFreeAsync(ctx->slot_ptr[slot], ctx->stream);
       if (e != cudaSuccess) return xns_cuda_fail(ctx, e, "cudaFreeAsync");
       ctx->slot_ptr[slot] = nullptr;
       ctx->slot_size[slot] = 0;
     }
-    size_t sz = bytes + bytes / 8;  // headroom so slowly growing calls do not reallocate each time
     cudaError_t e = cudaMallocAsync(&ctx->slot_ptr[slot], sz, ctx->stream);
     if (e != cudaSuccess) return xns_cuda_fail(ctx, e, "cudaMallocAsync");
     ctx->slot_size[slot] = sz;
@@ -232,6 +244,37 @@ const char *xns_last_error(const xns_ctx *ctx) { return ctx ? ctx->err.c_str() :
 int xns_set_stream(xns_ctx *ctx, void *stream) {
   if (!ctx) return XNS_ERR_ARG;
   ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+  return XNS_OK;
+}
+
+int xns_set_memory_limit(xns_ctx *ctx, uint64_t bytes) {
+  if (!ctx) return XNS_ERR_ARG;
+  size_t held = 0;
+  for (int s = 0; s < SLOT_COUNT; s++) held += ctx->slot_size[s];
+  if (bytes && held > bytes) {  // start again under the new cap
+    for (int s = 0; s < SLOT_COUNT; s++)
+      if (ctx->slot_ptr[s]) {
+        XNS_CUDA(ctx, cudaFreeAsync(ctx->slot_ptr[s], ctx->stream));
+        ctx->slot_ptr[s] = nullptr;
+        ctx->slot_size[s] = 0;
+      }
+    XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    // cached tables that lived in the released slots
+    ctx->tc_q.clear();
+    ctx->x_q.clear();
+    ctx->tc_bin = ctx->x_bin = 0;
+    ctx->tc_kt = ctx->x_kt = 0;
+    ctx->atoms_n.clear();
+  }
+  ctx->mem_limit = (size_t)bytes;
+  return XNS_OK;
+}
+
+int xns_inject_pipeline_stall(xns_ctx *ctx, uint64_t wait_limit_ns) {
+  if (!ctx) return XNS_ERR_ARG;
+  if (wait_limit_ns == 0 || wait_limit_ns > 2000000000ull)
+    return xns_fail(ctx, XNS_ERR_ARG, "inject_pipeline_stall: the wait limit must be in (0, 2 s]");
+  ctx->inject_stall_ns = wait_limit_ns;
   return XNS_OK;
 }
 

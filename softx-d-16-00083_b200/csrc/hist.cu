@@ -95,8 +95,10 @@ __global__ void elem_bbox_kernel(const double *__restrict__ X, const double *__r
   for (uint32_t i = a0 + blockIdx.x * blockDim.x + threadIdx.x; i < a1; i += gridDim.x * blockDim.x) {
     const double v[3] = {X[i], Y[i], Z[i]};
     for (int k = 0; k < 3; k++) {
-      mn[k] = fmin(mn[k], v[k]);
-      mx[k] = fmax(mx[k], v[k]);
+      // fmin / fmax skip a NaN: it widens the box to infinity instead, so that the plan rejects it
+      const bool nan = !(v[k] == v[k]);
+      mn[k] = fmin(mn[k], nan ? -INFINITY : v[k]);
+      mx[k] = fmax(mx[k], nan ? INFINITY : v[k]);
     }
   }
   for (int k = 0; k < 3; k++)

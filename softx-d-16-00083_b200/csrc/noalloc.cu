@@ -125,6 +125,12 @@ extern "C" int xns_int_1d_hist_noalloc(const uint64_t *hist_dev, const uint32_t 
   const uint32_t P = nel * (nel + 1) / 2;
   double q0 = 0, dq = 0;
   const bool uniform = xns_uniform_mesh(q, nq, &q0, &dq);
+  // one lane per M q values, at most SE_THREADS lanes: 8192 q on a uniform mesh, 2048 otherwise
+  const int M = uniform ? SE_M_UNIFORM : SE_M_DIRECT;
+  const uint32_t chunks = (nq + M - 1) / M;
+  int lanes = 1;
+  while (lanes < (int)chunks) lanes <<= 1;
+  if (lanes > SE_THREADS || (!uniform && nq > XNS_NOALLOC_MAX_Q_NONUNIFORM)) return XNS_ERR_LIMIT;
   // scratch layout: weights [nel][nq] | q mesh [nq] | tables [2P + nel] | +1e-8 histogram [P][nb] |
   // +1e-8 sums [P][nq] | per-CTA partial sums [G][P][nq]
   uint32_t eps_nb;
@@ -185,11 +191,6 @@ extern "C" int xns_int_1d_hist_noalloc(const uint64_t *hist_dev, const uint32_t 
   p.eps_nb = eps_nb;
   p.eps_inv_bw = 1.0 / eps_bin;
   BinSrc src{(const unsigned long long *)hist_dev, nhist, tpp, bin};
-  const int M = uniform ? SE_M_UNIFORM : SE_M_DIRECT;
-  const uint32_t chunks = (nq + M - 1) / M;
-  int lanes = 1;
-  while (lanes < (int)chunks) lanes <<= 1;
-  if (lanes > SE_THREADS) return XNS_ERR_LIMIT;
   if (uniform) {
     const size_t smem = sinc_smem_bytes(SE_M_UNIFORM, lanes, 0);
     sinc_tiles_kernel<SE_M_UNIFORM, false, BinSrc><<<(unsigned)grid, SE_THREADS, smem, s>>>(p, src, lanes);

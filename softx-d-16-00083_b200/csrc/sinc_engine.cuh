@@ -8,15 +8,18 @@
 // Records (r, w) arrive in tiles of up to SE_TILE produced cooperatively by a Source in shared
 // memory.  A lane owns a chunk of M consecutive q values, a slot of lanes walks the tile's records.
 // On a uniform mesh q_k = q0 + k dq the lane seeds s_0 = sin(q_{k0} r) w/r and the difference
-// d_0 = s_0 - s_{-1} = (sin(x) (1 - cos t) + cos(x) sin t) w/r (x = q_{k0} r, t = dq r) from an FP64
-// sine and cosine of the FP64 phase (xmath.cuh, on the FP64 pipe), rounded once to FP32, and runs the
-// sine recurrence in Reinsch's difference form,
+// d_0 = s_0 - s_{-1} = (sin(x) (1 - cos t) + cos(x) sin t) w/r (x = q_{k0} r, t = dq r) from an
+// accurate sine and cosine of the FP64-reduced phase (xmath.cuh: the MUFU approximations would add
+// coherently over the distance shells of a crystal), and runs the sine recurrence in Reinsch's
+// difference form,
 //   d_{k+1} = d_k - lam s_k,  s_{k+1} = s_k + d_{k+1},  lam = 4 sin^2(t/2),
 // which is the Chebyshev recurrence s_{k+1} = 2cos(t) s_k - s_{k-1} with 2cos(t) kept as 2 - lam: lam
 // carries full relative precision even for small t, so the phase does not drift the way a rounded
-// 2cos(t) (error 2^-24 / sin t per step) would on fine q meshes.  A lane runs four records side by
-// side, as two packed pairs (f32x2.cuh): per (record, q) term one FFMA and one FADD for the sine, plus
-// 3/4 FADD for the pairwise sum of the four, no transcendental, in 7 instructions per four terms.
+// 2cos(t) (error 2^-24 / sin t per step) would on fine q meshes.  A lane runs eight records side by
+// side, as four packed pairs (f32x2.cuh): per (record, q) term one FFMA and one FADD for the sine, plus
+// 7/8 FADD for the tree sum of the eight, no transcendental, in 13 instructions per eight terms.  The
+// next eight records' seeds are computed in the same straight-line block as this recurrence, so that
+// their latency overlaps its steps.
 //
 // Accumulation: FP32 sums over at most SE_FP32_GROUPS groups of four records, then FP64 totals in
 // shared memory, one column per chunk and warp (the lanes of a warp that own the same chunk add their
@@ -42,20 +45,21 @@
 namespace xns_sinc {
 
 constexpr int SE_THREADS = 128;
-// CTAs per SM the register allocation is sized for (168 registers a thread at 3).
-#ifndef SE_MIN_CTAS
-#define SE_MIN_CTAS 3
-#endif
-// Records per tile.  With 16 lanes per slot (1024 q) a lane takes 12 groups of four records per
-// tile; the FP64 totals take 32 KB, the records 15 KB: three CTAs (12 warps, at most 168 registers a
-// thread) share an SM.
+// CTAs per SM the register allocation is sized for (168 registers a thread).
+constexpr int SE_MIN_CTAS = 3;
+// Records per tile.  With 16 lanes per slot (1024 q) a lane takes 6 groups of eight records per tile;
+// the FP64 totals take 32 KB, the records 9 KB: three CTAs (12 warps) share an SM.
 constexpr int SE_TILE = 384;
-// q values per lane: M_UNIFORM for the recurrence (a seed costs ~25 FP64-pipe instructions, the
-// recurrence 1.75 issue slots per term), M_DIRECT for the per-term sine of a non-uniform mesh.
+// q values per lane: M_UNIFORM for the recurrence (a seed costs ~30 instructions, the recurrence
+// 1.6 issue slots per term), M_DIRECT for the per-term sine of a non-uniform mesh.
 constexpr int SE_M_UNIFORM = 64;
 constexpr int SE_M_DIRECT = 16;
-// Record groups (4 records each) a lane sums in FP32 before the sums go to FP64.
-constexpr int SE_FP32_GROUPS = 12;
+// Records a lane runs side by side (four packed pairs).
+constexpr int SE_GROUP = 8;
+// Record groups a lane sums in FP32 before the sums go to FP64 (at most 96 records, with the pair of
+// lanes that share a chunk at 1024 q; the error of these FP32 sums is the largest term of the error
+// budget at the deepest minima of a pattern).
+constexpr int SE_FP32_GROUPS = 6;
 // The +1e-8 histogram: bins of at least EPS_BIN_MIN, at most EPS_NB_MAX of them.
 constexpr double EPS_BIN_MIN = 0.05;
 constexpr uint32_t EPS_NB_MAX = 16384;
@@ -63,14 +67,13 @@ constexpr double SINC_EPS = 1e-8;  // CalcFunctions.cpp:581, :861
 
 struct PairRec {
   double r;    // distance (FP64)
-  double w;    // weight / r; 0 for a record that does not count
-  double a;    // w sin(t),            t = dq r
-  double b;    // w (1 - cos t) = 2 w sin^2(t/2)
+  float w;     // weight / r; 0 for a record that does not count
+  float a;     // w sin(t),            t = dq r
+  float b;     // w (1 - cos t) = 2 w sin^2(t/2)
   float lam;   // 4 sin^2(t/2) = 2 - 2 cos(t)
-  float pad;
 };
 
-__device__ __forceinline__ PairRec null_rec() { return PairRec{1.0, 0.0, 0.0, 0.0, 0.f, 0.f}; }
+__device__ __forceinline__ PairRec null_rec() { return PairRec{1.0, 0.f, 0.f, 0.f, 0.f}; }
 
 struct SincParams {
   double q0, dq;      // uniform mesh
@@ -93,11 +96,10 @@ __device__ __forceinline__ PairRec make_rec(const SincParams &p, uint32_t cls, d
   xns_math::xns_sincos64(0.5 * p.dq * r, &sh, &ch);
   const double wr = w / r;
   rec.r = r;
-  rec.w = wr;
-  rec.a = 2.0 * sh * ch * wr;
-  rec.b = 2.0 * sh * sh * wr;
+  rec.w = (float)wr;
+  rec.a = (float)(2.0 * sh * ch * wr);
+  rec.b = (float)(2.0 * sh * sh * wr);
   rec.lam = (float)(4.0 * sh * sh);
-  rec.pad = 0.f;
   if (p.eps_hist) {
     const uint32_t k = (uint32_t)fmin(r * p.eps_inv_bw, (double)(p.eps_nb - 1));
     atomicAdd(p.eps_hist + (size_t)cls * p.eps_nb + k, wr / r);
@@ -153,14 +155,14 @@ __global__ void __launch_bounds__(SE_THREADS, SE_MIN_CTAS) sinc_tiles_kernel(Sin
     float blk[M];
 #pragma unroll
     for (int k = 0; k < M; k++) blk[k] = 0.f;
-    if (active) {
+    if (active && DIRECT) {
       int nblk = 0;  // record groups in blk
       // a lane takes four records per step: e, e + S, e + 2S, e + 3S (S = slots)
       for (int e = slot; e < n; e += 4 * nslots) {
         PairRec R[4];
 #pragma unroll
         for (int g = 0; g < 4; g++) R[g] = e + g * nslots < n ? pr[e + g * nslots] : null_rec();
-        if (R[0].w == 0.0 && R[1].w == 0.0 && R[2].w == 0.0 && R[3].w == 0.0) continue;
+        if (R[0].w == 0.f && R[1].w == 0.f && R[2].w == 0.f && R[3].w == 0.f) continue;
         if (share == 1 && nblk == SE_FP32_GROUPS) {  // long tiles: FP32 sums stay short
 #pragma unroll
           for (int k = 0; k < M; k++) {
@@ -170,43 +172,67 @@ __global__ void __launch_bounds__(SE_THREADS, SE_MIN_CTAS) sinc_tiles_kernel(Sin
           nblk = 0;
         }
         nblk++;
-        if (DIRECT) {
-          float wr[4];
+        float wr[4];
 #pragma unroll
-          for (int g = 0; g < 4; g++) wr[g] = (float)R[g].w;
+        for (int g = 0; g < 4; g++) wr[g] = R[g].w;
+#pragma unroll
+        for (int k = 0; k < M; k++) {
+          float t = 0.f;
+#pragma unroll
+          for (int g = 0; g < 4; g++) t += xns_math::xns_sin(qd[k] * R[g].r) * wr[g];
+          blk[k] += t;
+        }
+      }
+    } else if (active) {
+      // a lane takes SE_GROUP records per step: e, e + S, ..., e + (SE_GROUP - 1) S (S = slots); the
+      // next group's seeds are computed in one straight-line block with this group's recurrence
+      constexpr int G = SE_GROUP, H = SE_GROUP / 2;
+      float s[G], d[G], lam[G];
+      auto seeds = [&](int e0, float *so, float *dO, float *lo_) {
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+          const PairRec R = e0 + g * nslots < n ? pr[e0 + g * nslots] : null_rec();
+          float sn, cs;
+          xns_math::xns_sincos(qk0 * R.r, &sn, &cs);
+          so[g] = sn * R.w;
+          dO[g] = fmaf(cs, R.a, sn * R.b);
+          lo_[g] = R.lam;
+        }
+      };
+      seeds(slot, s, d, lam);
+      int nblk = 0;  // record groups in blk
+      for (int e = slot; e < n; e += G * nslots) {
+        if (share == 1 && nblk == SE_FP32_GROUPS) {  // long tiles: FP32 sums stay short
 #pragma unroll
           for (int k = 0; k < M; k++) {
-            float t = 0.f;
-#pragma unroll
-            for (int g = 0; g < 4; g++) t += xns_math::xns_sin(qd[k] * R[g].r) * wr[g];
-            blk[k] += t;
+            acc64[k * ncol + col] += (double)blk[k];
+            blk[k] = 0.f;
           }
-        } else {
-          // seeds in FP64, each rounded once: s_0 = sin(x) w/r, d_0 = (cos(x) sin t + sin(x) (1 - cos t)) w/r
-          float s[4], d[4], lam[4];
+          nblk = 0;
+        }
+        nblk++;
+        using namespace xns_f2;
+        f2 S[H], D[H], L[H];
 #pragma unroll
-          for (int g = 0; g < 4; g++) {
-            double sn, cs;
-            xns_math::xns_sincos64(qk0 * R[g].r, &sn, &cs);
-            s[g] = (float)(sn * R[g].w);
-            d[g] = (float)__fma_rn(cs, R[g].a, sn * R[g].b);
-            lam[g] = R[g].lam;
-          }
-          // the recurrence on packed pairs of records (0, 1) and (2, 3): the same roundings as scalar
-          // FFMA / FADD, half the instructions
-          using namespace xns_f2;
-          f2 S01 = pack(s[0], s[1]), S23 = pack(s[2], s[3]), D01 = pack(d[0], d[1]), D23 = pack(d[2], d[3]);
-          const f2 L01 = pack(-lam[0], -lam[1]), L23 = pack(-lam[2], -lam[3]);
-          blk[0] += (s[0] + s[2]) + (s[1] + s[3]);
+        for (int h = 0; h < H; h++) {  // packed pairs of records (h, h + H)
+          S[h] = pack(s[h], s[h + H]);
+          D[h] = pack(d[h], d[h + H]);
+          L[h] = pack(-lam[h], -lam[h + H]);
+        }
+        seeds(e + G * nslots, s, d, lam);
+        {
+          const f2 u = add(add(S[0], S[1]), add(S[2], S[3]));
+          blk[0] += lo(u) + hi(u);
+        }
+        // the recurrence on packed pairs: the same roundings as scalar FFMA / FADD, half the instructions
 #pragma unroll
-          for (int k = 1; k < M; k++) {
-            D01 = xns_f2::fma(L01, S01, D01);
-            D23 = xns_f2::fma(L23, S23, D23);
-            S01 = add(S01, D01);
-            S23 = add(S23, D23);
-            const f2 u = add(S01, S23);  // (s0 + s2, s1 + s3)
-            blk[k] += lo(u) + hi(u);
-          }
+        for (int k = 1; k < M; k++) {
+#pragma unroll
+          for (int h = 0; h < H; h++) D[h] = xns_f2::fma(L[h], S[h], D[h]);
+#pragma unroll
+          for (int h = 0; h < H; h++) S[h] = add(S[h], D[h]);
+          const f2 u = add(add(S[0], S[1]), add(S[2], S[3]));
+          blk[k] += lo(u) + hi(u);
         }
       }
     }

@@ -73,6 +73,8 @@ struct XArgs {
   double scale;  // value of one unit of the Horner sum over the levels
   int *err;
   uint32_t ksplit;  // 0: stream-K over all units; else K parts per output tile (grid = parts x tiles)
+  unsigned long long wait_ns;  // bound of every pipeline wait (WAIT_LIMIT_NS unless a test asked less)
+  int no_loads;                // failure-path test (xns_inject_pipeline_stall): the loader issues nothing
 };
 
 template <class E>
@@ -132,9 +134,9 @@ __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) 
     if (lane == 0) {  // loader
       uint32_t fills[XSTAGES] = {};
       unsigned long long i = 0;
-      for (unsigned long long u = u0; u < u1; ++u, ++i) {
+      for (unsigned long long u = g.no_loads ? u1 : u0; u < u1; ++u, ++i) {
         const uint32_t s = (uint32_t)(i % XSTAGES), k = (uint32_t)(i / XSTAGES);
-        if (k > 0 && !mbar_wait(empty0 + 8 * s, (k - 1) & 1u, abort, WAIT_LIMIT_NS)) {
+        if (k > 0 && !mbar_wait(empty0 + 8 * s, (k - 1) & 1u, abort, g.wait_ns)) {
           abort_sh = 1;
           atomicOr(g.err, 1);
           break;
@@ -169,14 +171,14 @@ __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) 
         const bool seg_last = (u + 1 == u1) || ((u + 1) % KT == 0);
         const bool first = seg_first || in_chunk == 0;
         if (first && chunk >= 2) {  // the drain warps have read this buffer's previous chunk
-          if (!mbar_wait(tempty0 + 8 * (chunk & 1u), ((chunk >> 1) - 1) & 1u, abort, WAIT_LIMIT_NS)) {
+          if (!mbar_wait(tempty0 + 8 * (chunk & 1u), ((chunk >> 1) - 1) & 1u, abort, g.wait_ns)) {
             abort_sh = 1;
             atomicOr(g.err, 1);
             break;
           }
           tc_fence_after();
         }
-        if (!mbar_wait(full0 + 8 * s, k & 1u, abort, WAIT_LIMIT_NS)) {
+        if (!mbar_wait(full0 + 8 * s, k & 1u, abort, g.wait_ns)) {
           abort_sh = 1;
           atomicOr(g.err, 1);
           break;
@@ -231,7 +233,7 @@ __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) 
       in_chunk = 0;
       const uint32_t b = chunk & 1u;
       if (!E::ALT || b == h) {
-        const bool ok = mbar_wait(tfull0 + 8 * b, (chunk >> 1) & 1u, abort, WAIT_LIMIT_NS);
+        const bool ok = mbar_wait(tfull0 + 8 * b, (chunk >> 1) & 1u, abort, g.wait_ns);
         if (__any_sync(0xffffffffu, !ok)) {
           abort_sh = 1;
           if (lane == 0) atomicOr(g.err, 1);
@@ -368,7 +370,11 @@ __global__ void max_count_kernel(const unsigned long long *__restrict__ hist, ui
 // Launches the digit GEMM of scheme E; grid 0: one CTA per SM (stream-K over all units), otherwise the
 // given number of CTAs.
 template <class E>
-int launch_digit_gemm(xns_ctx *ctx, const XArgs &g, unsigned grid) {
+int launch_digit_gemm(xns_ctx *ctx, const XArgs &g0, unsigned grid) {
+  XArgs g = g0;
+  g.wait_ns = ctx->inject_stall_ns ? ctx->inject_stall_ns : WAIT_LIMIT_NS;
+  g.no_loads = ctx->inject_stall_ns != 0;
+  ctx->inject_stall_ns = 0;  // one call only
   static bool attr_set[XNS_MAX_DEVICES] = {};  // the attribute is per device; set once on each
   if (ctx->device < 0 || ctx->device >= XNS_MAX_DEVICES || !attr_set[ctx->device]) {
     XNS_CUDA(ctx, cudaFuncSetAttribute(sinc_exact_kernel<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, E::SMEM));

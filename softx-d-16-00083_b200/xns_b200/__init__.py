@@ -50,6 +50,8 @@ def _declare(lib):
     lib.xns_status_string.argtypes = [_int]
     lib.xns_status_string.restype = C.c_char_p
     lib.xns_set_stream.argtypes = [_p, _p]
+    lib.xns_set_memory_limit.argtypes = [_p, C.c_uint64]
+    lib.xns_inject_pipeline_stall.argtypes = [_p, C.c_uint64]
     lib.xns_last_kernel_ms.argtypes = [_p]
     lib.xns_last_kernel_ms.restype = _dbl
     lib.xns_kernel_launches.argtypes = [_p]
@@ -312,6 +314,15 @@ class Context:
 
     def set_stream(self, stream_ptr):
         self._check(lib.xns_set_stream(self._h, stream_ptr))
+
+    def inject_pipeline_stall(self, wait_limit_ns):
+        """Failure-path test: the next tensor-core transform's waits run out (see the header)."""
+        self._check(lib.xns_inject_pipeline_stall(self._h, int(wait_limit_ns)))
+
+    def set_memory_limit(self, nbytes):
+        """Caps the calc functions' device scratch in this context (0: no cap); a call that would need
+        more raises XnsError with status XNS_ERR_NOMEM (5)."""
+        self._check(lib.xns_set_memory_limit(self._h, int(nbytes)))
 
     # -- structure builder -----------------------------------------------------------------------
     def build_atoms(self, blocks, nel, seed=0):

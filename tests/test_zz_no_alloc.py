@@ -73,6 +73,38 @@ def test_noalloc_matches_allocating_entry_point(gpu_ctx):
     assert rel_err(out_x.cpu().numpy(), gx["I"]) < TOL_I
 
 
+def test_noalloc_large_histogram_and_nonuniform_mesh(gpu_ctx, oracle):
+    """A 10-cell rock-salt cube at 0.001 A (about 7200 atoms, 3 x 97,000 bins) on 4096 q: the deep
+    low-q minima of I(q), where the bin sum cancels to ~1e-5 of its terms, are where an FP32 sum shows.
+    The allocation-free result stays within TOL_I of the allocating entry point (exact integer-digit
+    sums) and of the oracle, on two calls in a row; then a non-uniform mesh (per-term sines) of 1500 q."""
+    import torch
+    from xns_b200 import synth
+    f = _noalloc()
+    els = synth.rocksalt_cube(cells=10, seed=21)
+    nh = synth.hist_size(els, 0.001)
+    h = gpu_ctx.calc_hist(els, nh, 0.001)
+    n_el = np.array([len(e) for e in els], dtype=np.uint32)
+    sl = np.array([3.63, 9.58])
+    q = synth.q_mesh(0.1, 25.0, 4096)
+    want = gpu_ctx.calc_int_1d_hist(h, n_el, nh, 0.001, q, 0, sl=sl)
+    ref = oracle.int_1d_hist(h, n_el, nh, 0.001, q, 0, sl=sl)
+    assert rel_err(want, ref) < TOL_I
+    dev = torch.device("cuda", 0)
+    dh = torch.from_numpy(h.view(np.int64)).to(dev)
+    out = torch.full((len(q),), float("nan"), dtype=torch.float64, device=dev)
+    for _ in range(2):
+        assert _call(f, dh, n_el, nh, 0.001, q, 0, None, sl, False, 0.0, out) == 0
+        got = out.cpu().numpy()
+        assert rel_err(got, want) < TOL_I
+        assert rel_err(got, ref) < TOL_I
+    qn = np.sort(np.random.default_rng(22).uniform(0.05, 20.0, 1500))
+    want_n = gpu_ctx.calc_int_1d_hist(h, n_el, nh, 0.001, qn, 0, sl=sl)
+    out_n = torch.full((len(qn),), float("nan"), dtype=torch.float64, device=dev)
+    assert _call(f, dh, n_el, nh, 0.001, qn, 0, None, sl, False, 0.0, out_n) == 0
+    assert rel_err(out_n.cpu().numpy(), want_n) < TOL_I
+
+
 def test_noalloc_rejects_sizes_beyond_its_limits(gpu_ctx):
     import torch
     f = _noalloc()
@@ -83,3 +115,8 @@ def test_noalloc_rejects_sizes_beyond_its_limits(gpu_ctx):
     h = torch.zeros(nel * (nel + 1) // 2 * nhist, dtype=torch.int64, device=dev)
     out = torch.zeros(16, dtype=torch.float64, device=dev)
     assert _call(f, h, n_el, nhist, 0.1, np.linspace(0.1, 5, 16), 0, None, np.ones(nel), False, 0.0, out) == XNS_ERR_LIMIT
+    # a non-uniform mesh takes 16 q per lane: at most XNS_NOALLOC_MAX_Q_NONUNIFORM (2048) points
+    h2 = torch.zeros(nhist, dtype=torch.int64, device=dev)
+    qn = np.sort(np.random.default_rng(3).uniform(0.1, 5.0, 2049))
+    out2 = torch.zeros(len(qn), dtype=torch.float64, device=dev)
+    assert _call(f, h2, [2], nhist, 0.1, qn, 0, None, np.ones(1), False, 0.0, out2) == XNS_ERR_LIMIT
