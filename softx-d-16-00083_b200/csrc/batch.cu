@@ -190,7 +190,7 @@ int batch_build(xns_batch *b, uint32_t nstruct, const uint32_t *nel, const uint3
   if ((st = xns_hist_check(ctx, b->hl))) return st;
   unsigned long long maxc = 0;
   if ((st = xns_tc_max_count(ctx, b->d_hist, cls, nhist, nhist, &maxc))) return st;
-  if ((st = xns_tc_exact_plan(ctx, b->d_hist, cls, nhist, nhist, bin, q, nq, maxc, b->d_G, &b->xl))) return st;
+  if ((st = xns_tc_exact_plan(ctx, b->d_hist, cls, nhist, nhist, bin, q, nq, maxc, b->d_G, &b->xl, true))) return st;
   if ((st = xns_stage_begin(ctx, STAGE_IQ))) return st;
   if ((st = xns_tc_exact_enqueue(ctx, b->xl))) return st;
   if ((st = batch_epilogue(b))) return st;

@@ -18,7 +18,11 @@
 //
 // Tile 128 q x N columns x 64 k (N = 16 or 32 for the transform, 64 for the plane), one CTA per SM,
 // 2 stages of {NA A-digit tiles, NB B-digit tiles}; warp 0 loads (cp.async.bulk), warp 1 issues the
-// MMAs, warps 2-9 drain tensor memory.  The accumulators are double-buffered in tensor memory
+// MMAs, warps 2-9 drain tensor memory.  For the sinc transform the A digits are not loaded: warps
+// 10-13 compute them into the stage (one q row per thread: an FP64 sine by rotation from one sincos
+// per row and k tile, the sinc by an FP64 reciprocal, the five digits in FP32 from a hi/lo split;
+// a fence.proxy.async makes the writes visible to the tensor core before the row's mbarrier arrival),
+// so the only HBM traffic is the count digits and the output.  The accumulators are double-buffered in tensor memory
 // (2 x levels x N <= 512 columns), so the MMAs of one chunk run while the previous chunk is drained;
 // with N <= 32 the two groups of four drain warps take alternate chunks (one buffer each), with N = 64
 // each group drains 32 columns of every chunk.  Waits are bounded as in tc_gemm.cu.
@@ -39,6 +43,9 @@ constexpr int XA = XM * XK * 2;            // 16 KB per S-digit tile
 constexpr int XSTAGES = 2;
 constexpr int CH_TILES = 2;                // k tiles per exact chunk (CH_K = 128)
 constexpr int XTHREADS = 320;
+constexpr int XDRAIN_THREADS = 256;              // warps 2-9
+constexpr int XGEN_WARPS = 8;                    // sinc-digit producers (warps 10-17): a q row, half the k
+constexpr int XTHREADS_GEN = XTHREADS + 32 * XGEN_WARPS;
 constexpr uint32_t XTMEM_COLS = 512;
 
 // A digit scheme: NA digit planes of the A operand, NB of the B operand, NL accumulator levels, and the
@@ -50,7 +57,7 @@ template <int NA_, int NB_, int NL_, int KIND, int N_>
 struct Scheme {
   static constexpr int NA = NA_, NB = NB_, NL = NL_, N = N_;
   static constexpr int XB = N * XK * 2;  // bytes per B-digit tile
-  static constexpr bool ALT = N <= 32;   // drain groups take alternate chunks (else split the columns)
+  static constexpr bool ALT = N <= 16;   // drain groups take alternate chunks (else split the columns)
   static constexpr int STAGE = NA * XA + NB * XB;
   static constexpr int SMEM = XSTAGES * STAGE + 1024;
   static_assert(N % 16 == 0 && N >= 16 && N <= 64, "N tile: 16, 32 or 64 columns");
@@ -75,10 +82,122 @@ struct XArgs {
   uint32_t ksplit;  // 0: stream-K over all units; else K parts per output tile (grid = parts x tiles)
   unsigned long long wait_ns;  // bound of every pipeline wait (WAIT_LIMIT_NS unless a test asked less)
   int no_loads;                // failure-path test (xns_inject_pipeline_stall): the loader issues nothing
+  // sinc digits made on chip (GEN): the q mesh (m_valid rows), the bin width and the bins used
+  const double *qv;
+  double bin;
+  uint32_t nh;
 };
 
-template <class E>
-__global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) {
+// Conversions between FP64 and FP32 by integer operations (no conversion-pipe instruction):
+// d with its low 29 mantissa bits cleared (24 significant bits, truncated toward zero) ...
+__device__ __forceinline__ double short_double(double d) {
+  return __hiloint2double(__double2hiint(d), __double2loint(d) & (int)0xe0000000);
+}
+// ... exactly as FP32 (0 below the FP32 normal range) ...
+__device__ __forceinline__ float f32_of_short(double d) {
+  const unsigned h = (unsigned)__double2hiint(d), l = (unsigned)__double2loint(d), mag = h & 0x7fffffffu;
+  const unsigned bits = ((mag - (896u << 20)) << 3) | (l >> 29) | (h & 0x80000000u);
+  return __uint_as_float(mag < (897u << 20) ? (h & 0x80000000u) : bits);
+}
+// ... and a normal FP32 (or 0) exactly as FP64.
+__device__ __forceinline__ double f64_of_f32(float f) {
+  const unsigned b = __float_as_uint(f), mag = b & 0x7fffffffu;
+  const unsigned hi = (mag ? (mag >> 3) + (896u << 20) : 0u) | (b & 0x80000000u);
+  return __hiloint2double((int)hi, (int)(mag << 29));
+}
+
+// 1/d for 1e-30 < d < 1e30: the FP32 reciprocal of d truncated to FP32 (relative error below 2^-21)
+// and two Newton steps in FP64, each squaring the relative error (to the FP64 rounding).
+__device__ __forceinline__ double recip64(double d) {
+  float rf;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rf) : "f"(f32_of_short(short_double(d))));
+  double r = f64_of_f32(rf);
+  double e = __fma_rn(-d, r, 1.0);
+  r = __fma_rn(r, e, r);
+  e = __fma_rn(-d, r, 1.0);
+  return __fma_rn(r, e, r);
+}
+
+// The five balanced base-256 digits of x = 128 v (|v| <= 1) as BF16 bit patterns (upper halves):
+// N = round(x 2^32) comes out of one FMA with 1.5 * 2^52 (the integer lands in the mantissa: low word
+// N mod 2^32, the low 20 bits of the high word 2^19 + floor(N / 2^32)); adding 0x80808080 biases each
+// of the four low bytes by 128 with the carries, so that byte j of the sum minus 128 is digit j and
+// the carried high part is the top digit:  x = sum_{i<5} dig[i] 256^-i + e, |dig[i]| <= 128,
+// |e| <= 2^-33.  A digit becomes an exact FP32 by planting its byte under the exponent of 2^23 and
+// subtracting 2^23 + 128; its BF16 is then the upper half of those bits.  dig[0] is the top digit.
+__device__ __forceinline__ void sinc_digits(double x, uint32_t *dig) {
+  const double t = __fma_rn(x, 4294967296.0, 6755399441055744.0);
+  const uint32_t lo = (uint32_t)__double2loint(t);
+  const int hi = (__double2hiint(t) & 0xfffff) - (1 << 19);
+  uint32_t lo2;
+  int hi2;
+  asm("add.cc.u32 %0, %2, 0x80808080;\n\taddc.s32 %1, %3, 0;" : "=r"(lo2), "=r"(hi2) : "r"(lo), "r"(hi));
+  const float B = 8388736.0f;  // 2^23 + 128
+  dig[0] = __float_as_uint(__int_as_float(0x4B000000 + hi2 + 128) - B);
+#pragma unroll
+  for (int j = 0; j < 4; j++)  // byte 3 - j of lo2 is digit 1 + j (the most significant first)
+    dig[1 + j] = __float_as_uint(__uint_as_float(__byte_perm(lo2, 0x4B000000u, 0x7540u | (3 - j))) - B);
+}
+
+// The sinc digits of 32 consecutive bins kb .. kb + 31 of one q row (q = qm), 8 bins per call of
+// chunk(), as the BF16 bit patterns of the five digit planes (one uint4 of 8 bins per plane).  Both the
+// on-chip producers and the HBM-plane kernel make every (row, k tile, half) with this same sequence, so
+// the two give identical digits: sin by rotation from an FP64 sincos at kb (drift over 32 bins
+// ~1e-14), x = q r_k stepped by q bin, 1/(x + 1e-8) from rcp.approx plus two Newton steps at kb (and
+// everywhere in the first k tile, where neighbouring x differ by factors up to 3), otherwise by three
+// Newton steps from the previous bin's reciprocal (relative error of that start below 1/64).
+struct SincRun {
+  double sn, cs, x, r, sd, cd, qb;
+  bool first_tile;
+  __device__ __forceinline__ void init(double qm, double bin, uint32_t kb, double sd_, double cd_) {
+    sd = sd_;
+    cd = cd_;
+    qb = qm * bin;
+    x = ((kb + 0.5) * bin) * qm;  // qrij = rij * q[iq] (CalcFunctions.cpp:858-861)
+    sincos(x, &sn, &cs);
+    sn *= 128.0;
+    cs *= 128.0;
+    first_tile = kb < XK;
+  }
+  __device__ __forceinline__ void chunk(uint32_t c, uint4 *w) {
+    uint32_t dig[NDS][8];
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+      const double den = x + 0.00000001;
+      if (first_tile || (c == 0 && e == 0)) {
+        r = recip64(den);
+      } else {
+        double er = __fma_rn(-den, r, 1.0);
+        r = __fma_rn(r, er, r);
+        er = __fma_rn(-den, r, 1.0);
+        r = __fma_rn(r, er, r);
+        er = __fma_rn(-den, r, 1.0);
+        r = __fma_rn(r, er, r);
+      }
+      // the reference's sin(q r)/(q r + 1e-8), times 128
+      uint32_t d5[NDS];
+      sinc_digits(sn * r, d5);
+#pragma unroll
+      for (int d = 0; d < NDS; d++) dig[d][e] = d5[d];
+      const double s1 = __fma_rn(sn, cd, cs * sd), c1 = __fma_rn(cs, cd, -(sn * sd));
+      sn = s1;
+      cs = c1;
+      x += qb;
+    }
+#pragma unroll
+    for (int d = 0; d < NDS; d++) {
+      w[d].x = __byte_perm(dig[d][0], dig[d][1], 0x7632);
+      w[d].y = __byte_perm(dig[d][2], dig[d][3], 0x7632);
+      w[d].z = __byte_perm(dig[d][4], dig[d][5], 0x7632);
+      w[d].w = __byte_perm(dig[d][6], dig[d][7], 0x7632);
+    }
+  }
+};
+
+__device__ __forceinline__ uint32_t chunk_offset(uint32_t row, uint32_t ch);
+
+template <class E, bool GEN>
+__global__ void __launch_bounds__(GEN ? XTHREADS_GEN : XTHREADS, 1) sinc_exact_kernel(const XArgs g) {
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) unsigned long long bars[2 * XSTAGES + 5];
   __shared__ uint32_t tmem_sh;
@@ -94,12 +213,12 @@ __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) 
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < XSTAGES; s++) {
-      mbar_init(full0 + 8 * s, 1);
+      mbar_init(full0 + 8 * s, GEN ? 1 + 32 * XGEN_WARPS : 1);  // the copy warp (+ every producer thread)
       mbar_init(empty0 + 8 * s, 1);
     }
     for (int b = 0; b < 2; b++) {
       mbar_init(tfull0 + 8 * b, 1);
-      mbar_init(tempty0 + 8 * b, E::ALT ? 128 : XTHREADS - 64);
+      mbar_init(tempty0 + 8 * b, E::ALT ? 128 : XDRAIN_THREADS);
     }
     mbar_init(drain, 1);
     abort_sh = 0;
@@ -146,9 +265,11 @@ __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) 
         const uint32_t mt = (uint32_t)(r % g.MT), nt = (uint32_t)(r / g.MT);
         const uint32_t dst = base + s * E::STAGE, bar = full0 + 8 * s;
         const size_t ao = ((size_t)mt * g.KT + kt) * XA, bo = ((size_t)nt * g.KT + kt) * E::XB;
-        mbar_expect_tx(bar, (uint32_t)E::STAGE);
+        mbar_expect_tx(bar, (uint32_t)(GEN ? E::NB * E::XB : E::STAGE));
+        if (!GEN) {
 #pragma unroll
-        for (int d = 0; d < E::NA; d++) bulk_g2s(dst + d * XA, g.A + d * g.a_plane + ao, XA, bar);
+          for (int d = 0; d < E::NA; d++) bulk_g2s(dst + d * XA, g.A + d * g.a_plane + ao, XA, bar);
+        }
 #pragma unroll
         for (int e = 0; e < E::NB; e++) bulk_g2s(dst + E::NA * XA + e * E::XB, g.B + e * g.b_plane + bo, E::XB, bar);
         fills[s] = k + 1;
@@ -215,13 +336,13 @@ __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) 
         mbar_wait(drain, 0, nullptr, DRAIN_LIMIT_NS);
       }
     }
-  } else {
+  } else if (warp < 10) {
     // drain: warp w reads TMEM lanes 32*(w%4) .. +31 (its quarter of the 128 rows).  Group h = 0, 1:
     // with ALT, chunks c with c % 2 == h (buffer h), all N columns; otherwise every chunk, columns
-    // 32 h .. 32 h + 31.
-    constexpr int COLS = E::ALT ? E::N : 32;
+    // h N/2 .. (h + 1) N/2 - 1.
+    constexpr int COLS = E::ALT ? E::N : E::N / 2;
     const uint32_t wq = warp & 3, h = (uint32_t)(warp - 2) >> 2;
-    const uint32_t lane_addr = tmem + ((wq * 32u) << 16) + (E::ALT ? 0u : h * 32u);
+    const uint32_t lane_addr = tmem + ((wq * 32u) << 16) + (E::ALT ? 0u : h * (uint32_t)COLS);
     double sum[COLS];
 #pragma unroll
     for (int j = 0; j < COLS; j++) sum[j] = 0.0;
@@ -241,19 +362,19 @@ __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) 
         }
         tc_fence_after();
 #pragma unroll
-        for (int c = 0; c < COLS; c += 16) {
-          double t[16];
+        for (int c = 0; c < COLS; c += 8) {
+          double t[8];
 #pragma unroll
-          for (int j = 0; j < 16; j++) t[j] = 0.0;
+          for (int j = 0; j < 8; j++) t[j] = 0.0;
 #pragma unroll
           for (int lev = 0; lev < E::NL; lev++) {  // Horner over the levels, top first
-            uint32_t rr[16];
-            tc_ld16_raw(lane_addr + b * BUFCOLS + lev * E::N + c, rr);
+            uint32_t rr[8];
+            tc_ld8_raw(lane_addr + b * BUFCOLS + lev * E::N + c, rr);
 #pragma unroll
-            for (int j = 0; j < 16; j++) t[j] = t[j] * 256.0 + (double)__uint_as_float(rr[j]);
+            for (int j = 0; j < 8; j++) t[j] = t[j] * 256.0 + (double)__uint_as_float(rr[j]);
           }
 #pragma unroll
-          for (int j = 0; j < 16; j++) sum[c + j] += t[j];
+          for (int j = 0; j < 8; j++) sum[c + j] += t[j];
         }
         tc_fence_before();
         mbar_arrive(tempty0 + 8 * b);
@@ -267,13 +388,50 @@ __global__ void __launch_bounds__(XTHREADS, 1) sinc_exact_kernel(const XArgs g) 
         if (m < g.m_valid) {
 #pragma unroll
           for (int j = 0; j < COLS; j++) {
-            const uint32_t n = nt * E::N + (E::ALT ? 0u : h * 32u) + j;
+            const uint32_t n = nt * E::N + (E::ALT ? 0u : h * (uint32_t)COLS) + j;
             if (n < g.n_valid && sum[j] != 0.0) atomicAdd(g.out + (size_t)n * g.ldo + m, sum[j] * scale);
           }
         }
 #pragma unroll
         for (int j = 0; j < COLS; j++) sum[j] = 0.0;
       }
+    }
+  }
+  if (GEN && warp >= 10) {
+    // sinc-digit producers: thread t makes q row t % 128, bins 32 (t / 128) .. +31 of every A tile of
+    // this CTA's units (SincRun: the same digits as the HBM planes)
+    const uint32_t t = (uint32_t)(warp - 10) * 32u + lane, row = t & 127u, half = t >> 7;
+    uint8_t *gsm = smem_raw + (base - smem_u32(smem_raw));
+    uint32_t cur_mt = 0xffffffffu;
+    double qm = 0.0, sd = 0.0, cd = 1.0;
+    unsigned long long i = 0;
+    for (unsigned long long u = u0; u < u1; ++u, ++i) {
+      const uint32_t s = (uint32_t)(i % XSTAGES), k = (uint32_t)(i / XSTAGES);
+      if (k > 0 && !mbar_wait(empty0 + 8 * s, (k - 1) & 1u, abort, g.wait_ns)) {
+        abort_sh = 1;
+        atomicOr(g.err, 1);
+        break;
+      }
+      const uint32_t kt = (uint32_t)(u % KT), mt = (uint32_t)((u / KT) % g.MT);
+      if (mt != cur_mt) {  // rows past the mesh have q = 0: zero digits
+        const uint32_t m = mt * XM + row;
+        qm = m < g.m_valid ? g.qv[m] : 0.0;
+        sincos(qm * g.bin, &sd, &cd);
+        cur_mt = mt;
+      }
+      SincRun run;
+      run.init(qm, g.bin, kt * XK + 32u * half, sd, cd);
+      uint8_t *st = gsm + s * E::STAGE;
+#pragma unroll 1
+      for (uint32_t c = 0; c < 4; c++) {
+        uint4 w[NDS];
+        run.chunk(c, w);
+        const uint32_t off = chunk_offset(row, 4u * half + c);
+#pragma unroll
+        for (int d = 0; d < NDS; d++) *(uint4 *)(st + d * XA + off) = w[d];
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes -> tensor-core reads
+      mbar_arrive(full0 + 8 * s);
     }
   }
   tc_fence_before();
@@ -294,41 +452,24 @@ __device__ __forceinline__ uint4 pack8(const float *v) {
   return *(const uint4 *)b;
 }
 
-// One CTA of 128 threads per (mt, kt) tile; a thread makes the 64 k of one row.  sin(x_k) comes from
-// one FP64 sincos at the row's first bin and the rotation by delta = q * bin (4 FMAs per bin; the
-// drift over 64 bins is ~1e-14, below the 1e-12 digit residual).
-__global__ void pack_sinc_digits_kernel(const double *__restrict__ q, uint32_t nq, double bin, uint32_t nh, uint32_t KT,
+// The sinc digits as planes in HBM, for a q mesh used again (streamed by the copy warp instead of made
+// on chip; SincRun makes the same digits).  One CTA of 256 threads per (mt, kt) tile: thread t makes
+// row t % 128, bins 32 (t / 128) .. +31.
+__global__ void pack_sinc_digits_kernel(const double *__restrict__ q, uint32_t nq, double bin, uint32_t KT,
                                         uint8_t *__restrict__ A, size_t a_plane) {
   const uint32_t tile = blockIdx.x, mt = tile / KT, kt = tile % KT;
-  const uint32_t row = threadIdx.x, m = mt * XM + row, kbase = kt * XK;
+  const uint32_t row = threadIdx.x & 127u, half = threadIdx.x >> 7, m = mt * XM + row;
   const double qm = m < nq ? q[m] : 0.0;
-  double s, c, sd, cd;
-  sincos(((kbase + 0.5) * bin) * qm, &s, &c);
-  sincos(bin * qm, &sd, &cd);
-  for (uint32_t ch = 0; ch < XK / 8; ch++) {
-    float dig[NDS][8];
+  double sd, cd;
+  sincos(qm * bin, &sd, &cd);
+  SincRun run;
+  run.init(qm, bin, kt * XK + 32u * half, sd, cd);
+  for (uint32_t c = 0; c < 4; c++) {
+    uint4 w[NDS];
+    run.chunk(c, w);
+    const size_t off = (size_t)tile * XA + chunk_offset(row, 4u * half + c);
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-      const uint32_t k = kbase + ch * 8 + i;
-      double v = 0.0;
-      if (m < nq && k < nh) {
-        const double x = ((k + 0.5) * bin) * qm;  // qrij = rij * q[iq] (CalcFunctions.cpp:858-861)
-        v = s / (x + 0.00000001);
-      }
-      double r = v * 128.0;
-#pragma unroll
-      for (int d = 0; d < NDS; d++) {
-        const double di = rint(r);
-        dig[d][i] = (float)di;
-        r = (r - di) * 256.0;
-      }
-      const double s1 = __fma_rn(s, cd, c * sd), c1 = __fma_rn(c, cd, -(s * sd));
-      s = s1;
-      c = c1;
-    }
-    const size_t off = (size_t)tile * XA + chunk_offset(row, ch);
-#pragma unroll
-    for (int d = 0; d < NDS; d++) *(uint4 *)(A + d * a_plane + off) = pack8(dig[d]);
+    for (int d = 0; d < NDS; d++) *(uint4 *)(A + d * a_plane + off) = w[d];
   }
 }
 
@@ -369,7 +510,7 @@ __global__ void max_count_kernel(const unsigned long long *__restrict__ hist, ui
 
 // Launches the digit GEMM of scheme E; grid 0: one CTA per SM (stream-K over all units), otherwise the
 // given number of CTAs.
-template <class E>
+template <class E, bool GEN>
 int launch_digit_gemm(xns_ctx *ctx, const XArgs &g0, unsigned grid) {
   XArgs g = g0;
   g.wait_ns = ctx->inject_stall_ns ? ctx->inject_stall_ns : WAIT_LIMIT_NS;
@@ -377,12 +518,12 @@ int launch_digit_gemm(xns_ctx *ctx, const XArgs &g0, unsigned grid) {
   ctx->inject_stall_ns = 0;  // one call only
   static bool attr_set[XNS_MAX_DEVICES] = {};  // the attribute is per device; set once on each
   if (ctx->device < 0 || ctx->device >= XNS_MAX_DEVICES || !attr_set[ctx->device]) {
-    XNS_CUDA(ctx, cudaFuncSetAttribute(sinc_exact_kernel<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, E::SMEM));
+    XNS_CUDA(ctx, cudaFuncSetAttribute(sinc_exact_kernel<E, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, E::SMEM));
     if (ctx->device >= 0 && ctx->device < XNS_MAX_DEVICES) attr_set[ctx->device] = true;
   }
   const unsigned long long units = (unsigned long long)g.NT * g.MT * g.KT;
   if (!grid) grid = (unsigned)std::min<unsigned long long>((unsigned long long)ctx->num_sms, units);
-  sinc_exact_kernel<E><<<grid, XTHREADS, E::SMEM, ctx->stream>>>(g);
+  sinc_exact_kernel<E, GEN><<<grid, GEN ? XTHREADS_GEN : XTHREADS, E::SMEM, ctx->stream>>>(g);
   XNS_LAUNCHED(ctx);
   return XNS_OK;
 }
@@ -393,10 +534,13 @@ int enqueue_exact(xns_ctx *ctx, const ExactLaunch &X) {
                                                                          X.b_plane, X.flags + 1);
   XNS_LAUNCHED(ctx);
   XArgs g{};
-  g.A = X.A;
+  g.A = X.A;  // null: made on chip
   g.B = X.B;
   g.a_plane = X.a_plane;
   g.b_plane = X.b_plane;
+  g.qv = X.qv;
+  g.bin = X.bin;
+  g.nh = X.nh;
   g.MT = X.MT;
   g.NT = X.NT;
   g.KT = X.KT;
@@ -407,7 +551,7 @@ int enqueue_exact(xns_ctx *ctx, const ExactLaunch &X) {
   g.err = X.flags;
   // level l holds 256^(NH-1-l)/128; the Horner sum weights it 256^(NL-1-l): one unit is 256^-(NDS-1)/128
   g.scale = ldexp(1.0, -8 * (NDS - 1)) / 128.0;
-  return launch_digit_gemm<SincScheme<NH, N>>(ctx, g, 0);
+  return X.A ? launch_digit_gemm<SincScheme<NH, N>, false>(ctx, g, 0) : launch_digit_gemm<SincScheme<NH, N>, true>(ctx, g, 0);
 }
 
 template <int NH>
@@ -508,7 +652,8 @@ __global__ void plane_intensity_kernel(const double *__restrict__ Ar, const doub
 }  // namespace
 
 int xns_tc_exact_plan(xns_ctx *ctx, const unsigned long long *d_hist, uint32_t ncols, uint32_t nh, size_t ldh, double bin,
-                      const double *q, uint32_t nq, unsigned long long max_count, double *d_G, ExactLaunch *X) {
+                      const double *q, uint32_t nq, unsigned long long max_count, double *d_G, ExactLaunch *X,
+                      bool planes) {
   *X = ExactLaunch();
   if (!ncols || !nq) return XNS_OK;
   if (max_count >> 32) return xns_fail(ctx, XNS_ERR_LIMIT, "exact transform: a bin count reaches 2^32");
@@ -528,24 +673,49 @@ int xns_tc_exact_plan(xns_ctx *ctx, const unsigned long long *d_hist, uint32_t n
   void *flags;
   if ((st = xns_scratch(ctx, SLOT_FLAGS, 64, &flags))) return st;
   X->flags = (int *)flags;
-  // sinc digits: rebuilt only when the q mesh, the bin width or the K extent change
-  X->a_plane = (size_t)X->MT * X->KT * XA;
-  void *A;
-  const bool same = ctx->x_bin == bin && ctx->x_kt == X->KT && ctx->x_q.size() == nq &&
-                    std::equal(q, q + nq, ctx->x_q.begin()) && ctx->slot_size[SLOT_X_A] >= NDS * X->a_plane;
-  if ((st = xns_scratch(ctx, SLOT_X_A, NDS * X->a_plane, &A))) return st;
-  if (!same) {
-    void *dq;
-    if ((st = xns_scratch(ctx, SLOT_QMESH, sizeof(double) * nq, &dq))) return st;
-    XNS_CUDA(ctx, cudaMemcpyAsync(dq, q, sizeof(double) * nq, cudaMemcpyHostToDevice, ctx->stream));
-    pack_sinc_digits_kernel<<<X->MT * X->KT, XM, 0, ctx->stream>>>((const double *)dq, nq, bin, nh, X->KT, (uint8_t *)A,
-                                                                    X->a_plane);
-    XNS_LAUNCHED(ctx);
-    ctx->x_q.assign(q, q + nq);
-    ctx->x_bin = bin;
-    ctx->x_kt = X->KT;
+  // the q mesh on the device (the sinc digits are made on chip from it)
+  void *dq;
+  if ((st = xns_scratch(ctx, SLOT_X_Q, sizeof(double) * nq, &dq))) return st;
+  XNS_CUDA(ctx, cudaMemcpyAsync(dq, q, sizeof(double) * nq, cudaMemcpyHostToDevice, ctx->stream));
+  X->qv = (const double *)dq;
+  X->bin = bin;
+  // A mesh seen for the first time gets its sinc digits made on chip (4.5 ms at 4096 q x 2.9e5 bins,
+  // no HBM planes); a mesh used again (or when the caller asks, as a batch replayed from a graph does)
+  // gets them as planes in HBM, made once (11.9 GB, 12 ms there) and streamed at copy bandwidth on every
+  // call (2.4 ms).  A memory limit that the planes would exceed keeps the digits on chip.
+  const size_t a_plane = (size_t)X->MT * X->KT * XA;
+  auto same_mesh = [&](const std::vector<double> &mq, double mbin, uint32_t mkt) {
+    return mbin == bin && mkt == X->KT && mq.size() == nq && std::equal(q, q + nq, mq.begin());
+  };
+  const bool cached = same_mesh(ctx->x_q, ctx->x_bin, ctx->x_kt) && ctx->slot_size[SLOT_X_A] >= NDS * a_plane;
+  bool want = cached || planes || same_mesh(ctx->x_seen_q, ctx->x_seen_bin, ctx->x_seen_kt);
+  if (want && !cached && ctx->mem_limit) {
+    size_t others = 0;
+    for (int k = 0; k < SLOT_COUNT; k++)
+      if (k != SLOT_X_A) others += ctx->slot_size[k];
+    want = others + NDS * a_plane <= ctx->mem_limit;
   }
-  X->A = (const uint8_t *)A;
+  ctx->x_seen_q.assign(q, q + nq);
+  ctx->x_seen_bin = bin;
+  ctx->x_seen_kt = X->KT;
+  void *A = nullptr;
+  if (want && (st = xns_scratch(ctx, SLOT_X_A, NDS * a_plane, &A))) {
+    if (st != XNS_ERR_NOMEM) return st;
+    want = false;  // no room for the planes: the digits stay on chip
+    ctx->err.clear();
+  }
+  if (want) {
+    if (!cached) {
+      pack_sinc_digits_kernel<<<X->MT * X->KT, 2 * XM, 0, ctx->stream>>>((const double *)dq, nq, bin, X->KT,
+                                                                          (uint8_t *)A, a_plane);
+      XNS_LAUNCHED(ctx);
+      ctx->x_q.assign(q, q + nq);
+      ctx->x_bin = bin;
+      ctx->x_kt = X->KT;
+    }
+    X->A = (const uint8_t *)A;
+    X->a_plane = a_plane;
+  }
   X->b_plane = (size_t)X->NT * X->KT * X->ntile * XK * 2;
   void *B;
   if ((st = xns_scratch(ctx, SLOT_TC_B, X->digits * X->b_plane, &B))) return st;
@@ -657,8 +827,8 @@ extern "C" int xns_calc_amp_plane(xns_ctx *ctx, const double *const *xyz_el, con
     const size_t a_plane = (size_t)MT * KT * XA, b_plane = (size_t)NT * KT * PXB;
     void *A, *B;
     if ((st = xns_scratch(ctx, SLOT_X_A, PD * a_plane, &A))) return st;
+    ctx->x_q.clear();  // the sinc-digit planes of the histogram transform share SLOT_X_A
     if ((st = xns_scratch(ctx, SLOT_TC_B, PD * b_plane, &B))) return st;
-    ctx->x_q.clear();  // the sinc-digit cache of the histogram transform shares SLOT_X_A
     const double *xe = dc.x + dc.off_el[e], *ye = dc.y + dc.off_el[e];
     plane_pack_a_kernel<<<MT * KT, XK, 0, ctx->stream>>>(xe, n, qx0, dqx, nqx, KT, (uint8_t *)A, a_plane);
     XNS_LAUNCHED(ctx);
@@ -695,7 +865,7 @@ extern "C" int xns_calc_amp_plane(xns_ctx *ctx, const double *const *xyz_el, con
       }
     }
     g.ksplit = ks;
-    if ((st = launch_digit_gemm<PlaneScheme>(ctx, g, ks * MT * NT))) return st;
+    if ((st = launch_digit_gemm<PlaneScheme, false>(ctx, g, ks * MT * NT))) return st;
     plane_accum_kernel<<<(unsigned)((npix + 255) / 256), 256, 0, ctx->stream>>>(
         (const double *)vC, nqx, nqy, qx0, dqx, qy0, dqy, vcoef ? (const double *)vcoef + 9 * e : nullptr,
         vcoef ? 0.0 : sl[e], Ar, Ai);

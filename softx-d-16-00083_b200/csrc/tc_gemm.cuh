@@ -61,22 +61,28 @@ int xns_tc_sinc_gemm(xns_ctx *ctx, const xns_tc::GemmArgs &g, int grid);
 // context for the last q mesh / bin / extent) and multiplies.  d_G receives ncols x nq FP64.
 int xns_tc_hist_transform(xns_ctx *ctx, const unsigned long long *d_hist, uint32_t ncols, uint32_t nh, size_t ldh,
                           double bin, const double *q, uint32_t nq, double *d_G);
-// The exact transform in steps: the plan (sinc digit planes, count digits chosen from max_count;
-// may synchronise), the launches (memsets and kernels only: can be captured in a CUDA graph), and the
-// check of its flags.  d_G: ncols x nq FP64.
+// The exact transform in steps: the plan (the q mesh on the device, sinc-digit planes for a mesh used
+// again, count digits chosen from max_count; may synchronise), the launches (memsets and kernels only:
+// can be captured in a CUDA graph), and the check of its flags.  d_G: ncols x nq FP64.
 struct ExactLaunch {
   const unsigned long long *hist = nullptr;
   uint32_t ncols = 0, nh = 0, nq = 0, MT = 0, NT = 0, KT = 0;
-  size_t ldh = 0, a_plane = 0, b_plane = 0;
+  size_t ldh = 0, b_plane = 0;
   int digits = 0;  // count digits: 2, 3 or 4 (counts below 2^16, 2^24, 2^32)
   uint32_t ntile = 0;  // columns per N tile: 16 or 32
-  const uint8_t *A = nullptr;
+  const double *qv = nullptr;  // the q mesh on the device (sinc digits made on chip) ...
+  double bin = 0;
+  const uint8_t *A = nullptr;  // ... or the sinc-digit planes in HBM (a mesh used again)
+  size_t a_plane = 0;
   uint8_t *B = nullptr;
   double *G = nullptr;
   int *flags = nullptr;
 };
+// planes: build the sinc-digit planes in HBM now (a plan whose launches are replayed) instead of on
+// the mesh's second use.
 int xns_tc_exact_plan(xns_ctx *ctx, const unsigned long long *d_hist, uint32_t ncols, uint32_t nh, size_t ldh, double bin,
-                      const double *q, uint32_t nq, unsigned long long max_count, double *d_G, ExactLaunch *X);
+                      const double *q, uint32_t nq, unsigned long long max_count, double *d_G, ExactLaunch *X,
+                      bool planes = false);
 int xns_tc_exact_enqueue(xns_ctx *ctx, const ExactLaunch &X);
 int xns_tc_exact_check(xns_ctx *ctx, const ExactLaunch &X);
 // Largest count of ncols histogram columns (synchronises).

@@ -37,20 +37,34 @@ __device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// As mbar_test, but a thread whose phase is not complete may be suspended in hardware for up to
+// hint_ns (woken early when the phase completes) instead of returning at once: waiting warps then
+// take no issue slots from the warps doing the work.
+__device__ __forceinline__ bool mbar_test_sleep(uint32_t bar, uint32_t parity, uint32_t hint_ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+constexpr uint32_t WAIT_HINT_NS = 20000;
 // Waits for the phase of the given parity to complete.  Returns false when *abort is raised (abort
-// may be null) or limit_ns of wall-clock time pass first.
+// may be null) or limit_ns of wall-clock time pass first; both are checked after every try (at most
+// WAIT_HINT_NS apart).
 __device__ inline bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort, unsigned long long limit_ns) {
   unsigned long long t0 = 0;
   for (uint32_t it = 0;; ++it) {
-    if (mbar_test(bar, parity)) return true;
-    if ((it & 31u) == 0) {
-      if (abort && *abort) return false;
-      const unsigned long long t = globaltimer();
-      if (it == 0)
-        t0 = t;
-      else if (t - t0 > limit_ns)
-        return false;
-    }
+    if (mbar_test_sleep(bar, parity, WAIT_HINT_NS)) return true;
+    if (abort && *abort) return false;
+    const unsigned long long t = globaltimer();
+    if (it == 0)
+      t0 = t;
+    else if (t - t0 > limit_ns)
+      return false;
   }
 }
 
@@ -92,6 +106,16 @@ __device__ __forceinline__ void tc_ld16_raw(uint32_t taddr, uint32_t *r) {
       "tcgen05.wait::ld.sync.aligned;"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
         "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+}
+
+// 32 lanes x 8 consecutive 32-bit accumulator columns, raw bits (load and wait in one statement).
+__device__ __forceinline__ void tc_ld8_raw(uint32_t taddr, uint32_t *r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
       : "r"(taddr)
       : "memory");
 }

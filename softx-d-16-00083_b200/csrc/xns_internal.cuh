@@ -33,7 +33,8 @@ enum ScratchSlot {
   SLOT_TC_A,            // split-BF16 sinc matrix (hi and lo planes, tensor-core tile order)
   SLOT_TC_B,            // split-BF16 histogram columns (hi and lo planes)
   SLOT_TC_OUT,          // FP64 sinc-transform output (columns x q)
-  SLOT_X_A,             // integer-digit planes of the sinc matrix (exact transform)
+  SLOT_X_A,             // integer-digit planes: the sinc matrix (a q mesh used again) or the 2D plane's A
+  SLOT_X_Q,             // the exact transform's q mesh
   SLOT_HFLAGS,          // histogram: out-of-range count and run queue
   SLOT_BATCH,           // batched ensemble: coordinates, schedules and per-structure tables
   SLOT_BATCH_HIST,      // batched ensemble: histograms
@@ -68,10 +69,11 @@ struct xns_ctx {
   std::vector<double> tc_q;
   double tc_bin = 0;
   uint32_t tc_kt = 0;
-  // the same for the integer-digit sinc planes in SLOT_X_A
-  std::vector<double> x_q;
-  double x_bin = 0;
-  uint32_t x_kt = 0;
+  // the integer-digit sinc planes in SLOT_X_A were made for this q mesh, bin width and K extent; the
+  // last mesh the exact transform saw (a second use builds the planes)
+  std::vector<double> x_q, x_seen_q;
+  double x_bin = 0, x_seen_bin = 0;
+  uint32_t x_kt = 0, x_seen_kt = 0;
   // private batch reused by the one-shot batched entry point (batch.cu)
   struct xns_batch *batch_cache = nullptr;
   // atoms per element of the last structure build (SLOT_ATOMS)

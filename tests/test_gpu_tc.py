@@ -69,6 +69,27 @@ def test_transform_cache_follows_mesh(gpu_ctx, scheme, tol):
     assert col_err(gpu_ctx.hist_transform(H, 0.004, q, scheme), G64) < tol
 
 
+def test_exact_digits_on_chip_then_planes():
+    """The exact transform makes a new q mesh's sinc digits on chip; the mesh's second use builds the
+    digit planes in HBM and later uses stream them.  Both ways make the same digits (one generator), so
+    the three calls agree to the order of the cross-CTA FP64 atomics, and match FP64.  A fresh
+    context, so that no earlier test has seen the mesh."""
+    import xns_b200
+    ctx = xns_b200.Context(0)
+    try:
+        rng = np.random.default_rng(12)
+        H = rng.integers(0, 3000, size=(3, 5000)).astype(np.uint64)
+        q = synth.q_mesh(0.1, 25.0, 700)
+        G64 = H.astype(np.float64) @ sinc_matrix(q, 5000, 0.002).T
+        Gs = [ctx.hist_transform(H, 0.002, q, "exact") for _ in range(3)]
+        for G in Gs:
+            assert col_err(G, G64) < 1e-8
+        assert np.allclose(Gs[0], Gs[1], rtol=1e-12, atol=0)
+        assert np.allclose(Gs[1], Gs[2], rtol=1e-12, atol=0)
+    finally:
+        ctx.close()
+
+
 def iq_from_g(G, n_el, w):
     """I(q) from the per-pair transforms (neutron weights): [sum N_e w_e^2 + 2 sum w_a w_b G_ab] / N."""
     nel = len(n_el)
