@@ -67,8 +67,8 @@ __global__ void sinc_eps_kernel(const double *__restrict__ H, uint32_t nb, doubl
 }
 
 size_t sinc_smem_bytes(int M, int lanes_per_slot, size_t stage_bytes) {
-  const int share = lanes_per_slot < 32 ? 32 / lanes_per_slot : 1;
-  return sizeof(double) * M * (SE_THREADS / share) + sizeof(PairRec) * SE_TILE + stage_bytes;
+  (void)lanes_per_slot;  // one FP64 column per thread whatever the slot width
+  return sizeof(double) * M * SE_THREADS + sizeof(PairRec) * SE_TILE + stage_bytes;
 }
 
 int sinc_upload_q(xns_ctx *ctx, const double *q, uint32_t nq, const double **d_q) {

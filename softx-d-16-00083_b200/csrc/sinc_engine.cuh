@@ -21,10 +21,9 @@
 // next eight records' seeds are computed in the same straight-line block as this recurrence, so that
 // their latency overlaps its steps.
 //
-// Accumulation: FP32 sums over at most SE_FP32_GROUPS groups of four records, then FP64 totals in
-// shared memory, one column per chunk and warp (the lanes of a warp that own the same chunk add their
-// FP32 sums by shuffle first), then FP64 per-CTA partial sums reduced in the epilogue.  1/q_k is
-// applied in the epilogue.  A mesh that is not uniform takes an accurate sine per term (DIRECT).
+// Accumulation: FP32 sums over at most SE_FP32_GROUPS groups of eight records, then per-thread FP64
+// totals in shared memory, then FP64 per-CTA partial sums reduced in the epilogue.  1/q_k is applied
+// in the epilogue.  A mesh that is not uniform takes an accurate sine per term (DIRECT).
 //
 // The +1e-8.  sin(q r)/(q r + 1e-8) = sin(q r)/(q r) - 1e-8 sin(q r)/(q r)^2 + O(1e-16): the second
 // term is a relative 1e-8/(q r) of each term, below FP32 resolution, but at the deepest minima of a
@@ -48,7 +47,7 @@ constexpr int SE_THREADS = 128;
 // CTAs per SM the register allocation is sized for (168 registers a thread).
 constexpr int SE_MIN_CTAS = 3;
 // Records per tile.  With 16 lanes per slot (1024 q) a lane takes 6 groups of eight records per tile;
-// the FP64 totals take 32 KB, the records 9 KB: three CTAs (12 warps) share an SM.
+// the FP64 totals take 64 KB, the records 9 KB: three CTAs (12 warps) share an SM.
 constexpr int SE_TILE = 384;
 // q values per lane: M_UNIFORM for the recurrence (a seed costs ~30 instructions, the recurrence
 // 1.6 issue slots per term), M_DIRECT for the per-term sine of a non-uniform mesh.
@@ -56,9 +55,8 @@ constexpr int SE_M_UNIFORM = 64;
 constexpr int SE_M_DIRECT = 16;
 // Records a lane runs side by side (four packed pairs).
 constexpr int SE_GROUP = 8;
-// Record groups a lane sums in FP32 before the sums go to FP64 (at most 96 records, with the pair of
-// lanes that share a chunk at 1024 q; the error of these FP32 sums is the largest term of the error
-// budget at the deepest minima of a pattern).
+// Record groups a lane sums in FP32 before the sums go to FP64 (48 records; the error of these FP32
+// sums is the largest term of the error budget at the deepest minima of a pattern).
 constexpr int SE_FP32_GROUPS = 6;
 // The +1e-8 histogram: bins of at least EPS_BIN_MIN, at most EPS_NB_MAX of them.
 constexpr double EPS_BIN_MIN = 0.05;
@@ -107,29 +105,23 @@ __device__ __forceinline__ PairRec make_rec(const SincParams &p, uint32_t cls, d
   return rec;
 }
 
-// Shared memory: [M][ncol] FP64 totals, then SE_TILE records, then the Source's own staging area.
-// ncol = SE_THREADS / (lanes of a warp that own one chunk).
+// Shared memory: [M][SE_THREADS] FP64 totals (one column per thread), then SE_TILE records, then the
+// Source's own staging area.
 template <int M, bool DIRECT, class Src>
 __global__ void __launch_bounds__(SE_THREADS, SE_MIN_CTAS) sinc_tiles_kernel(SincParams p, Src src, int lanes_per_slot) {
   extern __shared__ double acc64[];
-  const int share = lanes_per_slot < 32 ? 32 / lanes_per_slot : 1;
-  const int ncol = SE_THREADS / share;
+  constexpr int ncol = SE_THREADS;
   PairRec *pr = reinterpret_cast<PairRec *>(acc64 + M * ncol);
   void *stage = reinterpret_cast<void *>(pr + SE_TILE);
 
-  const int tid = threadIdx.x, lane = tid & 31;
+  const int tid = threadIdx.x, col = tid;
   const int nslots = SE_THREADS / lanes_per_slot;
   const int slot = tid / lanes_per_slot;
   const uint32_t k0 = (uint32_t)(tid % lanes_per_slot) * M;
-  const bool active = k0 < p.nq;  // the same for all lanes of a warp that share a chunk
-  // the first lane of a warp with a given chunk keeps that chunk's FP64 column
-  const bool owner = share == 1 || lane < lanes_per_slot;
-  const int col = share == 1 ? tid : (tid >> 5) * lanes_per_slot + lane;
+  const bool active = k0 < p.nq;
   const double qk0 = p.q0 + (double)k0 * p.dq;
-  if (owner) {
 #pragma unroll
-    for (int k = 0; k < M; k++) acc64[k * ncol + col] = 0.0;
-  }
+  for (int k = 0; k < M; k++) acc64[k * ncol + col] = 0.0;
   double qd[DIRECT ? M : 1];
   if (DIRECT) {
 #pragma unroll
@@ -141,7 +133,7 @@ __global__ void __launch_bounds__(SE_THREADS, SE_MIN_CTAS) sinc_tiles_kernel(Sin
        w += (unsigned long long)p.nshard * gridDim.x) {
     const int c = (int)src.cls(w);
     if (c != cur) {  // flush the previous class's FP64 totals to this CTA's slice
-      if (cur >= 0 && active && owner) {
+      if (cur >= 0 && active) {
         double *dst = p.partial + ((size_t)blockIdx.x * p.ncls + cur) * p.nq + k0;
 #pragma unroll
         for (int k = 0; k < M; k++) {
@@ -163,7 +155,7 @@ __global__ void __launch_bounds__(SE_THREADS, SE_MIN_CTAS) sinc_tiles_kernel(Sin
 #pragma unroll
         for (int g = 0; g < 4; g++) R[g] = e + g * nslots < n ? pr[e + g * nslots] : null_rec();
         if (R[0].w == 0.f && R[1].w == 0.f && R[2].w == 0.f && R[3].w == 0.f) continue;
-        if (share == 1 && nblk == SE_FP32_GROUPS) {  // long tiles: FP32 sums stay short
+        if (nblk == SE_FP32_GROUPS) {  // FP32 sums stay short
 #pragma unroll
           for (int k = 0; k < M; k++) {
             acc64[k * ncol + col] += (double)blk[k];
@@ -202,7 +194,7 @@ __global__ void __launch_bounds__(SE_THREADS, SE_MIN_CTAS) sinc_tiles_kernel(Sin
       seeds(slot, s, d, lam);
       int nblk = 0;  // record groups in blk
       for (int e = slot; e < n; e += G * nslots) {
-        if (share == 1 && nblk == SE_FP32_GROUPS) {  // long tiles: FP32 sums stay short
+        if (nblk == SE_FP32_GROUPS) {  // FP32 sums stay short
 #pragma unroll
           for (int k = 0; k < M; k++) {
             acc64[k * ncol + col] += (double)blk[k];
@@ -236,22 +228,13 @@ __global__ void __launch_bounds__(SE_THREADS, SE_MIN_CTAS) sinc_tiles_kernel(Sin
         }
       }
     }
-    // end of the tile: every lane of the warp is here (the flush shuffles)
-    if (share > 1) {
-#pragma unroll
-      for (int k = 0; k < M; k++) {
-        float v = blk[k];
-        for (int off = 16; off >= lanes_per_slot; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-        blk[k] = v;
-      }
-    }
-    if (active && owner) {
+    if (active) {
 #pragma unroll
       for (int k = 0; k < M; k++) acc64[k * ncol + col] += (double)blk[k];
     }
     __syncthreads();
   }
-  if (cur >= 0 && active && owner) {
+  if (cur >= 0 && active) {
     double *dst = p.partial + ((size_t)blockIdx.x * p.ncls + cur) * p.nq + k0;
 #pragma unroll
     for (int k = 0; k < M; k++)
