@@ -22,7 +22,7 @@
 // Bin decision, per pair: an FP32 estimate of r/bin with a proven error bound (count_tile_pair_t: a
 // centred estimate for tile pairs far apart, whose error scales with the tile size; a direct one
 // otherwise), computed for two pairs at a time on packed f32x2 pairs.  Pairs whose estimate lies
-// within the bound of a bin edge (about 1.5 % of the benchmark's), near the last bin or outside the
+// within the bound of a bin edge (about 0.75 % of the benchmark's), near the last bin or outside the
 // window are queued per warp and binned exactly, 32 at a time, with FP64 in the reference's operation
 // order (hist_bin.cuh).  Atom order inside a cell and list order inside a bucket come from atomics,
 // but counts do not depend on either.
@@ -48,9 +48,9 @@ constexpr int HW_THREADS = 32 * HW_WARPS;
 constexpr uint32_t WIN_MAX = 45 * 1024 + 512;  // largest window (bins) that fits with the warp stages
 constexpr uint32_t BUCKET = 1024;    // distance bucket of the tile-pair sort, in bins
 constexpr int SCAN_THREADS = 1024;
-constexpr int QUEUE = 64;            // queue entries per warp: u16 (i/2) << 9 | lane << 4 | 4-bit pair mask
+constexpr int QUEUE = 64;            // queue entries per warp: u32 (i/4) << 13 | lane << 8 | 8-bit pair mask
 // per warp: FP64 I tile, FP32 I-tile offsets (+ P_i), the queue (bytes)
-constexpr int WARP_STAGE = 3 * TILE_MAX * 8 + 4 * TILE_MAX * 4 + QUEUE * 2;
+constexpr int WARP_STAGE = 3 * TILE_MAX * 8 + 4 * TILE_MAX * 4 + QUEUE * 4;
 
 struct Tile {
   uint32_t start, count, elem, pad;
@@ -419,11 +419,13 @@ __device__ __forceinline__ bool far_pair(const PairGeom &g) { return g.R0 >= 2.0
 
 // One warp counts the pairs of one tile pair: the I tile's FP64 coordinates and FP32 offsets are
 // staged in the warp's shared memory (stage: WARP_STAGE bytes), the J tile's sit in registers (atoms
-// lane and lane + 32), the warp walks i two rows at a time (four independent chains).  SAME (a tile
+// lane and lane + 32), the warp walks i four rows at a time (four independent chains of two packed
+// pairs each).  SAME (a tile
 // against itself) keeps only i < j.  Each pair gets an FP32 estimate of r/bin with a proven error
 // bound; pairs whose estimate lies within the bound of a bin edge, near or beyond the last bin, or
-// outside the CTA's window are appended to the warp's queue (ballot + popc: consecutive entries) and
-// binned exactly with FP64 from the coordinates (hist_bin.cuh), one entry per lane, whenever 32 wait.
+// outside the CTA's window are appended to the warp's queue (one entry per lane and step with an
+// 8-bit mask; ballot + popc: consecutive entries) and binned exactly with FP64 from the coordinates
+// (hist_bin.cuh), one entry per lane, whenever 32 wait.
 //
 // Direct estimate (SAME and close tile pairs; u = 2^-24): dh is D rounded to float, dl its low part;
 // the I offsets are (x_i - c_I)/bin and the J offsets (x_j - c_J)/bin - dl, rounded to float.  Each
@@ -434,47 +436,60 @@ __device__ __forceinline__ bool far_pair(const PairGeom &g) { return g.R0 >= 2.0
 // bins).  r + 1.5*2^23 rounds r to an integer in the low mantissa bits (r < 2^22), which gives
 // round(r) and d without a conversion.
 //
-// Centred estimate (far tile pairs): with a = (x_i - c_I)/bin, b = (x_j - c_J)/bin,
-//   r^2 = R0^2 + num,  num = P_i - Q_j - 2 a.b,  P_i = 2 D.a + |a|^2,  Q_j = 2 D.b - |b|^2,
-// and r = R0 + delta with delta = num / (R0 + r) exactly.  P_i and Q_j are formed in FP64 per tile pair
-// and rounded to float; per pair num = (P_i - Q_j) + a.(-2 b) in FP32, r' = d2 rsqrt(d2) with
-// d2 = num + R0^2 only for the denominator, and t = num rcp(r' + R0) + (R0 - floor(R0) - 0.5) in one
-// FMA, so that floor(r) = floor(R0) + round(t).  Its error (centred_margin) is K0 + K1 |delta| with K0
-// of order u rho and K1 of order 20 u: it grows with the tile size, not with r, and at 1e5-bin
-// distances leaves about a quarter of the direct estimate's near-edge pairs.
+// Centred estimate (far tile pairs): with a = (x_i - c_I)/bin, b = (x_j - c_J)/bin and the bin
+// midpoint R = floor(R0) + 0.5 nearest the centres' distance,
+//   r^2 = R^2 + num,  num = P_i - Q_j - 2 a.b,  P_i = 2 D.a + |a|^2 + (R0^2 - R^2),  Q_j = 2 D.b - |b|^2,
+// and t = r - R = r - floor(R0) - 0.5, so that floor(r) = floor(R0) + round(t).  P_i and Q_j are formed
+// in FP64 per tile pair and rounded to float; per pair num = (P_i - Q_j) + a.(-2 b) in FP32,
+// d2 = num + R^2, y = rsqrt(d2) and t0 = d2 y - R (one FMA: r to a few ulp, so t0 is within ~5u r of
+// t), then one Newton step on t^2 + 2 R t - num = 0 whose derivative 2 r is 2 / y:
+//   t = t0 + (num - t0 (t0 + 2 R)) y / 2   (a subtraction and two FMAs),
+// which leaves the error of t0 only squared.  Its error (centred_margin) is K0 + K1 |t - r + R| with K0
+// of order u rho and K1 about 4u: it grows with the tile size, not with r; one MUFU operation per pair.
 struct CentredConsts {
-  float R0sq, R0f, R0fr, K1, mc;  // fast iff |d| <= mc - K1 |t|
-  int R0i;
+  float R2, NR, N2R, K1, mc;  // R^2 rounded, -R, -2 R (both exact); fast iff |d| <= mc - K1 |t|
+  int R0i;                    // floor(R0)
+  double S;                   // R0^2 - R^2, added to every P_i
 };
-// The bound, for r >= R0/2 (far_pair); each line is one source of error (first order in u):
-//   num:   |num~ - num| <= u(|P| + |Q|) + 2u|num| + 14u rho_I rho_J, |P| <= 2 R0 rho_I + rho_I^2 (Q alike);
-//          divided by r + R0 >= 1.5 R0 this is A + 2u|delta|;
-//   d2:    relative error eps_d <= 5u + 4 dnum_max / R0^2 (R0^2 rounded, num's error, one add);
-//   r':    rsqrt.approx 4u + product u + eps_d / 2;  den = r' + R0: eps_den <= eps_r + 2u;
-//   t:     rcp.approx 2u, the FMA's rounding u|t| <= u|delta| + u/2;
-// so |t - (r - floor(R0) - 0.5)| <= K0 + (5u + eps_den) |delta| and |delta| <= |t| + 1.
+// The bound, for r >= R0 - rho_I - rho_J >= R0 / 2 (far_pair), u = 2^-24 the unit roundoff (each FP32
+// rounding at most u relative), t~ = r~ - R where r~^2 = R^2 + num~ (num~ the computed num):
+//   num:    |num~ - num| <= u(|P| + |Q|) + 2u|num| + 12u rho_I rho_J (P, Q and the difference rounded;
+//           the dot product's roundings, |a.b| <= rho_I rho_J; the last add), with |P| <= 2 R0 rho_I +
+//           rho_I^2 + R0 + 1/4 and |Q| <= 2 R0 rho_J + rho_J^2;  |t~ - t| = |num~ - num| / (r + r~), and
+//           r + r~ >= 1.998 (R0 - rho_I - rho_J);  2u|num| / (r + r~) = 2u |t| (r + R) / (r + r~) <= 2uF|t|
+//           with F = 1/2 + (R0 + 1/2) / (2 (R0 - rho_I - rho_J)) (at most 3/2);
+//   Newton: t0 - t~ <= r (rsqrt 2.14u + d2's 5.1u / 2) + u|t0| <= 5.7u r and y within 4.7u of 1 / r~, so
+//           the step leaves (t0 - t~)(4.7u + (t0 - t~) / 2r) <= 44 u^2 r;  rounding t0 + 2R costs
+//           u |t0| (r + R) y / 2 <= uF|t|, the residual's rounding u^2 r more, the final FMA u|t|;
+// so |t - (r - R)| <= K0 + (3F + 1) u |t - r + R| + O(u^2), K0 = the absolute part of num's bound
+// divided by 1.998 (R0 - rho_I - rho_J), plus 50 u^2 (R0 + rho_I + rho_J).
 // The constants are bounds: evaluated in FP32 and enlarged by 2 % (more than FP32 rounding can take away).
 __device__ __forceinline__ CentredConsts centred_consts(const PairGeom &g) {
   const float u = 5.9604645e-08f;  // 2^-24
-  const float R0 = (float)g.R0, iR0 = 1.0f / R0;
-  const float rs = g.rhoI + g.rhoJ, rr = g.rhoI * g.rhoI + g.rhoJ * g.rhoJ + 14.0f * g.rhoI * g.rhoJ;
-  const float A = u * (4.0f / 3.0f * rs + rr * iR0 * (1.0f / 1.5f));
-  const float num_max = 2.0f * R0 * rs + rs * rs;
-  const float dnum_max = u * (2.0f * R0 * rs + rr) + 2.0f * u * num_max;
-  const float eps_d = 5.0f * u + 4.0f * dnum_max * iR0 * iR0;
-  const float eps_den = 0.5f * eps_d + 7.0f * u;
-  const float K1 = (5.0f * u + eps_den) * 1.02f;
-  // u/2 + rounding of R0fr; 1e-9 for FP64 errors of D, a, P, Q and the reference's own rounding
-  const float K0 = A * 1.02f + u + 1e-9f + R0 * 9.094947e-13f;  // 2^-40 R0
+  const float R0 = (float)g.R0;
+  const float rs = g.rhoI + g.rhoJ, rr = 12.0f * g.rhoI * g.rhoJ;
+  const float PQ = 2.0f * R0 * rs + g.rhoI * g.rhoI + g.rhoJ * g.rhoJ + R0 + 0.25f;
+  const float Lr = 1.998f * (R0 - rs) * 0.999999f;
+  const float F = (0.5f + (R0 + 0.5f) / (2.0f * (R0 - rs) * 0.999999f)) * 1.000001f;
+  const float K1 = (3.0f * F + 1.0f) * u * 1.02f;
+  // 1e-9 for FP64 errors of D, a, P, Q and the reference's own rounding
+  const float K0 = u * (PQ + rr) / Lr * 1.02f + 50.0f * u * u * (R0 + rs) * 1.02f + 1e-9f + R0 * 9.094947e-13f;
   CentredConsts c;
-  const double fl = floor(g.R0);
-  c.R0sq = (float)(g.R0 * g.R0);
-  c.R0f = R0;
-  c.R0fr = (float)(g.R0 - fl - 0.5);
+  const double fl = floor(g.R0), R = fl + 0.5;
+  c.R2 = (float)(R * R);
+  c.NR = (float)-R;
+  c.N2R = (float)(-2.0 * R);
+  c.S = (g.R0 - R) * (g.R0 + R);
   c.R0i = (int)fl;
   c.K1 = K1;
   c.mc = 0.5f - K0 - K1 - 1e-6f;
   return c;
+}
+
+// The correctly rounded fallback of the exact path, out of line: about one near pair in 2,000 needs it,
+// and inlined its FP64 divide and square root cost the counting loop registers and instruction cache.
+__device__ __noinline__ uint32_t ref_bin_slow(double d2, double bin, double inv_bin, double margin, uint32_t nhist) {
+  return ref_bin(d2, bin, inv_bin, margin, nhist);
 }
 
 template <bool SAME, bool WINDOW, bool CENTRED>
@@ -486,7 +501,7 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
   // that two 16-byte loads give both rows' values as packed pairs
   float *wIf = reinterpret_cast<float *>(wI + 3 * TILE_MAX);
   float4 *wI4 = reinterpret_cast<float4 *>(wIf);
-  uint16_t *queue = reinterpret_cast<uint16_t *>(wI4 + TILE_MAX);
+  uint32_t *queue = reinterpret_cast<uint32_t *>(wI4 + TILE_MAX);
   const uint32_t lane = threadIdx.x & 31;
   const Tile TI = p.tiles[tp.I], TJ = p.tiles[tp.J];
   const uint32_t ni = TI.count, nj = TJ.count;
@@ -526,7 +541,7 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
     wI[2 * TILE_MAX + i] = z;
     const double ax = (x - cI[0]) * ib, ay = (y - cI[1]) * ib, az = (z - cI[2]) * ib;
     float P = 0.f;
-    if (CENTRED) P = (float)(2.0 * (g.D[0] * ax + g.D[1] * ay + g.D[2] * az) + (ax * ax + ay * ay + az * az));
+    if (CENTRED) P = (float)(2.0 * (g.D[0] * ax + g.D[1] * ay + g.D[2] * az) + (ax * ax + ay * ay + az * az) + cc.S);
     float *row = wIf + (i >> 1) * 8 + (i & 1);
     row[0] = (float)ax;
     row[2] = (float)ay;
@@ -574,7 +589,7 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
   using xns_f2::splat;
   const xns_f2::f2 XJ0 = splat(xj0), YJ0 = splat(yj0), ZJ0 = splat(zj0), XJ1 = splat(xj1), YJ1 = splat(yj1),
                    ZJ1 = splat(zj1), MAGIC2 = splat(MAGIC);
-  xns_f2::f2 QJ0 = 0, QJ1 = 0, R0SQ2 = 0, R0F2 = 0, R0FR2 = 0, NK1_2 = 0, MC2 = 0;
+  xns_f2::f2 QJ0 = 0, QJ1 = 0, R2_2 = 0, NR2 = 0, N2R2 = 0, NK1_2 = 0, MC2 = 0;
   xns_f2::f2 DH0 = 0, DH1 = 0, DH2 = 0, MR2 = 0, M02 = 0;
   const xns_f2::f2 HALF2 = splat(0.5f), SIGN2 = 0x8000000080000000ull;  // SIGN2: flips both signs
   if (!CENTRED) {
@@ -587,9 +602,9 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
   if (CENTRED) {
     QJ0 = splat(qj0);
     QJ1 = splat(qj1);
-    R0SQ2 = splat(cc.R0sq);
-    R0F2 = splat(cc.R0f);
-    R0FR2 = splat(cc.R0fr);
+    R2_2 = splat(cc.R2);
+    NR2 = splat(cc.NR);
+    N2R2 = splat(cc.N2R);
     NK1_2 = splat(-cc.K1);
     MC2 = splat(cc.mc);
   }
@@ -599,13 +614,15 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
   uint32_t qn = 0, qd = 0;  // entries queued / binned (warp-uniform)
   unsigned bad = 0;
   // Lane l bins the pairs of queued entry qd + l exactly (l < n), then n entries are done.  An entry is
-  // one lane's near pairs of one row pair: rows i, i + 1 against that lane's J atoms (lane, lane + 32),
+  // one lane's near pairs of one step: rows i .. i + 3 against that lane's J atoms (lane, lane + 32),
   // bit k of the mask standing for row i + k / 2 and J atom lane + 32 (k & 1).  The warp drains full
-  // batches of 32 while it counts, so every lane has an entry.
+  // batches of 32 while it counts, so every lane has an entry.  The entries were stored by other lanes:
+  // __syncwarp orders those stores before the loads.
   auto drain = [&](uint32_t n) {
+    __syncwarp();
     const uint32_t e = lane < n ? queue[(qd + lane) & (QUEUE - 1)] : 0u;
-    const uint32_t src = (e >> 4) & 31u, row = (e >> 9) << 1;
-    uint32_t pm = e & 15u;
+    const uint32_t src = (e >> 8) & 31u, row = (e >> 13) << 2;
+    uint32_t pm = e & 255u;
     // the J atoms sit in lane src
     const double xb0 = __shfl_sync(0xffffffffu, Xj0, src), xb1 = __shfl_sync(0xffffffffu, Xj1, src);
     const double yb0 = __shfl_sync(0xffffffffu, Yj0, src), yb1 = __shfl_sync(0xffffffffu, Yj1, src);
@@ -618,7 +635,7 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
       const double d2 = ref_dist2(wI[a], wI[TILE_MAX + a], wI[2 * TILE_MAX + a], hi ? xb1 : xb0, hi ? yb1 : yb0,
                                   hi ? zb1 : zb0);
       uint32_t k;
-      if (!ref_bin_fast(d2, p.inv_bin, p.margin, nhm1, &k)) k = ref_bin(d2, p.bin, p.inv_bin, p.margin, p.nhist);
+      if (!ref_bin_fast(d2, p.inv_bin, p.margin, nhm1, &k)) k = ref_bin_slow(d2, p.bin, p.inv_bin, p.margin, p.nhist);
       if (k >= p.nhist) {
         bad++;
       } else if (WINDOW && k - base < W) {
@@ -668,14 +685,14 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
   {                                                                                         \
     using namespace xns_f2;                                                                 \
     const f2 num = add(sub(RW, QJ), xns_f2::fma(RX, XJ, xns_f2::fma(RY, YJ, mul(RZ, ZJ)))); \
-    const f2 d2 = add(num, R0SQ2);                                                          \
-    float y0, y1, c0_, c1_;                                                                 \
+    const f2 d2 = add(num, R2_2);                                                           \
+    float y0, y1;                                                                           \
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y0) : "f"(lo(d2)));                           \
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y1) : "f"(hi(d2)));                           \
-    const f2 den = xns_f2::fma(d2, pack(y0, y1), R0F2);                                     \
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(c0_) : "f"(lo(den)));                           \
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(c1_) : "f"(hi(den)));                           \
-    const f2 t = xns_f2::fma(num, pack(c0_, c1_), R0FR2); /* r - floor(R0) - 0.5 */         \
+    const f2 y = pack(y0, y1);                                                              \
+    const f2 t0 = xns_f2::fma(d2, y, NR2);                      /* r - R, to ~5u r */       \
+    const f2 res = xns_f2::fma(t0, sub(N2R2, t0), num);         /* num - t0 (t0 + 2R) */    \
+    const f2 t = xns_f2::fma(res, mul(y, HALF2), t0);           /* r - floor(R0) - 0.5 */   \
     const f2 tm = add(t, MAGIC2);                                                           \
     const f2 d = sub(t, sub(tm, MAGIC2));                                                   \
     const f2 m = xns_f2::fma(xns_f2::abs(t), NK1_2, MC2);                                   \
@@ -684,14 +701,13 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
     XNS_COUNT(fabsf(lo(d)) <= lo(m), slo, VLO, KLO, NM)                                     \
     XNS_COUNT(fabsf(hi(d)) <= hi(m), shi, VHI, KHI, NM)                                     \
   }
-  // lanes with near pairs in the step's row pair ROW, ROW + 1 append one entry each, in lane order;
-  // fewer than 32 entries wait between pushes and a push adds at most 32: never more than 63 queued
+  // lanes with near pairs in the step's rows ROW .. ROW + 3 append one entry each, in lane order;
+  // fewer than 32 entries wait between steps and a push adds at most 32: never more than 63 queued
 #define XNS_PUSH(NM, ROW)                                                                   \
   {                                                                                         \
     const unsigned nb = __ballot_sync(0xffffffffu, NM != 0);                                \
-    if (NM) queue[(qn + __popc(nb & below)) & (QUEUE - 1)] = (uint16_t)((((ROW) >> 1) << 9) | (lane << 4) | NM); \
+    if (NM) queue[(qn + __popc(nb & below)) & (QUEUE - 1)] = (((ROW) >> 2) << 13) | (lane << 8) | NM; \
     qn += __popc(nb);                                                                       \
-    while (qn - qd >= 32) drain(32);                                                        \
   }
   // a step: rows i .. i + 3 (two row pairs) against the lane's two J atoms; rows at or beyond ni hold
   // stale data, their pairs are not valid
@@ -728,14 +744,16 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
       XNS_DIRECT2(XB, YB, ZB, XJ0, YJ0, ZJ0, vc0, vd0, 0, 2, nmB)
       XNS_DIRECT2(XB, YB, ZB, XJ1, YJ1, ZJ1, vc1, vd1, 1, 3, nmB)
     }
-    XNS_PUSH(nmA, i)
-    XNS_PUSH(nmB, i + 2)
+    const uint32_t nm = nmA | (nmB << 4);  // bit k: row i + k / 2, J atom lane + 32 (k & 1)
+    XNS_PUSH(nm, i)
+    while (qn - qd >= 32) drain(32);
   }
 #undef XNS_PUSH
 #undef XNS_CENTRED2
 #undef XNS_DIRECT2
 #undef XNS_COUNT
   if (qn != qd) drain(qn - qd);
+  __syncwarp();  // every lane is done with the stage before the warp's next tile pair refills it
   return bad;
 }
 
