@@ -166,7 +166,7 @@ int batch_build(xns_batch *b, uint32_t nstruct, const uint32_t *nel, const uint3
   for (uint32_t s = 0; s < nstruct; s++) hs.st.push_back({si[s].e0, si[s].nel});
 
   if (autotune) {  // time the histogram launch for each candidate plan; keep the fastest
-    static const HistTuning cand[] = {{56, 45 * 1024 + 512}, {32, 45 * 1024 + 512}, {96, 45 * 1024 + 512}, {56, 16 * 1024}};
+    static const HistTuning cand[] = {{56, HIST_WIN_MAX}, {32, HIST_WIN_MAX}, {96, HIST_WIN_MAX}, {56, 16 * 1024}};
     double best = 1e300;
     for (const HistTuning &t : cand) {
       HistLaunch L;

@@ -43,14 +43,16 @@ namespace {
 
 constexpr int TILE_MAX = 64;         // atoms per tile
 constexpr int MAX_CELLS_AXIS = 256;
-constexpr int HW_WARPS = 16;
+constexpr int HW_WARPS = 20;         // at 96 registers a thread, 20 warps fill the register file
 constexpr int HW_THREADS = 32 * HW_WARPS;
-constexpr uint32_t WIN_MAX = 45 * 1024 + 512;  // largest window (bins) that fits with the warp stages
+constexpr uint32_t WIN_MAX = HIST_WIN_MAX;  // largest window (bins) that fits with the warp stages
 constexpr uint32_t BUCKET = 1024;    // distance bucket of the tile-pair sort, in bins
 constexpr int SCAN_THREADS = 1024;
 constexpr int QUEUE = 64;            // queue entries per warp: u32 (i/4) << 13 | lane << 8 | 8-bit pair mask
 // per warp: FP64 I tile, FP32 I-tile offsets (+ P_i), the queue (bytes)
 constexpr int WARP_STAGE = 3 * TILE_MAX * 8 + 4 * TILE_MAX * 4 + QUEUE * 4;
+// the window kernel's shared memory (window, 32 spare slots, stages, 16 static bytes) within 227 KB
+static_assert(4 * (WIN_MAX + 32) + WARP_STAGE * HW_WARPS + 16 <= 227 * 1024, "window and stages fit");
 
 struct Tile {
   uint32_t start, count, elem, pad;
@@ -548,6 +550,14 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
     row[4] = (float)az;
     row[6] = P;
   }
+  // Apart from a tile against itself, a pair's validity is not tested per pair: rows past the tile in
+  // its last step and J slots past the tile hold NaN, so their estimates are never fast (every
+  // comparison with NaN is false) and add 1 to the lane's spare slot; their near bits are dropped
+  // once per step (cmask and the row mask below).
+  if (!SAME && ni + lane < ((ni + 3u) & ~3u)) {
+    float *row = wIf + ((ni + lane) >> 1) * 8 + ((ni + lane) & 1);
+    row[0] = row[2] = row[4] = row[6] = __int_as_float(0x7fffffff);
+  }
   const uint32_t j0 = lane, j1 = lane + 32;
   const bool c0 = j0 < nj, c1 = j1 < nj;
   // the J tile stays in registers: FP64 for the exact path (other lanes fetch it by shuffle), FP32
@@ -583,6 +593,11 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
       xj1 = (float)bx1 - dl[0];
       yj1 = (float)by1 - dl[1];
       zj1 = (float)bz1 - dl[2];
+    }
+    if (!SAME) {
+      const float nan = __int_as_float(0x7fffffff);
+      if (!c0) xj0 = yj0 = zj0 = qj0 = nan;
+      if (!c1) xj1 = yj1 = zj1 = qj1 = nan;
     }
   }
   // the J atoms' values and the tile pair's constants as packed pairs (both halves equal)
@@ -709,13 +724,21 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
     if (NM) queue[(qn + __popc(nb & below)) & (QUEUE - 1)] = (((ROW) >> 2) << 13) | (lane << 8) | NM; \
     qn += __popc(nb);                                                                       \
   }
-  // a step: rows i .. i + 3 (two row pairs) against the lane's two J atoms; rows at or beyond ni hold
-  // stale data, their pairs are not valid
+  // a step: rows i .. i + 3 (two row pairs) against the lane's two J atoms.  A tile against itself
+  // tests validity per pair (i < j, both inside the tile); other tile pairs rely on the NaN padding.
+  const uint32_t cmask = (c0 ? 0x55u : 0u) | (c1 ? 0xAAu : 0u);  // near bits of the lane's real J atoms
   for (uint32_t i = 0; i < ni; i += 4) {
     const float4 pa = wI4[i], pb = wI4[i + 1], pc = wI4[i + 2], pd = wI4[i + 3];  // (x x' y y'), (z z' w w')
-    bool va0 = c0, va1 = c1, vb0 = c0 && i + 1 < ni, vb1 = c1 && i + 1 < ni;
-    bool vc0 = c0 && i + 2 < ni, vc1 = c1 && i + 2 < ni, vd0 = c0 && i + 3 < ni, vd1 = c1 && i + 3 < ni;
+    bool va0 = true, va1 = true, vb0 = true, vb1 = true, vc0 = true, vc1 = true, vd0 = true, vd1 = true;
     if (SAME) {
+      va0 = c0;
+      va1 = c1;
+      vb0 = c0 && i + 1 < ni;
+      vb1 = c1 && i + 1 < ni;
+      vc0 = c0 && i + 2 < ni;
+      vc1 = c1 && i + 2 < ni;
+      vd0 = c0 && i + 3 < ni;
+      vd1 = c1 && i + 3 < ni;
       va0 = va0 && i < j0;
       va1 = va1 && i < j1;
       vb0 = vb0 && i + 1 < j0;
@@ -744,7 +767,11 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
       XNS_DIRECT2(XB, YB, ZB, XJ0, YJ0, ZJ0, vc0, vd0, 0, 2, nmB)
       XNS_DIRECT2(XB, YB, ZB, XJ1, YJ1, ZJ1, vc1, vd1, 1, 3, nmB)
     }
-    const uint32_t nm = nmA | (nmB << 4);  // bit k: row i + k / 2, J atom lane + 32 (k & 1)
+    uint32_t nm = nmA | (nmB << 4);  // bit k: row i + k / 2, J atom lane + 32 (k & 1)
+    if (!SAME) {  // drop the NaN pairs: rows ni and beyond, J slots past the tile
+      const uint32_t v = ni - i;
+      nm &= cmask & (v >= 4 ? 0xFFu : (1u << (2 * v)) - 1u);
+    }
     XNS_PUSH(nm, i)
     while (qn - qd >= 32) drain(32);
   }

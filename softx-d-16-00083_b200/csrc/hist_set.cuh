@@ -22,9 +22,11 @@ struct HistSet {
 // the whole histogram exactly.
 // w_begin / max_pairs: this plan takes the tile pairs [w_begin, w_begin + max_pairs) of the structure's
 // enumeration (0: all of them, fewer than 2^32); the passes of a large structure add into one histogram.
+// The deepest window (bins) that fits in shared memory beside the counting warps' stages.
+constexpr uint32_t HIST_WIN_MAX = 42 * 1024 + 512;
 struct HistTuning {
   uint32_t cell_target = 56;
-  uint32_t win = 45 * 1024 + 512;
+  uint32_t win = HIST_WIN_MAX;
   uint32_t shard = 0, nshard = 1;
   unsigned long long w_begin = 0, max_pairs = 0;
   bool ordered = false;  // atoms of each cell in input order (same tiles in every pass or shard)
