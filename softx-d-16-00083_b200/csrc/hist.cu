@@ -494,7 +494,7 @@ __device__ __noinline__ uint32_t ref_bin_slow(double d2, double bin, double inv_
   return ref_bin(d2, bin, inv_bin, margin, nhist);
 }
 
-template <bool SAME, bool WINDOW, bool CENTRED>
+template <bool SAME, bool WINDOW, bool CENTRED, bool INWIN = false>
 __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const TilePair tp, const PairGeom &g,
                                                       uint8_t *stage, uint32_t *win, uint32_t base,
                                                       unsigned long long *h) {
@@ -625,6 +625,7 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
   }
   __syncwarp();
   const uint32_t below = (1u << lane) - 1u;  // lanes below this one
+  const uint32_t tbase4 = (uint32_t)tbase * 4u, Wl4 = Wl * 4u, spare4 = (W + lane) * 4u;  // byte offsets
   const double nhm1 = (double)p.nhist - 1.0;
   uint32_t qn = 0, qd = 0;  // entries queued / binned (warp-uniform)
   unsigned bad = 0;
@@ -663,14 +664,15 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
   };
   // FAST: the estimate's bin is certain and its slot is below Wl; a lane without a fast pair adds 1 to
   // its own spare slot instead (branch-free; the 32 spare slots are never flushed or read), near pairs
-  // set their bit K of the step's mask.
+  // set their bit K of the step's mask.  Slots are byte offsets (4 x the bin's slot, modulo 2^32): a
+  // slot of a valid pair lies within +-2^23, so the unsigned test against 4 Wl keeps its meaning.
 #define XNS_COUNT(FAST, SLOT, VALID, K, NM)                                                 \
   {                                                                                         \
-    const bool fast = (VALID) && (FAST) && (SLOT) < Wl;                                     \
+    const bool fast = (VALID) && (FAST) && (INWIN || (SLOT) < Wl4);                         \
     if (WINDOW) {                                                                           \
-      atomicAdd(win + (fast ? (SLOT) : W + lane), 1u);                                      \
+      atomicAdd(reinterpret_cast<uint32_t *>(reinterpret_cast<char *>(win) + (fast ? (SLOT) : spare4)), 1u); \
     } else if (fast) {                                                                      \
-      atomicAdd(h + (SLOT), 1ull);                                                          \
+      atomicAdd(h + ((SLOT) >> 2), 1ull);                                                   \
     }                                                                                       \
     NM |= ((VALID) && !fast) ? (1u << (K)) : 0u;                                            \
   }
@@ -691,8 +693,8 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
     const f2 t = add(r, MAGIC2);                                                            \
     const f2 d = sub(r, sub(t, MAGIC2));                                                    \
     const f2 m = xns_f2::fma(r, MR2, M02);                                                  \
-    const uint32_t slo = (uint32_t)(__float_as_int(lo(t)) - tbase) - (lo(d) < 0.f ? 1u : 0u); \
-    const uint32_t shi = (uint32_t)(__float_as_int(hi(t)) - tbase) - (hi(d) < 0.f ? 1u : 0u); \
+    const uint32_t slo = (uint32_t)__float_as_int(lo(t)) * 4u - tbase4 - (lo(d) < 0.f ? 4u : 0u); \
+    const uint32_t shi = (uint32_t)__float_as_int(hi(t)) * 4u - tbase4 - (hi(d) < 0.f ? 4u : 0u); \
     XNS_COUNT(fabsf(lo(d)) >= lo(m), slo, VLO, KLO, NM)                                     \
     XNS_COUNT(fabsf(hi(d)) >= hi(m), shi, VHI, KHI, NM)                                     \
   }
@@ -711,8 +713,8 @@ __device__ __forceinline__ unsigned count_tile_pair_t(const HistParams &p, const
     const f2 tm = add(t, MAGIC2);                                                           \
     const f2 d = sub(t, sub(tm, MAGIC2));                                                   \
     const f2 m = xns_f2::fma(xns_f2::abs(t), NK1_2, MC2);                                   \
-    const uint32_t slo = (uint32_t)(__float_as_int(lo(tm)) - tbase);                        \
-    const uint32_t shi = (uint32_t)(__float_as_int(hi(tm)) - tbase);                        \
+    const uint32_t slo = (uint32_t)__float_as_int(lo(tm)) * 4u - tbase4;                   \
+    const uint32_t shi = (uint32_t)__float_as_int(hi(tm)) * 4u - tbase4;                   \
     XNS_COUNT(fabsf(lo(d)) <= lo(m), slo, VLO, KLO, NM)                                     \
     XNS_COUNT(fabsf(hi(d)) <= hi(m), shi, VHI, KHI, NM)                                     \
   }
@@ -789,7 +791,14 @@ __device__ __forceinline__ unsigned count_tile_pair(const HistParams &p, const T
                                                     uint32_t base, unsigned long long *h) {
   const PairGeom g = pair_geom(p.tiles[tp.I], p.tiles[tp.J], p.inv_bin);
   if (tp.I == tp.J) return count_tile_pair_t<true, WINDOW, false>(p, tp, g, stage, win, base, h);
-  if (far_pair(g)) return count_tile_pair_t<false, WINDOW, true>(p, tp, g, stage, win, base, h);
+  if (far_pair(g)) {
+    // Every bin the tile pair can reach ([kmin, kmax], from the tiles' boxes, at or above the window's
+    // base inside a run) lies in the window and below the last bin and 2^22: the slot of a fast pair,
+    // its exact bin - base, needs no test (INWIN).
+    if (WINDOW && tp.kmax < min(base + p.win, min(p.nhist - 1u, 1u << 22)))
+      return count_tile_pair_t<false, WINDOW, true, true>(p, tp, g, stage, win, base, h);
+    return count_tile_pair_t<false, WINDOW, true>(p, tp, g, stage, win, base, h);
+  }
   return count_tile_pair_t<false, WINDOW, false>(p, tp, g, stage, win, base, h);
 }
 
