@@ -38,7 +38,7 @@ SL = [3.63, 9.58]
 HIST_FLOPS_PER_PAIR = 10  # the reference's per-pair FP64 arithmetic: 3 sub, 3 mul, 2 add, sqrt, divide
 # DRAM bytes (read + write) of one hist_window_kernel launch on the 30^3-cell cube, from an ncu capture
 # of this benchmark (dram__bytes_read.sum + dram__bytes_write.sum); re-measure when the kernel changes
-HIST_TRAFFIC_30 = 108.47e6 + 4.42e6
+HIST_TRAFFIC_30 = 108_363_520 + 4_282_112  # bytes per hist_window_kernel launch, rock-salt 30^3 cube (ncu, 1 pass)
 
 
 def workload(seed, cells=CELLS):
@@ -525,7 +525,7 @@ def ours(args, rank, world, local_rank):
                          "unit": "1e9 shared-memory increments/s", "frac": inc / atom_peak.value if atom_peak.value else None,
                          "traffic": HIST_TRAFFIC_30 if args.cells == CELLS else None,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one hist_window_kernel "
-                                           "launch of this workload (108.5 MB + 4.4 MB; 1-pass capture)",
+                                           "launch of this workload (108.4 MB + 4.3 MB; 1-pass capture)",
                          "peak_source": "measured in-process (conflict-free atomicAdd loop, xns_measure_smem_atomic_peak)",
                          "fp64_view": {"flops_per_pair": HIST_FLOPS_PER_PAIR, "peak_tflops": peak.value,
                                        "frac": HIST_FLOPS_PER_PAIR * pairs / (hist_avg * 1e-3) / 1e12 / peak.value}},
