@@ -515,8 +515,8 @@ def ours(args, rank, world, local_rank):
     line = {"metric": METRIC, "value": job_rate(units, pairs, ms_step), "unit": "pairs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "strong" if args.shard else "weak", "vs_baseline": None,
-            "dtype": "f32 distance estimate + f64 exact re-binning near bin edges, u64 counts (histogram); integer-digit "
-                     "tensor-core transform with exact sums (I(q)); f64 (PDF)",
+            "dtype": "f32 distance estimate + f64 exact re-binning near bin edges, u64 counts (histogram); f64 "
+                     "angle-split transform (I(q)); f64 (PDF)",
             "data": "synthetic (seeded)",
             "patterns_per_s": units / (ms_step * 1e-3),
             "config": config_block(els, nh, args.cells), "parallelism": par,

@@ -63,7 +63,8 @@ int xns_set_stream(xns_ctx *ctx, void *stream);
  * fixed device-memory budget per context; no counterpart in the reference. */
 int xns_set_memory_limit(xns_ctx *ctx, uint64_t bytes);
 /* Failure-path test of the tensor-core pipelines: the next tensor-core transform on this context
- * (the exact histogram -> I(q) transform or the 2D plane) runs with its copy warp issuing no copies
+ * (xns_hist_transform_exact, the batched ensembles' transform or the 2D plane; not the calc functions'
+ * FP64 histogram transform) runs with its copy warp issuing no copies
  * and every pipeline wait bounded by wait_limit_ns (at most 2 s, the kernels' own bound).  Its waits
  * run out, the kernel releases its tensor memory and returns, and that call fails with XNS_ERR_CUDA
  * ("a pipeline wait ran out of time"); the context stays usable and the following calls run
@@ -230,6 +231,17 @@ int xns_hist_transform_bf16x3(xns_ctx *ctx, const uint64_t *hist, uint32_t ncols
  * element, so I(q) stays within 1e-5 of FP64 even at the deep minima of small particles, where the
  * FP32-accumulated bf16x3 form loses precision.  Counts below 2^32 (XNS_ERR_LIMIT beyond). */
 int xns_hist_transform_exact(xns_ctx *ctx, const uint64_t *hist, uint32_t ncols, uint32_t nh, double bin,
+                             const double *q, uint32_t nq, double *G);
+
+/* The same G in FP64 by angle splitting, the form xns_calc_int_1d_hist and the fused entry points use:
+ * each bin distance r_k = R_h + r_l (R_h a multiple of 64 bins), sin(q r_k) = sin(q R_h) cos(q r_l) +
+ * cos(q R_h) sin(q r_l), so the bin sum is an FP64 product with K = 64 against per-q tables of 64
+ * cosines and sines, and the +1e-8 of the denominator is kept to first order (an FP32 product of the
+ * same form; the next order is below 1e-14 of the terms).  No sinc matrix and no cache: every call
+ * costs the same.  G carries FP64 rounding (about 1e-13 of its terms).  Scratch: 1.6 KB per q point,
+ * at most 48 bytes per bin, and the partial sums (at most 64 bytes per q point and split, about
+ * 16 x SMs x 64 / nq splits).  Counts below 2^53. */
+int xns_hist_transform_split(xns_ctx *ctx, const uint64_t *hist, uint32_t ncols, uint32_t nh, double bin,
                              const double *q, uint32_t nq, double *G);
 
 /* ---- 2D intensity on a flat Cartesian q plane ------------------------------------------------------ */

@@ -5,11 +5,11 @@
 //   I(q) = [ sum_e N_e w_e^2 + 2 sum_{a<=b} w_a w_b sum_k n_ab(k) sin(q r_k)/(q r_k + 1e-8) ] / N,
 //   r_k = (k + 0.5) * bin; empty bins contribute nothing (the reference skips them, :857).
 //
-// The contraction over bins runs on the tensor cores with integer digits and exact accumulation
-// (tc_exact.cu): at the deep low-q minima of I(q) the bin sum cancels to 1e-5..1e-6 of its terms, and
-// FP32 sums (FP32 recurrence or FP32 accumulators) leave 3e-5..5e-5 of I(q) there, while the exact
-// transform stays within 2e-6 of the FP64 reference.  The shared epilogue (sinc_engine.cu) applies
-// the weights, the self term, 1/N and the polarisation factor.
+// The contraction over bins runs in FP64 by angle splitting (hist_split.cu): at the deep low-q minima
+// of I(q) the bin sum cancels to 1e-5..1e-6 of its terms, and FP32 sums leave 3e-5..5e-5 of I(q)
+// there.  The transform yields sum_k (n(k) / r_k) sin(q r_k) and the first-order +1e-8 sum; the shared
+// epilogue (sinc_engine.cu) divides by q, subtracts 1e-8 T / q^2 and applies the weights, the self
+// term, 1/N and the polarisation factor.
 #include <string.h>
 
 #include "sinc_engine.cuh"
@@ -26,12 +26,13 @@ int xns_hist_iq_device(xns_ctx *ctx, const unsigned long long *d_hist, const uin
   double q0 = 0, dq = 0;
   const bool uniform = xns_uniform_mesh(q, nq, &q0, &dq);
   int st;
-  void *d_G;
+  void *d_G, *d_T;
   if ((st = xns_scratch(ctx, SLOT_PARTIAL, sizeof(double) * P * nq, &d_G))) return st;
+  if ((st = xns_scratch(ctx, SLOT_EPS_T, sizeof(double) * P * nq, &d_T))) return st;
   if ((st = xns_stage_begin(ctx, STAGE_IQ))) return st;
-  if ((st = xns_tc_hist_transform_exact(ctx, d_hist, P, nhist, nhist, bin, q, nq, (double *)d_G))) return st;
+  if ((st = xns_hist_transform_split(ctx, d_hist, P, nhist, nhist, bin, q, nq, (double *)d_G, (double *)d_T))) return st;
   if ((st = sinc_epilogue(ctx, 1, P, nel, 1, n_el, q, nq, uniform, q0, dq, d_w, ntot, polar, lambda, d_I,
-                          (const double *)d_G, false)))
+                          (const double *)d_G, true, true, (const double *)d_T)))
     return st;
   return xns_stage_end(ctx, STAGE_IQ);
 }

@@ -89,5 +89,9 @@ int xns_tc_exact_check(xns_ctx *ctx, const ExactLaunch &X);
 int xns_tc_max_count(xns_ctx *ctx, const unsigned long long *d_hist, uint32_t ncols, uint32_t nh, size_t ldh,
                      unsigned long long *max_count);
 // The whole contraction with integer digits and exact accumulation (tc_exact.cu).
+// Angle-split FP64 sums G = sum_k (n(k) / r_k) sin(q r_k) and T = sum_k (n(k) / r_k^2) sin(q r_k), columns
+// x nq each (hist_split.cu).
+int xns_hist_transform_split(xns_ctx *ctx, const unsigned long long *d_hist, uint32_t ncols, uint32_t nh, size_t ldh,
+                             double bin, const double *q, uint32_t nq, double *d_G, double *d_T);
 int xns_tc_hist_transform_exact(xns_ctx *ctx, const unsigned long long *d_hist, uint32_t ncols, uint32_t nh, size_t ldh,
                              double bin, const double *q, uint32_t nq, double *d_G);

@@ -41,6 +41,7 @@ enum ScratchSlot {
   SLOT_ATOMS,           // structure builder: the last build's atoms (x y z doubles, element-major)
   SLOT_EPS_HIST,        // sinc engine: the +1e-8 distance histogram
   SLOT_EPS_T,           // sinc engine: the +1e-8 sums per class and q
+  SLOT_SPLIT,           // angle-split transform: cos / sin tables, weighted histogram columns, partial sums
   SLOT_COUNT
 };
 

@@ -66,6 +66,7 @@ def _declare(lib):
     lib.xns_calc_int_2d.argtypes = [_p, _PP, _p, _u32, _p, _u32, _u32, _p, _p, _p, _u32, _dbl, _int, _PP, _p, _int, _p, _p]
     lib.xns_hist_transform_bf16x3.argtypes = [_p, _p, _u32, _u32, _dbl, _p, _u32, _p]
     lib.xns_hist_transform_exact.argtypes = [_p, _p, _u32, _u32, _dbl, _p, _u32, _p]
+    lib.xns_hist_transform_split.argtypes = [_p, _p, _u32, _u32, _dbl, _p, _u32, _p]
     _BATCH_IN = [_u32, _p, _p, _p, _u32, _dbl, _p, _u32, _int, _PP, _p, _int, _dbl]
     lib.xns_calc_batch_debye_hist.argtypes = [_p] + _BATCH_IN + [_p, _p]
     lib.xns_batch_create.argtypes = [_p] + _BATCH_IN + [_int, C.POINTER(_p)]
@@ -418,12 +419,14 @@ class Context:
         return Batch(self, structures, nhist, bin, q, source, sl, ff, polar, lam, autotune)
 
     def hist_transform(self, hist, bin, q, scheme="exact"):
-        """G[c, i] = sum_k hist[c, k] sin(q_i r_k)/(q_i r_k) on the tensor cores: scheme "bf16x3" (split
-        BF16, FP32 accumulation) or "exact" (integer digits, exact accumulation)."""
+        """G[c, i] = sum_k hist[c, k] sin(q_i r_k)/(q_i r_k + 1e-8): scheme "bf16x3" (split BF16 on the
+        tensor cores, FP32 accumulation), "exact" (integer digits on the tensor cores, exact accumulation)
+        or "split" (FP64 angle splitting, the form the calc functions use)."""
         hist = np.ascontiguousarray(np.atleast_2d(hist), dtype=np.uint64)
         q = _f64(q)
         G = np.zeros((hist.shape[0], len(q)))
-        fn = {"bf16x3": lib.xns_hist_transform_bf16x3, "exact": lib.xns_hist_transform_exact}[scheme]
+        fn = {"bf16x3": lib.xns_hist_transform_bf16x3, "exact": lib.xns_hist_transform_exact,
+              "split": lib.xns_hist_transform_split}[scheme]
         self._check(fn(self._h, _ptr(hist), hist.shape[0], hist.shape[1], bin, _ptr(q), len(q), _ptr(G)))
         return G
 

@@ -45,7 +45,9 @@ def test_batch_matches_single_structure_calls(gpu_ctx):
         hs = gpu_ctx.calc_hist(els, nh, bin)
         assert np.array_equal(h[off * nh:(off + P) * nh], hs), s
         Is = gpu_ctx.calc_int_1d_hist(hs, [len(e) for e in els], nh, bin, q, 0, sl=sl)
-        assert rel_err(I[s], Is) < 1e-10, s
+        # the batch transforms with the integer-digit GEMM, the single call with the FP64 angle split:
+        # they agree to the digits' quantization (~1e-12 of a sinc value)
+        assert rel_err(I[s], Is) < 1e-8, s
         off += P
 
 
@@ -59,7 +61,7 @@ def test_batch_xray_polar(gpu_ctx):
     for s, els in enumerate(structs):
         hs = gpu_ctx.calc_hist(els, nh, bin)
         Is = gpu_ctx.calc_int_1d_hist(hs, [len(e) for e in els], nh, bin, q, 1, ff=ff[s], polar=True, lam=1.5)
-        assert rel_err(I[s], Is) < 1e-10, s
+        assert rel_err(I[s], Is) < 1e-8, s  # digit GEMM against the FP64 angle split, as above
 
 
 @pytest.mark.parametrize("autotune", [False, True])

@@ -6,7 +6,7 @@
   more returns XNS_ERR_NOMEM before it queues work;
 * a pipeline wait that runs out: xns_inject_pipeline_stall makes the next tensor-core transform's copy
   warp issue nothing and bounds its waits to 5 ms; the waits give up, the kernel frees its tensor
-  memory and returns, the call reports XNS_ERR_CUDA.
+  memory and returns, the call (the integer-digit histogram transform) reports XNS_ERR_CUDA.
 After each, the same context computes the right answer again."""
 import numpy as np
 import pytest
@@ -58,15 +58,19 @@ def test_memory_limit_gives_nomem_then_recovers(oracle):
 def test_pipeline_wait_runs_out_and_context_recovers(gpu_ctx):
     import xns_b200
     g = load_golden("iqhist__rocksalt_xray")
-    args = (g["hist"], g["n_el"], int(g["nhist"]), float(g["bin"]), g["q"], 1)
-    kw = dict(ff=g["ff"], polar=True, lam=float(g["lam"]))
-    assert rel_err(gpu_ctx.calc_int_1d_hist(*args, **kw), g["I"]) < 1e-5
+    nh, bin, q = int(g["nhist"]), float(g["bin"]), g["q"]
+    H = np.asarray(g["hist"], dtype=np.uint64).reshape(-1, nh)
+    G64 = gpu_ctx.hist_transform(H, bin, q, "split")  # FP64, no tensor-core pipeline
+    G0 = gpu_ctx.hist_transform(H, bin, q, "exact")
+    assert np.max(np.abs(G0 - G64)) < 1e-8 * np.max(np.abs(G64))
     gpu_ctx.inject_pipeline_stall(5_000_000)  # 5 ms
     with pytest.raises(xns_b200.XnsError) as e:
-        gpu_ctx.calc_int_1d_hist(*args, **kw)
+        gpu_ctx.hist_transform(H, bin, q, "exact")
     assert e.value.status == XNS_ERR_CUDA and "ran out of time" in str(e.value)
-    # the next call (no injection) is whole again
-    assert rel_err(gpu_ctx.calc_int_1d_hist(*args, **kw), g["I"]) < 1e-5
+    # the next call (no injection) is whole again, and so are the calc functions
+    assert np.max(np.abs(gpu_ctx.hist_transform(H, bin, q, "exact") - G0)) < 1e-12 * np.max(np.abs(G0))
+    args = (g["hist"], g["n_el"], nh, bin, q, 1)
+    assert rel_err(gpu_ctx.calc_int_1d_hist(*args, ff=g["ff"], polar=True, lam=float(g["lam"])), g["I"]) < 1e-5
     # the limit must be positive and within the kernels' own bound
     with pytest.raises(xns_b200.XnsError) as e:
         gpu_ctx.inject_pipeline_stall(0)

@@ -29,7 +29,7 @@ def col_err(G, G64):
     return float(np.max(np.abs(G - G64).max(axis=1) / np.abs(G64).max(axis=1)))
 
 
-@pytest.mark.parametrize("scheme,tol", [("bf16x3", 2e-5), ("exact", 1e-8)])
+@pytest.mark.parametrize("scheme,tol", [("bf16x3", 2e-5), ("exact", 1e-8), ("split", 1e-11)])
 @pytest.mark.parametrize("ncols,nh,nq", [(1, 64, 128), (3, 1000, 200), (17, 4100, 300), (300, 2000, 130)])
 def test_transform_vs_fp64(gpu_ctx, scheme, tol, ncols, nh, nq):
     rng = np.random.default_rng(ncols + nh)
@@ -57,7 +57,24 @@ def test_exact_large_counts(gpu_ctx, top):
     assert e.value.status == 6
 
 
-@pytest.mark.parametrize("scheme,tol", [("bf16x3", 2e-5), ("exact", 1e-8)])
+def test_split_large_counts_and_edges(gpu_ctx):
+    """The angle-split transform takes counts up to 2^53 (FP64 weights), bins past the last block of
+    64, q = 0 (sin 0 / (0 + 1e-8) = 0), a q mesh that is not a multiple of 64 and one column (the
+    narrowest pass)."""
+    rng = np.random.default_rng(21)
+    for ncols, nh, nq, top in ((1, 70, 1, 1 << 40), (2, 4097, 65, 1 << 50), (4, 129, 63, 1 << 20)):
+        H = rng.integers(0, top, size=(ncols, nh)).astype(np.uint64)
+        q = np.concatenate([[0.0], np.sort(rng.uniform(0.01, 30.0, nq - 1))]) if nq > 1 else np.array([0.7])
+        G64 = H.astype(np.float64) @ sinc_matrix(q, nh, 0.003).T
+        G = gpu_ctx.hist_transform(H, 0.003, q, "split")
+        if nq > 1:
+            assert np.all(G[:, 0] == 0.0)
+            assert col_err(G[:, 1:], G64[:, 1:]) < 1e-11
+        else:
+            assert col_err(G, G64) < 1e-11
+
+
+@pytest.mark.parametrize("scheme,tol", [("bf16x3", 2e-5), ("exact", 1e-8), ("split", 1e-11)])
 def test_transform_cache_follows_mesh(gpu_ctx, scheme, tol):
     rng = np.random.default_rng(3)
     H = rng.integers(0, 1000, size=(2, 700)).astype(np.uint64)
