@@ -26,6 +26,7 @@
 
 #include "f32x2.cuh"
 #include "tc_gemm.cuh"
+#include "xmath.cuh"
 #include "xns_internal.cuh"
 
 namespace {
@@ -41,39 +42,6 @@ static_assert(SQ == TQ * (ST / SHL), "a CTA's threads cover its q tile");
 // Column stride of the G tables: 1, 2 or 4 (three columns are padded to four for 16-byte loads).
 __host__ __device__ constexpr int gstride(int cb) { return cb == 3 ? 4 : cb; }
 
-// sin and cos of x in FP64 to about one ulp for |x| < 2^20: x = n pi/2 + y (Cody-Waite, pi/2 as a
-// two-part FP64 sum), then the Taylor series of sin y to y^15 and of cos y to y^16 (truncation below
-// 5e-17 on |y| <= pi/4).
-__device__ __forceinline__ void sincos_fp64(double x, double *s, double *c) {
-  const double MAGIC = 6755399441055744.0;  // 1.5 * 2^52: rounds to an integer kept in the low word
-  const double TWO_OVER_PI = 0.63661977236758134308;
-  const double PIO2_HI = 1.5707963267948966192;
-  const double PIO2_LO = 6.123233995736766036e-17;
-  const double t = __fma_rn(x, TWO_OVER_PI, MAGIC);
-  const int n = __double2loint(t);
-  const double nd = t - MAGIC;
-  const double y = __fma_rn(-nd, PIO2_LO, __fma_rn(-nd, PIO2_HI, x));
-  const double y2 = y * y;
-  double sp = __fma_rn(y2, -1.0 / 1307674368000.0, 1.0 / 6227020800.0);  // -1/15!, 1/13!
-  sp = __fma_rn(y2, sp, -1.0 / 39916800.0);                               // -1/11!
-  sp = __fma_rn(y2, sp, 1.0 / 362880.0);                                  // 1/9!
-  sp = __fma_rn(y2, sp, -1.0 / 5040.0);                                   // -1/7!
-  sp = __fma_rn(y2, sp, 1.0 / 120.0);                                     // 1/5!
-  sp = __fma_rn(y2, sp, -1.0 / 6.0);                                      // -1/3!
-  sp = __fma_rn(y2 * y, sp, y);
-  double cp = __fma_rn(y2, 1.0 / 20922789888000.0, -1.0 / 87178291200.0);  // 1/16!, -1/14!
-  cp = __fma_rn(y2, cp, 1.0 / 479001600.0);                                  // 1/12!
-  cp = __fma_rn(y2, cp, -1.0 / 3628800.0);                                   // -1/10!
-  cp = __fma_rn(y2, cp, 1.0 / 40320.0);                                      // 1/8!
-  cp = __fma_rn(y2, cp, -1.0 / 720.0);                                       // -1/6!
-  cp = __fma_rn(y2, cp, 1.0 / 24.0);                                         // 1/4!
-  cp = __fma_rn(y2, cp, -0.5);                                               // -1/2!
-  cp = __fma_rn(y2, cp, 1.0);
-  const double a = (n & 1) ? cp : sp, b = (n & 1) ? sp : cp;
-  *s = (n & 2) ? -a : a;
-  *c = ((n + 1) & 2) ? -b : b;
-}
-
 // Tables per q tile qt: A64[qt][0][l][j] = cos(q r_l), A64[qt][1][l][j] = sin(q r_l) for q the tile's
 // j-th value (0 past nq), A32 the same rounded to float; qv the padded mesh.
 __global__ void split_tables_kernel(const double *__restrict__ qmesh, uint32_t nq, uint32_t nq_pad,
@@ -85,7 +53,7 @@ __global__ void split_tables_kernel(const double *__restrict__ qmesh, uint32_t n
   const double q = iq < nq ? qmesh[iq] : 0.0;
   if (l == 0) qv[iq] = q;
   double s, c;
-  sincos_fp64(q * ((l + 0.5) * bin), &s, &c);
+  xns_math::xns_sincos64_acc(q * ((l + 0.5) * bin), &s, &c);
   const size_t o = (size_t)(iq / SQ) * 2 * SLO * SQ + (size_t)l * SQ + iq % SQ;
   A64[o] = c;
   A64[o + SLO * SQ] = s;
@@ -182,8 +150,8 @@ __global__ void __launch_bounds__(ST, 1) split_sum_kernel(SplitArgs a) {
 #pragma unroll
   for (int t = 0; t < TQ; t++) {  // sin / cos(q R_h) at the thread's first block, and the rotation by SHL blocks
     const double q = a.qv[(size_t)qt * SQ + split_q(gq, t)];
-    sincos_fp64(q * ((hb + hl) * a.blk), &sH[t], &cH[t]);
-    sincos_fp64(q * (SHL * a.blk), &sR[t], &cR[t]);
+    xns_math::xns_sincos64_acc(q * ((hb + hl) * a.blk), &sH[t], &cH[t]);
+    xns_math::xns_sincos64_acc(q * (SHL * a.blk), &sR[t], &cR[t]);
   }
   const double *cq = c64 + 2 * gq, *sq = c64 + SLO * SQ + 2 * gq;
   const float *cqf = c32 + 2 * gq, *sqf = c32 + SLO * SQ + 2 * gq;

@@ -80,4 +80,37 @@ __device__ __forceinline__ float xns_sin(double x) {
   return s;
 }
 
+// sin and cos of x in FP64 to about one ulp for |x| < 2^20: the same quadrant reduction, then the
+// Taylor series of sin y to y^15 and of cos y to y^16 (truncation below 5e-17 on |y| <= pi/4), for
+// values that enter FP64 sums (the angle-split transforms).
+__device__ __forceinline__ void xns_sincos64_acc(double x, double *s, double *c) {
+  const double MAGIC = 6755399441055744.0;  // 1.5 * 2^52: rounds to an integer kept in the low word
+  const double TWO_OVER_PI = 0.63661977236758134308;
+  const double PIO2_HI = 1.5707963267948966192;
+  const double PIO2_LO = 6.123233995736766036e-17;
+  const double t = __fma_rn(x, TWO_OVER_PI, MAGIC);
+  const int n = __double2loint(t);
+  const double nd = t - MAGIC;
+  const double y = __fma_rn(-nd, PIO2_LO, __fma_rn(-nd, PIO2_HI, x));
+  const double y2 = y * y;
+  double sp = __fma_rn(y2, -1.0 / 1307674368000.0, 1.0 / 6227020800.0);  // -1/15!, 1/13!
+  sp = __fma_rn(y2, sp, -1.0 / 39916800.0);                               // -1/11!
+  sp = __fma_rn(y2, sp, 1.0 / 362880.0);                                  // 1/9!
+  sp = __fma_rn(y2, sp, -1.0 / 5040.0);                                   // -1/7!
+  sp = __fma_rn(y2, sp, 1.0 / 120.0);                                     // 1/5!
+  sp = __fma_rn(y2, sp, -1.0 / 6.0);                                      // -1/3!
+  sp = __fma_rn(y2 * y, sp, y);
+  double cp = __fma_rn(y2, 1.0 / 20922789888000.0, -1.0 / 87178291200.0);  // 1/16!, -1/14!
+  cp = __fma_rn(y2, cp, 1.0 / 479001600.0);                                  // 1/12!
+  cp = __fma_rn(y2, cp, -1.0 / 3628800.0);                                   // -1/10!
+  cp = __fma_rn(y2, cp, 1.0 / 40320.0);                                      // 1/8!
+  cp = __fma_rn(y2, cp, -1.0 / 720.0);                                       // -1/6!
+  cp = __fma_rn(y2, cp, 1.0 / 24.0);                                         // 1/4!
+  cp = __fma_rn(y2, cp, -0.5);                                               // -1/2!
+  cp = __fma_rn(y2, cp, 1.0);
+  const double a = (n & 1) ? cp : sp, b = (n & 1) ? sp : cp;
+  *s = (n & 2) ? -a : a;
+  *c = ((n + 1) & 2) ? -b : b;
+}
+
 }  // namespace xns_math
