@@ -358,6 +358,10 @@ def reference_workload_arm(args, rank):
         step = (lambda: R.calc_atoms([blk], 2)) if kind == "reference" else (lambda: R.build_atoms([blk], 2, 1))
         metric, unit, cores = "site pairs/s (structure build)", "pairs/s", 1
         sample = "block::calcAtoms on an atom-list block of %d sites (single-threaded in the reference)" % m
+    elif w == "learned":
+        print(json.dumps({"impl": "reference", "unavailable": "the learned binning correction has no counterpart in the "
+                          "reference; its exact path, calcIntDebye, is timed by --workload debye"}))
+        return 0
     else:
         raise ValueError(w)
     for _ in range(args.warmup):
@@ -991,6 +995,98 @@ def build_workload(args):
     return 0
 
 
+def learned_workload(args):
+    """Config 5, the learned binning correction, at the sizes one bench call can run: training structures
+    from the config-3 generator (fcc crystallites, 5 % substitution, Gaussian displacements) plus 10 %
+    random-packed amorphous clusters with atom counts log-uniform in [--learned-nmin, --learned-nmax]
+    (5k-50k by default; config 5 names 5k-2M), coarse 0.02 A histograms, the MLP trained on the GPU to
+    predict each coarse bin's moments, 2048 q in [0.1, 20); the exact double sum of the held-out
+    structures is the arbiter (tolerance 1e-4, else the exact path is used).  Then the scale case: one
+    fcc sphere of --scale-atoms atoms (1e7 by default), coarse histogram -> I(q) with and without the
+    correction, against the 0.001 A histogram's I(q) (binning error below (q 0.001)^2 / 24 = 1.7e-5 at
+    q = 20): the exact double sum of 5e13 pairs is out of reach (its per-pair +1e-8 histogram updates
+    alone take hours).  Progress on stderr; one JSON line on stdout."""
+    import time
+
+    import xns_b200
+    from xns_b200 import learned, synth
+    T0 = time.perf_counter()
+
+    def say(msg):
+        print("[%7.1f s] %s" % (time.perf_counter() - T0, msg), file=sys.stderr, flush=True)
+
+    ctx = _ctx0()
+    sync = __import__("torch").cuda.synchronize
+    q = synth.q_mesh(0.1, 20.0, 2048)
+    structs, sls = learned.training_structures(args.learned_count, seed=0, nmin=args.learned_nmin,
+                                               nmax=args.learned_nmax)
+    ns = [sum(len(e) for e in st) for st in structs]
+    say("%d training structures, %d-%d atoms" % (len(structs), min(ns), max(ns)))
+    lc = learned.LearnedCorrector(ctx, q, tol=1e-4)
+    t0 = time.perf_counter()
+    lc.fit(structs, sls)
+    fit_s = time.perf_counter() - t0
+    say("fit done: %s" % json.dumps(lc.validation))
+    # throughput of both paths on the same structures (the first 32 of the set)
+    sub, subl = structs[:32], sls[:32]
+    sync()
+    t0 = time.perf_counter()
+    I_c, hs, s0, _ = learned.hist_pass(ctx, sub, subl, q, learned.COARSE_BIN)
+    I_l = lc.corrected(I_c, hs, s0)
+    sync()
+    t_learned = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    I_x = learned.exact_pass(ctx, sub, subl, q)
+    sync()
+    t_exact = time.perf_counter() - t0
+    say("throughput: learned %.3f s, exact %.3f s for %d structures" % (t_learned, t_exact, len(sub)))
+    line = {"metric": "patterns/s", "value": len(sub) / t_learned, "unit": "patterns/s", "n_gpus": 1,
+            "higher_is_better": True, "workload": "learned binning correction (config 5, scaled)",
+            "config": {"structures": len(structs), "atoms_min": int(min(ns)), "atoms_max": int(max(ns)),
+                       "q": "2048 in [0.1, 20)", "coarse_bin": learned.COARSE_BIN, "mlp": "3 layers, width 256, GELU, "
+                       "BF16 weights, FP32 accumulation", "holdout": "12.5 %", "tolerance": 1e-4},
+            "exact_patterns_per_s": len(sub) / t_exact, "learned_vs_exact_speed": t_exact / t_learned,
+            "fit_s": fit_s, "validation": lc.validation, "trusted": bool(lc.trusted),
+            "path_chosen": "learned" if lc.trusted else "exact (the validated error exceeds the tolerance)",
+            "throughput_sample": "%d structures, %d-%d atoms" % (len(sub), min(ns[:32]), max(ns[:32])),
+            "max_rel_err_learned_vs_exact_on_sample": float(learned.max_rel_err(I_l, I_x).max())}
+    if args.scale_atoms > 0:
+        els = synth.fcc_sphere(n=args.scale_atoms, a=3.61, sigma=0.05, seed=5)
+        n = len(els[0])
+        say("scale case: %d atoms" % n)
+
+        def hist_iq(bin):
+            sync()
+            t0 = time.perf_counter()
+            nh = synth.hist_size(els, bin)
+            h = ctx.calc_hist(els, nh, bin)
+            I = ctx.calc_int_1d_hist(h, [n], nh, bin, q, xns_b200.NEUTRON, sl=[1.0])
+            sync()
+            return I, h, nh, time.perf_counter() - t0
+
+        I_c, hc, nh, t_c = hist_iq(learned.COARSE_BIN)
+        say("coarse histogram and I(q): %.1f s" % t_c)
+        h = learned.weighted_hist(els, [1.0], hc, nh)
+        s0 = learned.self_term(els, [1.0])
+        t0 = time.perf_counter()
+        I_lc = I_c + learned.correction(ctx, h, lc._moments_pred(h), q, s0)
+        t_corr = time.perf_counter() - t0
+        unif = np.tile(np.array([[0.0, 1.0 / 12.0]], np.float32), (nh, 1))
+        I_u = I_c + learned.correction(ctx, h, unif, q, s0)
+        I_f, _, _, t_f = hist_iq(0.001)
+        say("0.001 A histogram and I(q): %.1f s" % t_f)
+        line["scale_case"] = {"atoms": n, "pairs": n * (n - 1) // 2, "q_points": len(q),
+                              "coarse_path_s": t_c + t_corr, "fine_path_s": t_f,
+                              "reference": "I(q) from the 0.001 A histogram (binning error < 1.7e-5 at q = 20)",
+                              "max_rel_err_vs_fine": {"coarse": float(learned.max_rel_err(I_c, I_f)),
+                                                      "uniform_bins": float(learned.max_rel_err(I_u, I_f)),
+                                                      "learned": float(learned.max_rel_err(I_lc, I_f))}}
+    lc.close()
+    ctx.close()
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1002,14 +1098,21 @@ def main():
                     help="histogram workload: skip the other configurations' keys (Debye, 2D plane, batch)")
     ap.add_argument("--cells", type=int, default=CELLS,
                     help="cube edge in unit cells (default 30, the benchmark; smaller only for profiler captures)")
-    ap.add_argument("--workload", default="histogram", choices=["histogram", "debye", "2d", "batch", "build"],
+    ap.add_argument("--workload", default="histogram", choices=["histogram", "debye", "2d", "batch", "build",
+                                                                "learned"],
                     help="histogram (default, the headline: rock-salt cube histogram + rPDF + I(q)); debye (fcc "
                          "sphere exact Debye sum), 2d (q plane), batch (ensemble of spheres) and build (structure "
-                         "builder on an atom-list block) run on one GPU")
+                         "builder on an atom-list block) and learned (config 5: the learned binning correction, "
+                         "scaled) run on one GPU")
     ap.add_argument("--batch-count", type=int, default=256, help="batch workload: structures in the ensemble")
     ap.add_argument("--cells2d", type=int, default=63, help="2d workload: crystallite edge in fcc cells (63: 1e6 atoms)")
     ap.add_argument("--mesh2d", type=int, default=1024, help="2d workload: q and phi points")
     ap.add_argument("--build-sites", type=int, default=200000, help="build workload: sites of the atom-list block")
+    ap.add_argument("--learned-count", type=int, default=256, help="learned workload: training structures")
+    ap.add_argument("--learned-nmin", type=int, default=5000, help="learned workload: smallest structure (atoms)")
+    ap.add_argument("--learned-nmax", type=int, default=50000, help="learned workload: largest structure (atoms)")
+    ap.add_argument("--scale-atoms", type=int, default=10000000,
+                    help="learned workload: atoms of the scale case's fcc sphere (0: no scale case)")
     ap.add_argument("--shard", action="store_true",
                     help="histogram workload with N ranks: split one structure over the ranks (strong scaling) "
                          "instead of one structure per rank")
@@ -1025,6 +1128,8 @@ def main():
         return batch_workload(args)
     if args.workload == "build" and args.impl == "ours":
         return build_workload(args)
+    if args.workload == "learned" and args.impl == "ours":
+        return learned_workload(args)
     if args.impl == "reference":
         if args.workload != "histogram":
             return reference_workload_arm(args, rank)
