@@ -193,7 +193,7 @@ int xns_pdf_and_debye_from_hist_device(xns_ctx *ctx, const uint64_t *hist_dev, c
  * loading the library holds until exit.
  * Accuracy: the result is xns_calc_int_1d_hist's quantity computed another way -- an FP32 sine
  * recurrence over the bins with FP64 seeds and FP64 sums (the engine of the exact Debye sum) instead
- * of the integer-digit tensor-core sums -- and agrees with it within 1e-5 relative at every q, the deep
+ * of the FP64 angle-split sums -- and agrees with it within 1e-5 relative at every q, the deep
  * low-q minima of I(q) included (the GPU tests check a 10-cell rock-salt cube at 0.001 A on 4096 q).
  * Limits: at most XNS_NOALLOC_MAX_ELEMENTS elements; at most XNS_NOALLOC_MAX_Q q points on a uniform
  * mesh and XNS_NOALLOC_MAX_Q_NONUNIFORM on any other; and the array must hold, each region rounded up

@@ -76,7 +76,7 @@ def test_noalloc_matches_allocating_entry_point(gpu_ctx):
 def test_noalloc_large_histogram_and_nonuniform_mesh(gpu_ctx, oracle):
     """A 10-cell rock-salt cube at 0.001 A (about 7200 atoms, 3 x 97,000 bins) on 4096 q: the deep
     low-q minima of I(q), where the bin sum cancels to ~1e-5 of its terms, are where an FP32 sum shows.
-    The allocation-free result stays within TOL_I of the allocating entry point (exact integer-digit
+    The allocation-free result stays within TOL_I of the allocating entry point (FP64 angle-split
     sums) and of the oracle, on two calls in a row; then a non-uniform mesh (per-term sines) of 1500 q."""
     import torch
     from xns_b200 import synth
