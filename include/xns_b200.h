@@ -236,11 +236,12 @@ int xns_hist_transform_exact(xns_ctx *ctx, const uint64_t *hist, uint32_t ncols,
 /* The same G in FP64 by angle splitting, the form xns_calc_int_1d_hist and the fused entry points use:
  * each bin distance r_k = R_h + r_l (R_h a multiple of 64 bins), sin(q r_k) = sin(q R_h) cos(q r_l) +
  * cos(q R_h) sin(q r_l), so the bin sum is an FP64 product with K = 64 against per-q tables of 64
- * cosines and sines, and the +1e-8 of the denominator is kept to first order (an FP32 product of the
- * same form; the next order is below 1e-14 of the terms).  No sinc matrix and no cache: every call
- * costs the same.  G carries FP64 rounding (about 1e-13 of its terms).  Scratch: 1.6 KB per q point,
- * at most 48 bytes per bin, and the partial sums (at most 64 bytes per q point and split, about
- * 16 x SMs x 64 / nq splits).  Counts below 2^53. */
+ * cosines and sines, and the +1e-8 of the denominator is kept to first order (sum_k n_k sin(q r_k) / r_k^2
+ * by an FP64 rotation over the bins, per bin below 20 A and in 0.02 A bins beyond, within 5e-12 of the
+ * terms; the next order is below 1e-14 of the terms).  No sinc matrix and no cache: every call costs
+ * the same.  G carries FP64 rounding (about 1e-13 of its terms).  Scratch: 1 KB per q point, at most 32
+ * bytes per bin, 8 bytes per column and bin below 20 A, and the partial sums (at most 32 bytes per q
+ * point and split, about 16 x SMs x 64 / nq splits).  Counts below 2^53. */
 int xns_hist_transform_split(xns_ctx *ctx, const uint64_t *hist, uint32_t ncols, uint32_t nh, double bin,
                              const double *q, uint32_t nq, double *G);
 

@@ -11,20 +11,23 @@
 // so with g_h,l = n(64 h + l) / r_k,
 //   G(q) = sum_h [ sin(q R_h) sum_l g_h,l cos(q r_l) + cos(q R_h) sum_l g_h,l sin(q r_l) ].
 // The inner sums are a product with K = 64 against two tables of 64 cosines and sines per q; the
-// outer weights sin / cos(q R_h) follow h by a rotation.  Per (q, bin, column): two FP64 FMAs for G
-// and two FP32 FMAs for T (the 1e-8 term needs ~1e-3 relative; FP32 sums on the FP32 pipe, beside
-// the FP64 pipe), instead of a sinc value and its digits per element.
+// outer weights sin / cos(q R_h) follow h by a rotation.  Per (q, bin, column): two FP64 FMAs, instead
+// of a sinc value and its digits per element.  T is summed by sinc_eps_kernel (an FP64 rotation over
+// bins) from n / r^2: exactly per bin below EPS_R_FINE, and beyond it in bins of EPS_W (a multiple
+// of the bin) with the phase at the bin centre.  Moving a term's phase by at most EPS_W / 2 changes
+// eps T / q^2 by at most eps EPS_W / (2 EPS_R_FINE) = 5e-12 of the sum's term magnitudes n / (q r).
 //
-// split_sum_kernel: a CTA takes 64 q (the tables, 96 KB, in shared memory) and a range of blocks h;
-// each thread takes 4 q x CB columns and every 16th block of the range.  Partial sums per CTA are
-// reduced over the CTA's threads in a fixed order and over the h ranges by split_reduce_kernel, so
-// the result does not depend on scheduling.
+// split_sum_kernel: a CTA takes 64 q (the tables, 64 KB, in shared memory) and a range of blocks h;
+// each thread takes 4 q x CB columns and every 16th block of the range, each step's 16 blocks of
+// weights staged in shared memory by cp.async (two stages).  Partial sums per CTA are reduced over the
+// CTA's threads in a fixed order and over the h ranges by split_reduce_kernel, so the result does not
+// depend on scheduling.
 #include <string.h>
 
 #include <algorithm>
 #include <vector>
 
-#include "f32x2.cuh"
+#include "sinc_engine.cuh"
 #include "tc_gemm.cuh"
 #include "xmath.cuh"
 #include "xns_internal.cuh"
@@ -39,14 +42,13 @@ constexpr int TQ = 4;     // q per thread
 constexpr int CBMAX = 4;  // columns per pass
 static_assert(SQ == TQ * (ST / SHL), "a CTA's threads cover its q tile");
 
-// Column stride of the G tables: 1, 2 or 4 (three columns are padded to four for 16-byte loads).
-__host__ __device__ constexpr int gstride(int cb) { return cb == 3 ? 4 : cb; }
+// Column stride of the G table: the columns of a pass.
+__host__ __device__ constexpr int gstride(int cb) { return cb; }
 
 // Tables per q tile qt: A64[qt][0][l][j] = cos(q r_l), A64[qt][1][l][j] = sin(q r_l) for q the tile's
-// j-th value (0 past nq), A32 the same rounded to float; qv the padded mesh.
+// j-th value (0 past nq); qv the padded mesh.
 __global__ void split_tables_kernel(const double *__restrict__ qmesh, uint32_t nq, uint32_t nq_pad,
-                                    double bin, double *__restrict__ A64, float *__restrict__ A32,
-                                    double *__restrict__ qv) {
+                                    double bin, double *__restrict__ A64, double *__restrict__ qv) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;  // (q, l) with l fastest
   if (i >= nq_pad * SLO) return;
   const uint32_t iq = i / SLO, l = i % SLO;
@@ -57,33 +59,42 @@ __global__ void split_tables_kernel(const double *__restrict__ qmesh, uint32_t n
   const size_t o = (size_t)(iq / SQ) * 2 * SLO * SQ + (size_t)l * SQ + iq % SQ;
   A64[o] = c;
   A64[o + SLO * SQ] = s;
-  A32[o] = (float)c;
-  A32[o + SLO * SQ] = (float)s;
 }
 
-// G1[k][c] = n_c(k) / r_k and G2[k][c] = n_c(k) / r_k^2 (float) for the columns c0 .. c0 + cb - 1 of
-// this pass, zero past nh and in the padding.
+// G1[k][c] = n_c(k) / r_k for the columns c0 .. c0 + cb - 1 of this pass, zero past nh.
 __global__ void split_weights_kernel(const unsigned long long *__restrict__ hist, size_t ldh, uint32_t c0, uint32_t cb,
-                                     uint32_t gs, uint32_t nh, uint32_t nh_pad, double bin, double *__restrict__ G1,
-                                     float *__restrict__ G2) {
+                                     uint32_t nh, uint32_t nh_pad, double bin, double *__restrict__ G1) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nh_pad) return;
   const double r = (k + 0.5) * bin;
-  for (uint32_t c = 0; c < gs; c++) {
-    const double n = (c < cb && k < nh) ? (double)hist[(size_t)(c0 + c) * ldh + k] : 0.0;
-    const double g = n / r;
-    G1[(size_t)k * gs + c] = g;
-    G2[(size_t)k * gs + c] = (float)(g / r);
+  for (uint32_t c = 0; c < cb; c++) {
+    const double n = k < nh ? (double)hist[(size_t)(c0 + c) * ldh + k] : 0.0;
+    G1[(size_t)k * cb + c] = n / r;
   }
+}
+
+// The +1e-8 histograms: H[c][b] = sum of n_c(k) / r_k^2 over the bins k of [b ratio, (b + 1) ratio)
+// that lie in [k_lo, k_hi), for every column.
+constexpr double EPS_R_FINE = 20.0;  // A: T per bin below this distance
+constexpr double EPS_W = 0.02;       // A: T in bins of at least this width beyond it
+__global__ void split_eps_hist_kernel(const unsigned long long *__restrict__ hist, size_t ldh, uint32_t ncols, uint32_t k_lo,
+                                      uint32_t k_hi, double bin, uint32_t ratio, uint32_t nb, double *__restrict__ H) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;  // (c, b)
+  if (i >= ncols * nb) return;
+  const uint32_t c = i / nb, b = i % nb;
+  double s = 0;
+  for (uint32_t k = max(k_lo, b * ratio); k < min(k_hi, (b + 1) * ratio); k++) {
+    const double r = (k + 0.5) * bin;
+    s += (double)hist[(size_t)c * ldh + k] / (r * r);
+  }
+  H[i] = s;
 }
 
 struct SplitArgs {
   const double *A64;
-  const float *A32;
   const double *G1;
-  const float *G2;
   const double *qv;
-  double *part;  // [split][2][CB][nq_pad]: G sums, then T sums
+  double *part;  // [split][CB][nq_pad]
   uint32_t nhi, nq_pad, nsplit, hi_per_split;
   double blk;  // 64 bin
 };
@@ -95,11 +106,11 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
-// Shared memory of split_sum_kernel: the q tile's tables (FP64 cos, sin; FP32 cos, sin: 96 KB), then two
-// stages of one step's G rows (16 blocks x 64 bins x GS columns, FP64 and FP32).
-__host__ __device__ constexpr size_t split_stage_bytes(int gs) { return (size_t)SHL * SLO * gs * (8 + 4); }
+// Shared memory of split_sum_kernel: the q tile's tables (FP64 cos, sin: 64 KB), then two stages of
+// one step's G rows (16 blocks x 64 bins x GS columns): 112 KB at three columns, two CTAs per SM.
+__host__ __device__ constexpr size_t split_stage_bytes(int gs) { return (size_t)SHL * SLO * gs * 8; }
 __host__ __device__ constexpr size_t split_smem_bytes(int gs) {
-  return (size_t)2 * SLO * SQ * (8 + 4) + 2 * split_stage_bytes(gs);
+  return (size_t)2 * SLO * SQ * 8 + 2 * split_stage_bytes(gs);
 }
 
 // A thread's q: 2g, 2g + 1, 32 + 2g, 33 + 2g of the tile (g = thread % 16), so that the 16 threads of a
@@ -107,45 +118,37 @@ __host__ __device__ constexpr size_t split_smem_bytes(int gs) {
 __device__ __forceinline__ uint32_t split_q(uint32_t g, int t) { return (t < 2 ? 0u : 32u) + 2 * g + (t & 1); }
 
 template <int CB>
-__global__ void __launch_bounds__(ST, 1) split_sum_kernel(SplitArgs a) {
+__global__ void __launch_bounds__(ST, 2) split_sum_kernel(SplitArgs a) {
   constexpr int GS = gstride(CB);
-  constexpr uint32_t G1N = SHL * SLO * GS;  // doubles (and floats) of one step's G rows
+  constexpr uint32_t G1N = SHL * SLO * GS;  // doubles of one step's G rows
   extern __shared__ __align__(16) unsigned char smem[];
   double *c64 = reinterpret_cast<double *>(smem);  // [SLO][SQ] cos, then [SLO][SQ] sin
-  float *c32 = reinterpret_cast<float *>(c64 + 2 * SLO * SQ);
-  double *gs64 = reinterpret_cast<double *>(c32 + 2 * SLO * SQ);  // [stage][G1N]
-  float *gs32 = reinterpret_cast<float *>(gs64 + 2 * G1N);           // [stage][G1N]
+  double *gs64 = c64 + 2 * SLO * SQ;               // [stage][G1N]
   const uint32_t qt = blockIdx.x / a.nsplit, sp = blockIdx.x % a.nsplit;
   const uint32_t hb = sp * a.hi_per_split, he = min(hb + a.hi_per_split, a.nhi);
   const uint32_t nsteps = (he - hb + SHL - 1) / SHL;
-  // one step's G rows: blocks hb + SHL s .. + SHL - 1 are contiguous in the tables; blocks past the
+  // one step's G rows: blocks hb + SHL s .. + SHL - 1 are contiguous in the table; blocks past the
   // last one are not copied (their threads do not read them)
   auto prefetch = [&](uint32_t s, uint32_t stage) {
     const uint32_t h0 = hb + s * SHL, nrow = min((uint32_t)SHL, a.nhi - h0);
-    const uint32_t n1 = nrow * SLO * GS / 2, n2 = nrow * SLO * GS / 4;  // 16-byte pieces
+    const uint32_t n1 = nrow * SLO * GS / 2;  // 16-byte pieces
     const double *g1 = a.G1 + (size_t)h0 * SLO * GS;
-    const float *g2 = a.G2 + (size_t)h0 * SLO * GS;
     double *d1 = gs64 + stage * G1N;
-    float *d2 = gs32 + stage * G1N;
     for (uint32_t i = threadIdx.x; i < n1; i += ST) cp_async16(d1 + 2 * i, g1 + 2 * i);
-    for (uint32_t i = threadIdx.x; i < n2; i += ST) cp_async16(d2 + 4 * i, g2 + 4 * i);
     cp_async_commit();
   };
   if (nsteps) prefetch(0, 0);
-  {  // the tile's tables: 64 KB FP64, 32 KB FP32
+  {  // the tile's tables
     const double2 *src = reinterpret_cast<const double2 *>(a.A64 + (size_t)qt * 2 * SLO * SQ);
     double2 *dst = reinterpret_cast<double2 *>(c64);
     for (uint32_t i = threadIdx.x; i < 2 * SLO * SQ / 2; i += ST) dst[i] = src[i];
-    const float4 *s32 = reinterpret_cast<const float4 *>(a.A32 + (size_t)qt * 2 * SLO * SQ);
-    float4 *d32 = reinterpret_cast<float4 *>(c32);
-    for (uint32_t i = threadIdx.x; i < 2 * SLO * SQ / 4; i += ST) d32[i] = s32[i];
   }
   const uint32_t gq = threadIdx.x % (ST / SHL), hl = threadIdx.x / (ST / SHL);
-  double acc1[TQ][CB], acc2[TQ][CB];
+  double acc[TQ][CB];
 #pragma unroll
   for (int t = 0; t < TQ; t++)
 #pragma unroll
-    for (int c = 0; c < CB; c++) acc1[t][c] = acc2[t][c] = 0.0;
+    for (int c = 0; c < CB; c++) acc[t][c] = 0.0;
   double sH[TQ], cH[TQ], sR[TQ], cR[TQ];
 #pragma unroll
   for (int t = 0; t < TQ; t++) {  // sin / cos(q R_h) at the thread's first block, and the rotation by SHL blocks
@@ -154,7 +157,6 @@ __global__ void __launch_bounds__(ST, 1) split_sum_kernel(SplitArgs a) {
     xns_math::xns_sincos64_acc(q * (SHL * a.blk), &sR[t], &cR[t]);
   }
   const double *cq = c64 + 2 * gq, *sq = c64 + SLO * SQ + 2 * gq;
-  const float *cqf = c32 + 2 * gq, *sqf = c32 + SLO * SQ + 2 * gq;
   for (uint32_t s = 0; s < nsteps; s++) {
     cp_async_wait_all();
     __syncthreads();  // step s's rows have landed; every thread is done with the other stage
@@ -162,17 +164,11 @@ __global__ void __launch_bounds__(ST, 1) split_sum_kernel(SplitArgs a) {
     const uint32_t h = hb + s * SHL + hl;
     if (h < he) {
       double c1[TQ][CB], s1[TQ][CB];
-      xns_f2::f2 c2[TQ / 2][CB], s2[TQ / 2][CB];  // FP32 sums, q pairs (2g, 2g + 1), (32 + 2g, 33 + 2g)
 #pragma unroll
       for (int t = 0; t < TQ; t++)
 #pragma unroll
         for (int c = 0; c < CB; c++) c1[t][c] = s1[t][c] = 0.0;
-#pragma unroll
-      for (int t = 0; t < TQ / 2; t++)
-#pragma unroll
-        for (int c = 0; c < CB; c++) c2[t][c] = s2[t][c] = 0ull;
       const double *g1 = gs64 + (s & 1) * G1N + hl * SLO * GS;
-      const float *g2 = gs32 + (s & 1) * G1N + hl * SLO * GS;
 #pragma unroll 4
       for (int l = 0; l < SLO; l++) {
         const double2 ca = *reinterpret_cast<const double2 *>(cq + l * SQ);
@@ -180,56 +176,21 @@ __global__ void __launch_bounds__(ST, 1) split_sum_kernel(SplitArgs a) {
         const double2 sa = *reinterpret_cast<const double2 *>(sq + l * SQ);
         const double2 sb = *reinterpret_cast<const double2 *>(sq + l * SQ + 32);
         const double cv[TQ] = {ca.x, ca.y, cb.x, cb.y}, sv[TQ] = {sa.x, sa.y, sb.x, sb.y};
-        const xns_f2::f2 cfp[2] = {*reinterpret_cast<const xns_f2::f2 *>(cqf + l * SQ),
-                                   *reinterpret_cast<const xns_f2::f2 *>(cqf + l * SQ + 32)};
-        const xns_f2::f2 sfp[2] = {*reinterpret_cast<const xns_f2::f2 *>(sqf + l * SQ),
-                                   *reinterpret_cast<const xns_f2::f2 *>(sqf + l * SQ + 32)};
-        double g[GS];
-        float gf[GS];
-        if constexpr (GS == 4) {
-          const double2 u = *reinterpret_cast<const double2 *>(g1 + l * GS);
-          const double2 v = *reinterpret_cast<const double2 *>(g1 + l * GS + 2);
-          const float4 w = *reinterpret_cast<const float4 *>(g2 + l * GS);
-          g[0] = u.x;
-          g[1] = u.y;
-          g[2] = v.x;
-          g[3] = v.y;
-          gf[0] = w.x;
-          gf[1] = w.y;
-          gf[2] = w.z;
-          gf[3] = w.w;
-        } else {
+        double g[CB];
 #pragma unroll
-          for (int c = 0; c < GS; c++) {
-            g[c] = g1[l * GS + c];
-            gf[c] = g2[l * GS + c];
-          }
-        }
+        for (int c = 0; c < CB; c++) g[c] = g1[l * GS + c];
 #pragma unroll
-        for (int c = 0; c < CB; c++) {
+        for (int c = 0; c < CB; c++)
 #pragma unroll
           for (int t = 0; t < TQ; t++) {
             c1[t][c] = __fma_rn(cv[t], g[c], c1[t][c]);
             s1[t][c] = __fma_rn(sv[t], g[c], s1[t][c]);
           }
-          const xns_f2::f2 gp = xns_f2::splat(gf[c]);
-#pragma unroll
-          for (int t = 0; t < TQ / 2; t++) {
-            c2[t][c] = xns_f2::fma(cfp[t], gp, c2[t][c]);
-            s2[t][c] = xns_f2::fma(sfp[t], gp, s2[t][c]);
-          }
-        }
       }
 #pragma unroll
-      for (int t = 0; t < TQ; t++) {
+      for (int t = 0; t < TQ; t++)
 #pragma unroll
-        for (int c = 0; c < CB; c++) {
-          acc1[t][c] = __fma_rn(sH[t], c1[t][c], __fma_rn(cH[t], s1[t][c], acc1[t][c]));
-          const float cc = (t & 1) ? xns_f2::hi(c2[t / 2][c]) : xns_f2::lo(c2[t / 2][c]);
-          const float ss = (t & 1) ? xns_f2::hi(s2[t / 2][c]) : xns_f2::lo(s2[t / 2][c]);
-          acc2[t][c] = __fma_rn(sH[t], (double)cc, __fma_rn(cH[t], (double)ss, acc2[t][c]));
-        }
-      }
+        for (int c = 0; c < CB; c++) acc[t][c] = __fma_rn(sH[t], c1[t][c], __fma_rn(cH[t], s1[t][c], acc[t][c]));
     }
 #pragma unroll
     for (int t = 0; t < TQ; t++) {  // on to the thread's next block, SHL blocks on
@@ -238,35 +199,31 @@ __global__ void __launch_bounds__(ST, 1) split_sum_kernel(SplitArgs a) {
       cH[t] = __fma_rn(cH[t], cR[t], -(sv * sR[t]));
     }
   }
-  // reduce over the 16 block lanes in a fixed order: red[hl][which][c][j]
+  // reduce over the 16 block lanes in a fixed order: red[hl][c][j]
   __syncthreads();
   double *red = c64;
 #pragma unroll
   for (int t = 0; t < TQ; t++)
 #pragma unroll
-    for (int c = 0; c < CB; c++) {
-      const uint32_t j = split_q(gq, t);
-      red[((size_t)(hl * 2 + 0) * CB + c) * SQ + j] = acc1[t][c];
-      red[((size_t)(hl * 2 + 1) * CB + c) * SQ + j] = acc2[t][c];
-    }
+    for (int c = 0; c < CB; c++) red[((size_t)hl * CB + c) * SQ + split_q(gq, t)] = acc[t][c];
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < 2 * CB * SQ; i += ST) {  // i = (which * CB + c) * SQ + j
+  for (uint32_t i = threadIdx.x; i < CB * SQ; i += ST) {  // i = c * SQ + j
     double sum = 0;
-    for (int l = 0; l < SHL; l++) sum += red[(size_t)l * 2 * CB * SQ + i];
-    const uint32_t wc = i / SQ, j = i % SQ;
-    a.part[((size_t)sp * 2 * CB + wc) * a.nq_pad + (size_t)qt * SQ + j] = sum;
+    for (int l = 0; l < SHL; l++) sum += red[(size_t)l * CB * SQ + i];
+    const uint32_t c = i / SQ, j = i % SQ;
+    a.part[((size_t)sp * CB + c) * a.nq_pad + (size_t)qt * SQ + j] = sum;
   }
 }
 
-// out_G[c0 + c][iq] and out_T[...] = sums of the parts over the splits, in split order.
+// out_G[c0 + c][iq] = sum of the parts over the splits, in split order.
 __global__ void split_reduce_kernel(const double *__restrict__ part, uint32_t nsplit, uint32_t cb, uint32_t nq,
-                                    uint32_t nq_pad, uint32_t c0, double *__restrict__ outG, double *__restrict__ outT) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;  // (which, c, iq)
-  if (i >= 2 * cb * nq) return;
-  const uint32_t iq = i % nq, wc = i / nq, which = wc / cb, c = wc % cb;
+                                    uint32_t nq_pad, uint32_t c0, double *__restrict__ outG) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;  // (c, iq)
+  if (i >= cb * nq) return;
+  const uint32_t iq = i % nq, c = i / nq;
   double s = 0;
-  for (uint32_t p = 0; p < nsplit; p++) s += part[((size_t)p * 2 * cb + wc) * nq_pad + iq];
-  (which ? outT : outG)[(size_t)(c0 + c) * nq + iq] = s;
+  for (uint32_t p = 0; p < nsplit; p++) s += part[((size_t)p * cb + c) * nq_pad + iq];
+  outG[(size_t)(c0 + c) * nq + iq] = s;
 }
 
 template <int CB>
@@ -292,22 +249,26 @@ int xns_hist_transform_split(xns_ctx *ctx, const unsigned long long *d_hist, uin
   nsplit = std::min<uint32_t>(nsplit, std::max<uint32_t>(1, nhi / SHL));
   const uint32_t hps = (nhi + nsplit - 1) / nsplit;
   nsplit = (nhi + hps - 1) / hps;
+  // the +1e-8 histograms: per bin below k_fine (EPS_R_FINE), in bins of ratio bins (EPS_W) above it
+  const uint32_t ratio = std::max<uint32_t>(1, (uint32_t)std::ceil(EPS_W / bin - 1e-9));
+  const uint32_t neps = (nh + ratio - 1) / ratio;
+  const uint32_t k_fine = std::min(nh, std::min(neps * ratio, ((uint32_t)std::ceil(EPS_R_FINE / bin) + ratio - 1) / ratio * ratio));
   auto up = [](size_t b) { return (b + 255) / 256 * 256; };
-  const size_t bA64 = up(sizeof(double) * (size_t)nqt * 2 * SLO * SQ), bA32 = up(sizeof(float) * (size_t)nqt * 2 * SLO * SQ);
-  const size_t bqv = up(sizeof(double) * nq_pad), bG1 = up(sizeof(double) * (size_t)nh_pad * gsmax);
-  const size_t bG2 = up(sizeof(float) * (size_t)nh_pad * gsmax), bpart = up(sizeof(double) * (size_t)nsplit * 2 * cbmax * nq_pad);
-  const size_t bq = up(sizeof(double) * nq);
+  const size_t bA64 = up(sizeof(double) * (size_t)nqt * 2 * SLO * SQ), bqv = up(sizeof(double) * nq_pad);
+  const size_t bG1 = up(sizeof(double) * (size_t)nh_pad * gsmax), bpart = up(sizeof(double) * (size_t)nsplit * cbmax * nq_pad);
+  const size_t bq = up(sizeof(double) * nq), beps = up(sizeof(double) * (size_t)ncols * neps);
+  const size_t bfine = up(sizeof(double) * (size_t)ncols * std::max<uint32_t>(k_fine, 1));
   void *base;
   int st;
-  if ((st = xns_scratch(ctx, SLOT_SPLIT, bA64 + bA32 + bqv + bG1 + bG2 + bpart + bq, &base))) return st;
+  if ((st = xns_scratch(ctx, SLOT_SPLIT, bA64 + bqv + bG1 + bpart + bq + beps + bfine, &base))) return st;
   char *p = (char *)base;
   double *A64 = (double *)p;
-  float *A32 = (float *)(p += bA64);
-  double *qv = (double *)(p += bA32);
+  double *qv = (double *)(p += bA64);
   double *G1 = (double *)(p += bqv);
-  float *G2 = (float *)(p += bG1);
-  double *part = (double *)(p += bG2);
+  double *part = (double *)(p += bG1);
   double *dqm = (double *)(p += bpart);
+  double *heps = (double *)(p += bq);
+  double *hfine = (double *)(p += beps);
   {  // the q values as given (not a fitted uniform mesh)
     void *h;
     if ((st = xns_pinned(ctx, sizeof(double) * nq, &h))) return st;
@@ -315,17 +276,16 @@ int xns_hist_transform_split(xns_ctx *ctx, const unsigned long long *d_hist, uin
     memcpy(h, q, sizeof(double) * nq);
     XNS_CUDA(ctx, cudaMemcpyAsync(dqm, h, sizeof(double) * nq, cudaMemcpyHostToDevice, ctx->stream));
   }
-  split_tables_kernel<<<(nq_pad * SLO + 255) / 256, 256, 0, ctx->stream>>>(dqm, nq, nq_pad, bin, A64, A32, qv);
+  split_tables_kernel<<<(nq_pad * SLO + 255) / 256, 256, 0, ctx->stream>>>(dqm, nq, nq_pad, bin, A64, qv);
   XNS_LAUNCHED(ctx);
   for (uint32_t c0 = 0; c0 < ncols; c0 += CBMAX) {
-    const uint32_t cb = std::min<uint32_t>(CBMAX, ncols - c0), gs = gstride(cb);
-    split_weights_kernel<<<(nh_pad + 255) / 256, 256, 0, ctx->stream>>>(d_hist, ldh, c0, cb, gs, nh, nh_pad, bin, G1, G2);
+    const uint32_t cb = std::min<uint32_t>(CBMAX, ncols - c0);
+    split_weights_kernel<<<(nh_pad + 255) / 256, 256, 0, ctx->stream>>>(d_hist + (size_t)c0 * ldh, ldh, 0, cb, nh, nh_pad,
+                                                                        bin, G1);
     XNS_LAUNCHED(ctx);
     SplitArgs a;
     a.A64 = A64;
-    a.A32 = A32;
     a.G1 = G1;
-    a.G2 = G2;
     a.qv = qv;
     a.part = part;
     a.nhi = nhi;
@@ -342,7 +302,26 @@ int xns_hist_transform_split(xns_ctx *ctx, const unsigned long long *d_hist, uin
     }
     if (st) return st;
     XNS_LAUNCHED(ctx);
-    split_reduce_kernel<<<(2 * cb * nq + 255) / 256, 256, 0, ctx->stream>>>(part, nsplit, cb, nq, nq_pad, c0, d_G, d_T);
+    split_reduce_kernel<<<(cb * nq + 255) / 256, 256, 0, ctx->stream>>>(part, nsplit, cb, nq, nq_pad, c0, d_G);
+    XNS_LAUNCHED(ctx);
+  }
+  // T (sinc_eps_kernel adds into a zeroed T): per bin below k_fine, in the coarse bins above it
+  XNS_CUDA(ctx, cudaMemsetAsync(d_T, 0, sizeof(double) * ncols * nq, ctx->stream));
+  if (k_fine) {
+    split_eps_hist_kernel<<<(ncols * k_fine + 255) / 256, 256, 0, ctx->stream>>>(d_hist, ldh, ncols, 0, k_fine, bin, 1,
+                                                                               k_fine, hfine);
+    XNS_LAUNCHED(ctx);
+    dim3 eg((nq + 127) / 128, (k_fine + xns_sinc::EPS_RUN - 1) / xns_sinc::EPS_RUN, ncols);
+    xns_sinc::sinc_eps_kernel<<<eg, 128, 0, ctx->stream>>>(hfine, k_fine, bin, 0.0, 0.0, dqm, nq, d_T);
+    XNS_LAUNCHED(ctx);
+  }
+  if (k_fine < nh) {
+    split_eps_hist_kernel<<<(ncols * neps + 255) / 256, 256, 0, ctx->stream>>>(d_hist, ldh, ncols, k_fine, nh, bin, ratio,
+                                                                             neps, heps);
+    XNS_LAUNCHED(ctx);
+    // (the coarse bins below k_fine hold nothing)
+    dim3 eg((nq + 127) / 128, (neps + xns_sinc::EPS_RUN - 1) / xns_sinc::EPS_RUN, ncols);
+    xns_sinc::sinc_eps_kernel<<<eg, 128, 0, ctx->stream>>>(heps, neps, ratio * bin, 0.0, 0.0, dqm, nq, d_T);
     XNS_LAUNCHED(ctx);
   }
   XNS_CUDA(ctx, cudaGetLastError());
