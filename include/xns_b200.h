@@ -70,6 +70,13 @@ int xns_set_memory_limit(xns_ctx *ctx, uint64_t bytes);
  * ("a pipeline wait ran out of time"); the context stays usable and the following calls run
  * normally.  Affects one call.  No counterpart in the reference. */
 int xns_inject_pipeline_stall(xns_ctx *ctx, uint64_t wait_limit_ns);
+/* Path of the exact Debye double sum (xns_calc_int_debye, xns_calc_int_partial_debye and their
+ * shards) on a uniform q mesh: on (the default), the integer tensor cores (terms as 8-bit digit products
+ * summed exactly in tensor memory, then in FP64) whenever the largest pair distance is at most 256
+ * times the smallest nonzero one; off, or outside that range or on a mesh that is not uniform, the
+ * FP32 sine recurrence on the FMA pipe.  Both agree with the reference within its tolerance; the
+ * tensor-core path is the more accurate and the faster.  No counterpart in the reference. */
+int xns_debye_tensor_cores(xns_ctx *ctx, int on);
 /* Device time of the most recent call's kernels, in milliseconds (CUDA events). */
 double xns_last_kernel_ms(const xns_ctx *ctx);
 /* Number of kernels the library launched since the context was created. */

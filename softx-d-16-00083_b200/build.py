@@ -25,7 +25,7 @@ NVCC_FLAGS = GENCODE + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                         "-Xptxas", "-warn-spills"]
 
 HOST_SOURCES = ["writers.cpp"]  # host-only parts of the library, in host/
-SOURCES = ["context.cu", "schedule.cu", "hist.cu", "sinc_engine.cu", "debye.cu", "hist_iq.cu", "hist_split.cu", "pdf.cu",
+SOURCES = ["context.cu", "schedule.cu", "hist.cu", "sinc_engine.cu", "debye.cu", "debye_tc.cu", "hist_iq.cu", "hist_split.cu", "pdf.cu",
            "amp2d.cu", "noalloc.cu", "tc_gemm.cu", "tc_exact.cu", "batch.cu", "mlp.cu", "learned.cu", "builder.cu",
            "rearrange.cu"]
 

@@ -278,6 +278,12 @@ int xns_inject_pipeline_stall(xns_ctx *ctx, uint64_t wait_limit_ns) {
   return XNS_OK;
 }
 
+int xns_debye_tensor_cores(xns_ctx *ctx, int on) {
+  if (!ctx) return XNS_ERR_ARG;
+  ctx->debye_tc = on != 0;
+  return XNS_OK;
+}
+
 double xns_last_kernel_ms(const xns_ctx *ctx) { return ctx ? ctx->last_ms : 0; }
 
 uint64_t xns_kernel_launches(const xns_ctx *ctx) { return ctx ? ctx->launches : 0; }

@@ -15,6 +15,15 @@
 
 using namespace xns_sinc;
 
+namespace xns_sinc {
+// debye_tc.cu: the pair sums on the integer tensor cores into SLOT_PARTIAL ([grid][ncls][nq], grid in
+// *grid_out) and the +1e-8 sums into SLOT_EPS_T; *used false (and nothing queued) when the mesh or the
+// distances do not suit it.
+int debye_tc(xns_ctx *ctx, const DevCoords &dc, const std::vector<Segment> &sa, const std::vector<Segment> &sb,
+             const std::vector<uint32_t> &cls, const std::vector<uint32_t> &same, uint32_t ncls, double q0, double dq,
+             uint32_t nq, double rmax, uint32_t shard, uint32_t nshard, bool *used, int *grid_out);
+}  // namespace xns_sinc
+
 namespace {
 
 constexpr int DB_TI = 8, DB_TJ = 48;
@@ -110,9 +119,26 @@ static int debye_device(xns_ctx *ctx, const DevCoords &dc, uint32_t nblocks, con
           cls.push_back(part * P + t);
           same.push_back(a == b && u == v);
         }
+  int st;
+  if ((st = xns_stage_begin(ctx, STAGE_DEBYE))) return st;
+  {
+    double q0 = 0, dq = 0;
+    if (ctx->debye_tc && xns_uniform_mesh(q, nq, &q0, &dq)) {
+      bool used = false;
+      int tgrid = 1;
+      if ((st = debye_tc(ctx, dc, sa, sb, cls, same, nparts * P, q0, dq, nq, rmax, shard, nshard, &used, &tgrid)))
+        return st;
+      if (used) {
+        if ((st = sinc_epilogue(ctx, tgrid, nparts * P, nel, nblocks, n_el_block, q, nq, true, q0, dq, d_w, dc.ntot, polar,
+                                lambda, d_out, (const double *)ctx->slot_ptr[SLOT_PARTIAL], true, shard == 0,
+                                (const double *)ctx->slot_ptr[SLOT_EPS_T])))
+          return st;
+        return xns_stage_end(ctx, STAGE_DEBYE);
+      }
+    }
+  }
   std::vector<SegPair> sched;
   unsigned long long ntiles = xns_build_schedule(sa, sb, cls, same, DB_TI, DB_TJ, &sched);
-  int st;
   SegPair *d_sp = nullptr;
   if (ntiles && (st = xns_upload_schedule(ctx, sched, &d_sp))) return st;
   double q0 = 0, dq = 0;
@@ -128,7 +154,7 @@ static int debye_device(xns_ctx *ctx, const DevCoords &dc, uint32_t nblocks, con
   if (!uniform && (st = sinc_upload_q(ctx, q, nq, &p.q))) return st;
   AtomPairSrc src{dc.x, dc.y, dc.z, d_sp, (int)sched.size()};
   int grid = 0;
-  if ((st = xns_stage_begin(ctx, STAGE_DEBYE))) return st;
+  if ((st = xns_stage_begin(ctx, STAGE_DEBYE))) return st;  // (again: the sinc engine's stage alone)
   if ((st = run_sinc(ctx, p, src, sizeof(double) * 3 * (DB_TI + DB_TJ), uniform, rmax, &grid))) return st;
   if ((st = sinc_epilogue(ctx, grid, p.ncls, nel, nblocks, n_el_block, q, nq, uniform, q0, dq, d_w, dc.ntot, polar, lambda,
                           d_out, nullptr, true, shard == 0, (const double *)ctx->slot_ptr[SLOT_EPS_T])))

@@ -64,6 +64,7 @@ struct xns_ctx {
   size_t slot_size[SLOT_COUNT] = {};
   size_t mem_limit = 0;  // cap on the sum of slot_size (0: none), xns_set_memory_limit
   unsigned long long inject_stall_ns = 0;  // xns_inject_pipeline_stall: consumed by the next digit GEMM
+  bool debye_tc = true;                    // xns_debye_tensor_cores: the Debye sum on the integer tensor cores
   void *pinned = nullptr;  // pinned host staging
   size_t pinned_size = 0;
   // the sinc matrix held in SLOT_TC_A was built for this q mesh, bin width and K extent

@@ -52,6 +52,7 @@ def _declare(lib):
     lib.xns_set_stream.argtypes = [_p, _p]
     lib.xns_set_memory_limit.argtypes = [_p, C.c_uint64]
     lib.xns_inject_pipeline_stall.argtypes = [_p, C.c_uint64]
+    lib.xns_debye_tensor_cores.argtypes = [_p, _int]
     lib.xns_last_kernel_ms.argtypes = [_p]
     lib.xns_last_kernel_ms.restype = _dbl
     lib.xns_kernel_launches.argtypes = [_p]
@@ -319,6 +320,11 @@ class Context:
     def inject_pipeline_stall(self, wait_limit_ns):
         """Failure-path test: the next tensor-core transform's waits run out (see the header)."""
         self._check(lib.xns_inject_pipeline_stall(self._h, int(wait_limit_ns)))
+
+    def debye_tensor_cores(self, on):
+        """Path of the exact Debye sum on a uniform q mesh: the integer tensor cores (True, the default)
+        or the FP32 sine recurrence (False); see the header."""
+        self._check(lib.xns_debye_tensor_cores(self._h, int(bool(on))))
 
     def set_memory_limit(self, nbytes):
         """Caps the calc functions' device scratch in this context (0: no cap); a call that would need
