@@ -647,13 +647,17 @@ def debye_measure(ctx, steps, warmup):
     achieved = 4.0 * pairs * len(q) / (kms * 1e-3) / 1e12
     line = {"metric": "atom-pairs/s", "value": pairs / (ms * 1e-3), "unit": "pairs/s", "n_gpus": 1, "steps": steps,
             "warmup": warmup, "ms_per_step": ms, "kernel_ms": kms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 terms (f64 seeds), f64 reductions", "data": "synthetic (seeded)",
+            "vs_baseline": None, "data": "synthetic (seeded)",
+            "dtype": "int8 digit products on the tensor cores (sin/cos of coarse q: 3 digits; offsets x r_min/r: 4), "
+                     "exact int32 sums, f64 reductions",
             "patterns_per_s": 1e3 / ms,
             "config": {"workload": "exact Debye, fcc sphere 5000 atoms a=4.078 A sigma=0.05 A, neutron, 1024 q in [0.1,10)",
                        "pairs_per_step": pairs, "nq": len(q), "l2": "flushed (512 MB write) before every timed step"},
-            "roofline": {"kernel": "sinc_tiles_kernel<AtomPairSrc>", "bound": "fp32", "achieved": achieved, "peak": p32,
+            "roofline": {"kernel": "debye_tc_kernel (tcgen05 kind::i8)", "bound": "fp32-equivalent: 4 flops per (pair, q) "
+                         "term against the FP32 peak, the measure of the FP32 sine recurrence it replaces",
+                         "achieved": achieved, "peak": p32,
                          "unit": "TFLOP/s", "frac": achieved / p32, "traffic": None, "flops_per_term": 4,
-                         "time": "kernel-only stage (sinc kernel, +1e-8 kernel, epilogue)",
+                         "time": "kernel-only stage (closest-pair pass, tensor-core kernel, +1e-8 kernel, epilogue)",
                          "peak_source": "measured in-process (FFMA loop, xns_measure_fma_peak)"},
             "e2e": {"value": pairs / (ms * 1e-3), "unit": "pairs/s", "ms_per_step": ms, "h2d_bytes_per_step": n * 24 + 8 * 1024,
                     "d2h_bytes_per_step": 8 * 1024},

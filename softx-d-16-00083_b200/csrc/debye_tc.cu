@@ -29,8 +29,8 @@
 // alternate units, each group into its own stage: lane l of the group's warp w writes records
 // 4l .. 4l + 3 of A rows PA w .. PA w + PA - 1 (and 64 + ...) and B rows 2w, 2w + 1 (and 16 + ...), one
 // 32-bit store per (row, digit plane) into the 128-byte-swizzled K-major stage.  Waits are bounded
-// (tc_ptx.cuh); the record warps and each generator group share a named barrier per unit, behind a
-// single bounded waiter.
+// (tc_ptx.cuh): record and generator threads each wait on the mbarriers themselves, and the drain warps
+// share a named barrier behind a single bounded waiter.
 #include <math.h>
 #include <string.h>
 
@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(DT_THREADS, 1) debye_tc_kernel(const DtArgs g)
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) unsigned long long bars[2 * DT_STAGES + 5 + 2 * DT_NREC];
   __shared__ uint32_t tmem_sh;
-  __shared__ int abort_sh, gen_stop[DT_GROUPS], rec_stop, drain_stop;
+  __shared__ int abort_sh, drain_stop;
   const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
   uint8_t *gsm = smem_raw + (base - smem_u32(smem_raw));
   RecTab *rec = reinterpret_cast<RecTab *>(gsm + DT_STAGES * DT_STAGE);
@@ -197,8 +197,6 @@ __global__ void __launch_bounds__(DT_THREADS, 1) debye_tc_kernel(const DtArgs g)
       mbar_init(rempty0 + 8 * b, 32 * DT_GEN);  // every thread of the consuming generator group
     }
     abort_sh = 0;
-    gen_stop[0] = gen_stop[1] = 0;
-    rec_stop = 0;
     drain_stop = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -401,19 +399,14 @@ __global__ void __launch_bounds__(DT_THREADS, 1) debye_tc_kernel(const DtArgs g)
         const uint32_t kb = (uint32_t)fmin(r * g.eps_inv_bw, (double)(g.eps_nb - 1));
         atomicAdd(g.eps_hist + (size_t)cls * g.eps_nb + kb, ir * ir);
       }
-      // one bounded wait until the generator group has read the table's previous unit, then the record
-      // warps' barrier (the stop flag is read after it)
-      if (kr == 0) {
-        bool ok = !*abort;
-        if (ok && p > 0) ok = mbar_wait(rempty0 + 8 * b, (p - 1) & 1u, abort, g.wait_ns);
-        if (!ok) {
-          abort_sh = 1;
-          atomicOr(g.err, 1);
-          rec_stop = 1;
-        }
+      // wait (bounded) until the generator group has read the table's previous unit
+      bool ok = !*abort;
+      if (ok && p > 0) ok = mbar_wait(rempty0 + 8 * b, (p - 1) & 1u, abort, g.wait_ns);
+      if (!ok) {
+        abort_sh = 1;
+        atomicOr(g.err, 1);
+        break;
       }
-      asm volatile("bar.sync 3, %0;" ::"n"(32 * DT_REC) : "memory");
-      if (rec_stop) break;
       RecTab &R = rec[b];
       R.E0[ks] = e0;
       R.W1[ks] = w1;
@@ -445,23 +438,16 @@ __global__ void __launch_bounds__(DT_THREADS, 1) debye_tc_kernel(const DtArgs g)
     for (unsigned long long u = u0 + G, iu = G; u < u1; u += DT_GROUPS, iu += DT_GROUPS) {
       const uint32_t b = (uint32_t)(iu % DT_NREC), p = (uint32_t)(iu / DT_NREC);
       const uint32_t s = (uint32_t)(iu % DT_STAGES), k = (uint32_t)(iu / DT_STAGES);  // stage, its use
-      // one bounded wait for the stage and the unit's record table, then the group's barrier (the stop
-      // flag is read after it)
-      if (t == 0) {
-        bool ok = !*abort;
-        if (ok && k > 0) ok = mbar_wait(empty0 + 8 * s, (k - 1) & 1u, abort, g.wait_ns);
-        if (ok) ok = mbar_wait(rfull0 + 8 * b, p & 1u, abort, g.wait_ns);
-        if (!ok) {
-          abort_sh = 1;
-          atomicOr(g.err, 1);
-          gen_stop[G] = 1;
-        }
+      // every thread waits (bounded) for the stage and the unit's record table itself: the group's warps
+      // run ahead of one another as far as the stages allow, and a wait that runs out stops them all
+      bool ok = !*abort;
+      if (ok && k > 0) ok = mbar_wait(empty0 + 8 * s, (k - 1) & 1u, abort, g.wait_ns);
+      if (ok) ok = mbar_wait(rfull0 + 8 * b, p & 1u, abort, g.wait_ns);
+      if (!ok) {
+        abort_sh = 1;
+        atomicOr(g.err, 1);
+        break;
       }
-      asm volatile("bar.sync %0, %1;" ::"r"(1 + G), "n"(32 * DT_GEN) : "memory");
-      if (gen_stop[G]) break;
-      // the table's phase is complete (its next one needs this group's arrivals): the test acquires the
-      // record warps' writes in this thread
-      if (!mbar_test(rfull0 + 8 * b, p & 1u)) atomicOr(g.err, 1);
       const RecTab &R = rec[b];
       uint8_t *st = gsm + s * DT_STAGE;
       // A: rows 8 gw + a (sin) and 64 + 8 gw + a (cos), records 4 l + c
