@@ -95,8 +95,7 @@ struct DtArgs {
   uint32_t PA;             // coarse points per generator warp (8 PA <= 64; A rows past 8 PA are zero)
   double q0, dq;
   uint32_t nq, ncls;
-  double rmin;             // B scale: s = rmin / r
-  double unit;             // one unit of the level sum, in sin(q r) / r
+  const unsigned long long *dmin2;  // the closest pair's squared distance (FP64 bits): B scale s = r_min / r
   double *out;             // [grid][ncls][nq], zeroed: each CTA's sums in its own slice
   double *cbuf;            // [grid][128][16]: each CTA's row sums at a segment's end
   double *eps_hist;        // the +1e-8 histogram [ncls][eps_nb] (null: not kept)
@@ -210,6 +209,15 @@ __global__ void __launch_bounds__(DT_THREADS, 1) debye_tc_kernel(const DtArgs g)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tmem_sh;
+  // r_min from the closest-pair pass (read on the device: no round trip through the host); one unit of
+  // the level sum (levels i + j <= 3, N_A N_B / 2^16) with A = N_A / (127 2^16), B = N_B / (127 2^24)
+  // and S = sum A B / r_min
+  double rmin;
+  {
+    const double m2 = __longlong_as_double((long long)*g.dmin2);
+    rmin = (m2 > 0.0 && m2 < INFINITY) ? sqrt(m2) * (1.0 - 1e-12) : 1.0;
+  }
+  const double unit = 1.0 / (127.0 * 127.0 * 16777216.0 * rmin);
   const unsigned long long units = g.ntp * g.MT;
   const unsigned long long u0 = units * blockIdx.x / gridDim.x, u1 = units * (blockIdx.x + 1) / gridDim.x;
 
@@ -341,7 +349,7 @@ __global__ void __launch_bounds__(DT_THREADS, 1) debye_tc_kernel(const DtArgs g)
             const uint32_t a = (k - k0) / span;
             const int b = (int)((k - k0) % span) - (int)g.H, bb = b < 0 ? -b : b;
             const double csc = cb[a * 16 + bb], ccs = cb[(DT_QA + a) * 16 + bb];
-            o[k] += (csc + (b < 0 ? -ccs : ccs)) * g.unit;
+            o[k] += (csc + (b < 0 ? -ccs : ccs)) * unit;
           }
           asm volatile("bar.sync 4, 128;" ::: "memory");  // before the next segment rewrites the scratch
         }
@@ -415,7 +423,7 @@ __global__ void __launch_bounds__(DT_THREADS, 1) debye_tc_kernel(const DtArgs g)
       R.F[0][ks] = f1;
       R.F[1][ks] = f2;
       R.F[2][ks] = f4;
-      R.s[ks] = g.rmin * ir;
+      R.s[ks] = rmin * ir;
       mbar_arrive(rfull0 + 8 * b);
     }
   } else {
@@ -571,6 +579,25 @@ __global__ void debye_tc_rmin_kernel(const DtArgs g, unsigned long long *dmin) {
   if (lane == 0 && m < INFINITY) atomicMin(dmin, (unsigned long long)__double_as_longlong(m));
 }
 
+// Adds the slices 1 .. grid - 1 of p ([grid][n]) to slice 0 in a fixed order: warp w of a block sums
+// the slices 1 + w, 9 + w, ... of 32 consecutive entries, then the block adds the warps' sums in order.
+__global__ void __launch_bounds__(256) slice_sum_kernel(double *__restrict__ p, uint32_t grid, size_t n) {
+  __shared__ double part[8][32];
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const size_t i = (size_t)blockIdx.x * 32 + lane;
+  double s = 0.0;
+  if (i < n)
+    for (uint32_t c = 1 + w; c < grid; c += 8) s += p[(size_t)c * n + i];
+  part[w][lane] = s;
+  __syncthreads();
+  if (w == 0 && i < n) {
+    double t = p[i];
+#pragma unroll
+    for (int k = 0; k < 8; k++) t += part[k][lane];
+    p[i] = t;
+  }
+}
+
 }  // namespace
 
 namespace xns_sinc {
@@ -619,31 +646,25 @@ int debye_tc(xns_ctx *ctx, const DevCoords &dc, const std::vector<Segment> &sa, 
   g.nq = nq;
   g.ncls = ncls;
   // the smallest distance of the whole structure (every shard) sets the B scale: every shard then writes
-  // each term with the same digits, and the shards add up to the one-call sums
-  double rmin = 0;
+  // each term with the same digits, and the shards add up to the one-call sums.  The kernel reads it on
+  // the device; the host checks it once the work is queued (a structure with r_max > 256 r_min, where B
+  // would lose more than 8 bits, then takes the sinc engine instead)
+  void *df;
+  if ((st = xns_scratch(ctx, SLOT_FLAGS, 64, &df))) return st;
+  unsigned long long *d_min = (unsigned long long *)df;
+  int *d_err = (int *)((char *)df + 16);
+  XNS_CUDA(ctx, cudaMemsetAsync(d_min, 0x7f, sizeof(unsigned long long), ctx->stream));
+  XNS_CUDA(ctx, cudaMemsetAsync(d_err, 0, sizeof(int), ctx->stream));
   if (ntp) {
-    void *d;
-    if ((st = xns_scratch(ctx, SLOT_FLAGS, 64, &d))) return st;
-    unsigned long long *d_min = (unsigned long long *)d, h_min = 0;
-    XNS_CUDA(ctx, cudaMemsetAsync(d_min, 0x7f, sizeof(unsigned long long), ctx->stream));
     DtArgs ga = g;
     ga.shard = 0;
     ga.nshard = 1;
     ga.ntp = ntp_all;
-    debye_tc_rmin_kernel<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(ga, d_min);
+    debye_tc_rmin_kernel<<<ctx->num_sms * 16, 256, 0, ctx->stream>>>(ga, d_min);
     XNS_LAUNCHED(ctx);
-    XNS_CUDA(ctx, cudaMemcpyAsync(&h_min, d_min, sizeof(h_min), cudaMemcpyDeviceToHost, ctx->stream));
-    XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    double m2;
-    memcpy(&m2, &h_min, sizeof m2);
-    if (!(m2 > 0) || !std::isfinite(m2)) return XNS_OK;  // no pair counts: the sinc engine's path
-    rmin = sqrt(m2) * (1.0 - 1e-12);
-    if (rmax > 256.0 * rmin) return XNS_OK;  // B digits would lose more than 8 bits: the sinc engine
   }
-  g.rmin = rmin;
-  // one unit of the level sum (levels i + j <= 3, N_A N_B / 2^16): A = N_A / (127 2^16),
-  // B = N_B / (127 2^24), S = sum A B / r_min
-  g.unit = 1.0 / (127.0 * 127.0 * 16777216.0 * (rmin > 0 ? rmin : 1.0));
+  g.dmin2 = d_min;
+  g.err = d_err;
   // one CTA per SM; each CTA's sums in its own slice (summed in order by the epilogue), then its scratch
   const unsigned long long units = ntp * MT;
   const unsigned grid = (unsigned)std::max<unsigned long long>(1, std::min<unsigned long long>((unsigned long long)ctx->num_sms, units));
@@ -662,9 +683,6 @@ int debye_tc(xns_ctx *ctx, const DevCoords &dc, const std::vector<Segment> &sa, 
   if ((st = xns_scratch(ctx, SLOT_EPS_HIST, hb, &d))) return st;
   XNS_CUDA(ctx, cudaMemsetAsync(d, 0, hb, ctx->stream));
   g.eps_hist = (double *)d;
-  if ((st = xns_scratch(ctx, SLOT_FLAGS, 64, &d))) return st;
-  XNS_CUDA(ctx, cudaMemsetAsync(d, 0, sizeof(int), ctx->stream));
-  g.err = (int *)d;
   g.wait_ns = WAIT_LIMIT_NS;
   if (ntp) {
     static bool attr_set[XNS_MAX_DEVICES] = {};
@@ -682,11 +700,25 @@ int debye_tc(xns_ctx *ctx, const DevCoords &dc, const std::vector<Segment> &sa, 
   dim3 eg((nq + 127) / 128, (enb + EPS_RUN - 1) / EPS_RUN, ncls);
   sinc_eps_kernel<<<eg, 128, 0, ctx->stream>>>(g.eps_hist, enb, ebin, q0, dq, nullptr, nq, (double *)d);
   XNS_LAUNCHED(ctx);
+  // the CTAs' slices into slice 0, in a fixed order
+  if (grid > 1) {
+    const size_t n = (size_t)ncls * nq;
+    slice_sum_kernel<<<(unsigned)((n + 31) / 32), 256, 0, ctx->stream>>>(g.out, grid, n);
+    XNS_LAUNCHED(ctx);
+  }
   int herr = 0;
-  XNS_CUDA(ctx, cudaMemcpyAsync(&herr, g.err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  unsigned long long h_min = 0;
+  XNS_CUDA(ctx, cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  XNS_CUDA(ctx, cudaMemcpyAsync(&h_min, d_min, sizeof(h_min), cudaMemcpyDeviceToHost, ctx->stream));
   XNS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   if (herr) return xns_fail(ctx, XNS_ERR_CUDA, "Debye: a tensor-core pipeline wait ran out");
-  *grid_out = (int)grid;
+  if (ntp) {
+    double m2;
+    memcpy(&m2, &h_min, sizeof m2);
+    if (!(m2 > 0) || !std::isfinite(m2)) return XNS_OK;          // no pair counts: the sinc engine's path
+    if (rmax > 256.0 * sqrt(m2) * (1.0 - 1e-12)) return XNS_OK;  // B would lose more than 8 bits
+  }
+  *grid_out = 1;
   *used = true;
   return XNS_OK;
 }
