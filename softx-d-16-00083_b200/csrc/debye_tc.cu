@@ -8,24 +8,24 @@
 // The mesh is split into coarse points Q_a = q_{c_a}, c_a = a (2H + 1) + H, and offsets q_b = b dq,
 // |b| <= H, so that sin((Q_a +- q_b) r) = sin(Q_a r) cos(q_b r) +- cos(Q_a r) sin(q_b r).  Per pair
 // record r (the K dimension of a GEMM):
-//   A (128 rows): sin(Q_a r) for 64 coarse points, then cos(Q_a r);
+//   A (128 rows): sin(Q_a r) for up to 64 coarse points, then cos(Q_a r) (rows of unused points zero);
 //   B (32 rows):  cos(q_b r) s(r) for b = 0..15, then sin(q_b r) s(r), s(r) = r_min / r <= 1
 //                 (rows of offsets past H are zero);
 // C = A B^T summed over records gives C_sc (sin rows x cos columns) and C_cs (cos rows x sin columns),
 // and S(Q_a +- q_b) = (C_sc +- C_cs) / r_min.  Both operands are written as 8-bit digits (A:
 // round(127 v 2^16) in three, the top one signed; B: round(127 v 2^24) in four signed ones).  The four B digit
-// planes lie one after another, which makes them one 128-row operand: one MMA per A digit plane and
-// K step (N = 128) multiplies that plane by all four B planes exactly into int32 tensor-memory
-// accumulators, and the drain warps combine the twelve digit products by level in FP64 every DT_CH
-// units.  Every term is thus carried to ~6e-8 (A) and 2^-31 r / r_min (B) of its size and summed in
+// planes lie one after another, which makes them one 128-row operand: one MMA per A digit plane i and
+// K step (N = 128, 96, 64: B planes 0 .. 3 - i) multiplies exactly into int32 tensor-memory
+// accumulators the nine digit products of level i + j <= 3, and the drain warps combine them by level
+// in FP64 every DT_CH units.  Every term is thus carried to ~6e-8 (A) and 2^-31 r / r_min (B) of its size and summed in
 // integers, against FP32 rounding per term and FP32 block sums in the sinc engine; the call falls
 // back to the sinc engine when r_max / r_min > 2^8.
 //
 // One CTA per SM, units (a tile pair of 8 x 16 atoms = 128 records, times the q tiles) split evenly
 // over the CTAs.  Warp 0 issues the MMAs, warps 1-4 drain tensor memory, warps 5-8 make the records:
 // thread k computes record k's FP64 sines and cosines (e^{i Q_0 r}, the coarse and offset steps and
-// their powers) for every unit, one unit ahead, into a ring of four tables (the atom coordinates of the
-// next unit load meanwhile).  Warps 9-24 are two generator groups of eight that make the digits of
+// their powers) for every unit into the record table of the unit's generator group, as soon as the
+// group has read its previous unit (the atom coordinates of the next unit load meanwhile).  Warps 9-24 are two generator groups of eight that make the digits of
 // alternate units, each group into its own stage: lane l of the group's warp w writes records
 // 4l .. 4l + 3 of A rows PA w .. PA w + PA - 1 (and 64 + ...) and B rows 2w, 2w + 1 (and 16 + ...), one
 // 32-bit store per (row, digit plane) into the 128-byte-swizzled K-major stage.  Waits are bounded
@@ -57,7 +57,7 @@ constexpr int DT_GROUPS = 2;   // generator groups: group i % 2 makes unit i
 // Units per accumulator chunk: an accumulator gains one digit product of |.| <= 255 * 128 per record,
 // so 256 units (32768 records) keep every int32 sum below 1.07e9.
 constexpr int DT_CH = 256;
-constexpr int DT_GEN = 8;                                  // warps of a generator group (one per stage)
+constexpr int DT_GEN = 8;                                  // warps of a generator group
 constexpr int DT_REC = 4;                                  // record warps: one record a thread
 constexpr int DT_W_REC = 5, DT_W_GEN = DT_W_REC + DT_REC;  // first record warp, first generator warp
 constexpr int DT_THREADS = 32 * (DT_W_GEN + DT_GROUPS * DT_GEN);  // MMA, 4 drain, 4 record, generators
