@@ -632,8 +632,10 @@ DEBYE_GOLDEN = os.path.join(ROOT, "tests", "golden", "debye__fcc5000_neutron.npz
 def debye_measure(ctx, steps, warmup):
     """Exact Debye double sum (calcIntDebye), fcc sphere a = 4.078 A cropped to 5000 atoms, Gaussian
     displacement 0.05 A, neutron b = 7.63 fm, 1024 q in [0.1, 10).  `value` = atom pairs / call time of
-    the host-buffer C-ABI call (coordinates in, I(q) out); roofline: the FP32 pipe at 4 flops per
-    (pair, q) term over the kernel-only stage time.  The error is against the reference's own
+    the host-buffer C-ABI call (coordinates in, I(q) out).  The sum runs on the integer tensor cores
+    (debye_tc_kernel, the default on a uniform mesh); its roofline is stated as the FP32 sine recurrence's
+    was, 4 flops per (pair, q) term over the kernel-only stage time against the FP32 peak, so that the two
+    paths compare on one scale.  The error is against the reference's own
     calcIntDebye of the same input (tests/golden, made by tests/golden/make_golden.py)."""
     import xns_b200
     from xns_b200 import synth
